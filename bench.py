@@ -1,0 +1,340 @@
+"""Benchmark of the B200 `nextevent_path_tracer` (plain NEE+MIS) on the 1M-triangle workload.
+
+One step = one full render of the heightfield-and-spheres scene (512x512-vertex
+fBm floor + 2000 icospheres, 50% Oren-Nayar / 50% Lambert+Phong, 4 area
+lights, 1,162,250 triangles) at 1024x512, 64 spp, max depth 16
+(num_path_vertices 18): 33.5M camera paths. Inputs are synthetic and seeded
+(wurstrenderer_b200/scenes.py); the scene is resident in HBM before timing.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank renders the whole image with its own random streams
+(weak scaling: per-GPU work fixed) and the FP64 films are summed onto rank 0
+with one NCCL reduce per step. Rank 0 prints one JSON line.
+
+`value` is device time (CUDA events on the renderer's stream, summed over the K
+steps, max over ranks); `e2e` is the same metric through the public C ABI call
+with host output (wr_render: film copied device->host inside the timed region).
+The CPU baseline runs the oracle (the reference's own renderer code compiled
+here, or its FP64 restatement) on the box's host cores on a bounded sample of
+the same workload (full frame at reduced spp; per-path work is unchanged).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "heightfield_spheres_1M: 1024x512, 64 spp, num_path_vertices 18 (max depth 16), 1,162,250 triangles"
+METRIC = "Mpaths/s"
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def scene_path(rank, world, dist):
+    """Writes the seeded workload once per node (rank 0), shared by the other ranks."""
+    from wurstrenderer_b200 import scenes
+    d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_v1")
+    p = os.path.join(d, "heightfield_spheres.json")
+    if rank == 0 and not os.path.exists(p + ".done"):
+        scenes.write_heightfield_spheres(d)
+        open(p + ".done", "w").write("ok")
+    if world > 1:
+        dist.barrier()
+    while not os.path.exists(p + ".done"):
+        time.sleep(0.1)
+    return p
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.rows = []
+        self.proc = None
+        self.gpu = gpu_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def extend_traffic_per_ray():
+    """DRAM bytes per extend ray from the committed ncu capture summary, when present."""
+    p = os.path.join(ROOT, "profiles", "extend_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_baseline(path, budget_s=20.0):
+    """The reference's renderer code (oracle/_ref) or the oracle's restatement on the host cores."""
+    import oracle
+    cores = os.cpu_count() or 1
+    try:
+        import oracle as o
+        if o.reference_available():
+            out = os.path.join(tempfile.gettempdir(), "wurst_ref_bench.pfm")
+            spp = 1
+            rep = o.run_reference(path, out, spp=spp)
+            # grow the sample until it takes a few seconds of the budget
+            while rep["seconds"] < budget_s / 4 and spp < 64:
+                spp *= 2
+                rep = o.run_reference(path, out, spp=spp)
+            return {"value": rep["paths"] / rep["seconds"] / 1e6, "unit": METRIC, "cores": rep["threads"],
+                    "kind": "reference",
+                    "sample": "full 1024x512 frame at %d spp (%d paths), reference PathNeeRenderer::render() with "
+                              "Embree replaced by the oracle's FP32 BVH ray caster" % (spp, rep["paths"])}
+    except Exception as e:  # fall through to the restatement
+        print("reference baseline unavailable: %s" % e, file=sys.stderr)
+    sc = oracle.OracleScene(path)
+    spp = 1
+    _, sec, paths = sc.render(spp=spp, threads=cores)
+    while sec < budget_s / 4 and spp < 64:
+        spp *= 2
+        _, sec, paths = sc.render(spp=spp, threads=cores)
+    return {"value": paths / sec / 1e6, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": "full 1024x512 frame at %d spp (%d paths), FP64 oracle restatement" % (spp, paths)}
+
+
+def run_reference_arm(args, rank):
+    """--impl reference: the reference's CPU implementation on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    import oracle
+    path = scene_path(0, 1, None)
+    cores = os.cpu_count() or 1
+    use_ref = oracle.reference_available()
+    kind = "reference" if use_ref else "port"
+    spp_sample = 1
+    times, paths_total = [], 0
+    sc = None if use_ref else oracle.OracleScene(path)
+    out = os.path.join(tempfile.gettempdir(), "wurst_ref_arm.pfm")
+    for i in range(args.warmup + args.steps):
+        if use_ref:
+            rep = oracle.run_reference(path, out, spp=spp_sample, salt=i + 1)
+            sec, paths, threads = rep["seconds"], rep["paths"], rep["threads"]
+        else:
+            _, sec, paths = sc.render(spp=spp_sample, salt=i + 1, threads=cores)
+            threads = cores
+        if i >= args.warmup:
+            times.append(sec)
+            paths_total += paths
+    total = sum(times)
+    value = paths_total / total / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD,
+                       "sample": "each step: full 1024x512 frame at %d spp (same scene, same per-path work)" % spp_sample},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
+                             "sample": "full 1024x512 frame at %d spp per step, %d steps" % (spp_sample, args.steps)},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--queue-capacity", type=int, default=0)
+    args = ap.parse_args()
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local_rank = env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import wurstrenderer_b200 as wr
+
+    dist = None
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    wr.set_device(local_rank)
+    path = scene_path(rank, world, dist)
+
+    t0 = time.perf_counter()
+    scene = wr.Scene.from_file(path)
+    load_s = time.perf_counter() - t0
+    info = scene.info
+    W, H = info["width"], info["height"]
+    spp, nverts = info["num_spp"], info["num_path_vertices"]
+    film = torch.empty((H, W, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
+    qc = args.queue_capacity or None
+
+    def step(seed):
+        scene.render_device(film.data_ptr(), seed=seed, queue_capacity=qc)
+        st = scene.stats
+        if world > 1:
+            dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
+        return st
+
+    for i in range(args.warmup):
+        step(1000 * rank + i)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    dev_ms, launches, iters = 0.0, 0, 0
+    wall0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.fill_(float(i))               # evict L2 between timed steps (outside the per-step device timing)
+        torch.cuda.synchronize()
+        st = step(7919 * (rank + 1) + i)
+        dev_ms += st["render_ms"]
+        launches += st["kernel_launches"]
+        iters += st["iterations"]
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - wall0) * 1e3
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    paths_per_rank = W * H * spp
+    value = paths_per_rank * world * args.steps / (max_ms / 1e3) / 1e6
+
+    # end to end through the public C ABI with host output (device->host copy of the film inside)
+    host = np.empty((H, W, 3), np.float64)
+    e2e_ms = 0.0
+    for i in range(args.steps):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        scene.render(seed=424242 + i, out=host, queue_capacity=qc)
+        e2e_ms += (time.perf_counter() - a) * 1e3
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = paths_per_rank * world * args.steps / (float(e2e_t.item()) / 1e3) / 1e6
+
+    # one profiled render (per-kernel events + traversal counters) for the roofline, outside the timed region
+    scene.render_device(film.data_ptr(), seed=99, queue_capacity=qc, profile=2)
+    prof = scene.stats
+    kn = wr.KERNELS
+    k_ms = dict(zip(kn, prof["kernel_ms"]))
+    k_cnt = dict(zip(kn, prof["kernel_count"]))
+    k_items = dict(zip(kn, prof["kernel_items"]))
+    rays = k_items["extend"]
+    nv, nt = prof["extend_node_visits"], prof["extend_tri_tests"]
+    alg_bytes = 48 * rays + 64 * nv + 48 * nt            # 32 B ray in + 16 B hit out + 64 B/node + 48 B/triangle
+    launches_e = max(1, k_cnt["extend"])
+    avg_ms = k_ms["extend"] / launches_e
+    achieved = (alg_bytes / launches_e) / (avg_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    tr = extend_traffic_per_ray()
+    traffic = None
+    if tr:
+        traffic = tr["dram_bytes_per_ray"] * rays / launches_e
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
+                "alg_bytes_per_launch": alg_bytes / launches_e, "avg_launch_ms": avg_ms,
+                "rays_per_launch": rays / launches_e, "node_visits_per_ray": nv / max(1, rays),
+                "tri_tests_per_ray": nt / max(1, rays),
+                "kernel_share": {k: k_ms[k] / max(1e-9, sum(k_ms.values())) for k in kn}}
+
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 film + CDF build)", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": WORKLOAD, "parallelism": "replicas x%d, FP64 film reduce" % world,
+                       "l2": "256 MB buffer written between timed steps; path state > L2",
+                       "queue_capacity": prof["queue_capacity"], "grid_trace": prof["grid_trace"],
+                       "grid_shade": prof["grid_shade"], "scene_load_s": load_s,
+                       "bvh_nodes": info["bvh_nodes"], "bvh_depth": info["bvh_depth"],
+                       "iterations_per_step": iters / args.steps, "wall_ms_per_step": wall_ms / args.steps},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 104,
+                    "d2h_bytes_per_step": W * H * 3 * 8},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "clocks": clk,
+            "mrays_per_s": (k_items["extend"] + k_items["shadow"]) * world * args.steps / (max_ms / 1e3) / 1e6}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(path)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

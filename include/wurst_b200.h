@@ -1,0 +1,158 @@
+/*
+ * wurst_b200.h -- C ABI of the B200-native `nextevent_path_tracer`.
+ *
+ * Drop-in boundary for the reference's NEE+MIS integrator
+ * (jamornsriwasansak/wurstrenderer). The reference exposes the path as a
+ * Renderer plugin selected by name from a simple2 scene JSON and writes PFM
+ * images; this header is the plain-C surface underneath that boundary, with
+ * no C++ or torch types: plain pointers, sizes and status codes.
+ *
+ * Conventions: every function returns WR_OK (0) or a nonzero status and never
+ * throws across the ABI; wr_last_error() describes the last failure on the
+ * calling thread. Output buffers are owned by the caller. Each scene handle
+ * owns one CUDA stream on the current device; a handle is not re-entrant (one
+ * call at a time per handle), different handles may be used concurrently.
+ * Images are W*H*3 doubles, row 0 = top, x fastest, RGB -- the layout of the
+ * reference's Film / Fimage (src/common/film.h, src/common/floatimage.h).
+ */
+#ifndef WURST_B200_H
+#define WURST_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WR_ABI_VERSION 1
+
+/* status codes */
+#define WR_OK 0
+#define WR_ERR_INVALID_ARGUMENT 1
+#define WR_ERR_IO 2
+#define WR_ERR_PARSE 3
+#define WR_ERR_UNSUPPORTED 4
+#define WR_ERR_CUDA 5
+#define WR_ERR_OUT_OF_MEMORY 6
+#define WR_ERR_TIMEOUT 7
+
+typedef struct wr_scene wr_scene;
+
+typedef struct wr_render_desc {
+    int num_spp;             /* samples per pixel; <= 0 takes "num_spp" of the render entry (default 16) */
+    int num_path_vertices;   /* <= 0 takes "num_path_vertices" of the render entry (default 10) */
+    unsigned int seed;       /* selects the random streams; 0 is a valid seed */
+    int render_index;        /* which "render" entry supplies the defaults */
+    int queue_capacity;      /* wavefront slots; 0 = default (tuned) */
+    int grid_trace;          /* persistent blocks of the traversal kernels; 0 = occupancy-derived */
+    int grid_shade;          /* persistent blocks of shade / raygen; 0 = occupancy-derived */
+    int use_graph;           /* 1: replay captured CUDA graphs of the bounce loop; 0: plain launches */
+    int profile;             /* 0: off; 1: per-kernel CUDA-event timing (plain launches);
+                                2: timing + traversal counters (node visits, triangle tests) */
+    int reserved[7];
+} wr_render_desc;
+
+typedef struct wr_render_stats {
+    double render_ms;                 /* device time of the bounce loop + resolve */
+    unsigned long long paths;         /* camera samples traced (W*H*spp) */
+    unsigned long long iterations;    /* wavefront iterations executed */
+    unsigned int max_shadow_queue;    /* largest shadow-ray queue seen */
+    unsigned int queue_capacity;      /* wavefront slots used */
+    int grid_trace, grid_shade;
+    unsigned long long kernel_launches;   /* kernels launched by the render */
+    /* per-kernel totals, filled when desc.profile != 0 (index: WR_K_*) */
+    double kernel_ms[6];
+    unsigned long long kernel_count[6];   /* launches */
+    unsigned long long kernel_items[6];   /* rays / paths processed */
+    unsigned long long extend_node_visits, extend_tri_tests;   /* profile == 2 */
+    unsigned long long shadow_node_visits, shadow_tri_tests;
+} wr_render_stats;
+
+#define WR_K_EXTEND 0
+#define WR_K_SHADE 1
+#define WR_K_RAYGEN 2
+#define WR_K_SHADOW 3
+#define WR_K_ADVANCE 4
+#define WR_K_RESOLVE 5
+
+typedef struct wr_scene_info {
+    int width, height;                /* camera resolution */
+    int num_spp, num_path_vertices;   /* of render entry 0 (defaults when absent) */
+    unsigned long long num_triangles;
+    int num_meshes, num_lights, has_envmap;
+    int bvh_nodes, bvh_depth;
+    double bvh_sah_cost;
+    double build_ms;                  /* scene parse + BVH + upload + CDF build */
+    int num_renders;
+} wr_scene_info;
+
+/* Parses a simple2 scene JSON (Simple2Parser::Parse, src/sceneio/simple2parser.h:84-100),
+ * loads its OBJ/MTL meshes and envmap, builds the BVH and the FP64 light /
+ * environment CDFs, and uploads everything to the current CUDA device. */
+int wr_scene_create(const char *scene_json_path, wr_scene **out);
+
+/* Same from JSON text (the --jsimple2parse path, src/main.cpp:12-15);
+ * relative mesh paths resolve against base_dir (NULL: current directory). */
+int wr_scene_create_from_json(const char *json_text, const char *base_dir, wr_scene **out);
+
+void wr_scene_destroy(wr_scene *scene);
+
+/* Host-only validation of a scene (no GPU needed): parses the JSON and its
+ * meshes and builds the BVH exactly as wr_scene_create does, fills `info`
+ * (build_ms covers parse + BVH only) and uploads nothing. */
+int wr_scene_inspect(const char *scene_json_path, wr_scene_info *info);
+
+int wr_scene_get_info(const wr_scene *scene, wr_scene_info *info);
+
+/* Replaces the camera with a simple2 "camera" JSON object
+ * (ThinlensCamera::FromSimple2ParseJson, src/camera/thinlens.h:13-26). */
+int wr_scene_set_camera_json(wr_scene *scene, const char *camera_json);
+
+/* Renders with the NEE+MIS integrator ("nextevent_path_tracer",
+ * PathNeeRenderer::render, src/renderer/pathnextevent.h:152-191) and copies
+ * the W*H*3 image (base/spp + splat/(spp*W*H)) into host memory. desc may be
+ * NULL (defaults). */
+int wr_render(wr_scene *scene, const wr_render_desc *desc, double *out_rgb);
+
+/* Same, writing the image to device memory (W*H*3 doubles on the scene's
+ * device); no host copy. */
+int wr_render_device(wr_scene *scene, const wr_render_desc *desc, double *out_rgb_device);
+
+int wr_get_render_stats(const wr_scene *scene, wr_render_stats *stats);
+
+/* Closest-hit queries (EmbreeAccel::intersectTriangleInfo,
+ * src/accel/embreeaccel.h:425-464). rays: n x 8 floats
+ * (ox, oy, oz, tnear, dx, dy, dz, tfar) in host memory. Outputs (host):
+ * geom_id = Embree geomID (mesh attach order, -1 on a miss), prim_id =
+ * triangle within the mesh, t = hit distance, uv = 2 floats per ray
+ * (barycentric weights of vertices 1 and 2). uv may be NULL. */
+int wr_trace_closest(wr_scene *scene, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *uv);
+
+/* Occlusion queries (EmbreeAccel::isIntersect, src/accel/embreeaccel.h:336-351). */
+int wr_trace_occluded(wr_scene *scene, const float *rays, int n, int *occluded);
+
+/* Traversal statistics for a ray batch: totals of inner-node visits and
+ * triangle tests (the counts that define the traversal kernel's algorithmic bytes). */
+int wr_trace_stats(wr_scene *scene, const float *rays, int n, int any_hit, unsigned long long *node_visits,
+                   unsigned long long *tri_tests);
+
+/* PFM output in the reference's layout (FimageIo::SavePfmColor, src/common/floatimage.h:435-462). */
+int wr_write_pfm(const char *path, const double *rgb, int width, int height);
+
+/* Whole simple2 flow of the reference CLI (src/main.cpp:5-15,
+ * src/sceneio/simple2parser.h:102-223): load the scene, render every
+ * "nextevent_path_tracer" entry of "render" and write its "output" PFM next
+ * to the scene JSON. Other integrators return WR_ERR_UNSUPPORTED. */
+int wr_run_simple2(const char *scene_json_path);
+int wr_run_jsimple2(const char *json_text);
+
+/* Makes `device` the current CUDA device of the calling thread for this
+ * library (scene handles remember the device they were created on). */
+int wr_set_device(int device);
+
+const char *wr_last_error(void);
+int wr_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WURST_B200_H */

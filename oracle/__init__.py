@@ -126,7 +126,7 @@ def reference_available() -> bool:
 
 
 def run_reference(json_path, out_pfm, spp=None, vertices=None, salt=0, crop=None, serial=False,
-                  raw=None, camera=None, timeout=None, env=None):
+                  raw=None, camera=None, timeout=None, env=None, threads=None):
     """Runs the reference's own renderer code (oracle/_ref) and returns its JSON report."""
     cmd = [REF_BIN, "render", json_path, out_pfm]
     if spp is not None:
@@ -139,6 +139,8 @@ def run_reference(json_path, out_pfm, spp=None, vertices=None, salt=0, crop=None
         cmd += ["--crop"] + [str(int(c)) for c in crop]
     if serial:
         cmd += ["--serial"]
+    if threads is not None:
+        cmd += ["--threads", str(int(threads))]
     if raw is not None:
         cmd += ["--raw", raw]
     if camera is not None:

@@ -16,12 +16,12 @@
 //
 // Usage:
 //   wurst_ref render <scene.json> <out.pfm> [--spp N] [--vertices V] [--salt S]
-//            [--crop x0 y0 x1 y1] [--serial] [--raw out.f64] [--camera '<json>']
+//            [--crop x0 y0 x1 y1] [--serial] [--threads T] [--raw out.f64] [--camera '<json>']
 //   wurst_ref trace <scene.json> <rays.f32> <hits.bin>
 // `render` without --crop/--serial calls PathNeeRenderer::render() itself
 // (all hardware threads). --serial/--crop run the same per-tile loop as
-// render() (pathnextevent.h:152-191) over the selected tiles on one thread,
-// calling the reference's evalContribution and Film.
+// render() (pathnextevent.h:152-191) over the selected tiles on --threads
+// threads (default one), calling the reference's evalContribution and Film.
 // Prints one JSON line: {"seconds": render time, "paths": samples traced, ...}.
 
 #include "common/wurst.h"
@@ -171,6 +171,7 @@ int cmd_render(int argc, char **argv) {
     int spp = -1, nverts = -1, renderIndex = 0;
     unsigned salt = 0;
     bool serial = false, crop = false;
+    int threads = 1;
     int cx0 = 0, cy0 = 0, cx1 = 0, cy1 = 0;
     std::string raw, cam;
     for (int i = 4; i < argc; ++i) {
@@ -182,6 +183,7 @@ int cmd_render(int argc, char **argv) {
         else if (a == "--raw") raw = argv[++i];
         else if (a == "--camera") cam = argv[++i];
         else if (a == "--render-index") renderIndex = atoi(argv[++i]);
+        else if (a == "--threads") threads = std::max(1, atoi(argv[++i]));
         else if (a == "--crop") { crop = true; cx0 = atoi(argv[++i]); cy0 = atoi(argv[++i]); cx1 = atoi(argv[++i]); cy1 = atoi(argv[++i]); }
         else throw std::runtime_error("unknown option " + a);
     }
@@ -224,21 +226,29 @@ int cmd_render(int argc, char **argv) {
         film.mBaseScalingFactor = 1.0 / double(r->mNumSpp);
         film.mAtomicScalingFactor = 1.0 / double(r->mNumSpp) / double(npix);
         if (r->mNumPathVertices > 1) {
-            for (const TileB &b : sel) {
-                const Ibound2 bound(b.lo, b.hi);
-                const int tileSeed = bound.pMin[0] * H + bound.pMin[1];
-                shared_ptr<Sampler> ts = sampler->clone(tileSeed);
-                for (const Ivec2 pixel : bound) {
-                    ts->setPixel(pixel);
-                    for (int i = 0; i < r->mNumSpp; ++i) {
-                        Splat splats[2];
-                        r->evalContribution(splats, ts.get(), pixel);
-                        film.addSample(splats[0].mRaster, splats[0].mContrib);
-                        film.atomicAddSample(splats[1].mRaster, splats[1].mContrib);
-                        ts->nextSample();
+            std::atomic<size_t> next(0);
+            auto worker = [&]() {
+                for (size_t ti = next++; ti < sel.size(); ti = next++) {
+                    const TileB &b = sel[ti];
+                    const Ibound2 bound(b.lo, b.hi);
+                    const int tileSeed = bound.pMin[0] * H + bound.pMin[1];
+                    shared_ptr<Sampler> ts = sampler->clone(tileSeed);
+                    for (const Ivec2 pixel : bound) {
+                        ts->setPixel(pixel);
+                        for (int i = 0; i < r->mNumSpp; ++i) {
+                            Splat splats[2];
+                            r->evalContribution(splats, ts.get(), pixel);
+                            film.addSample(splats[0].mRaster, splats[0].mContrib);
+                            film.atomicAddSample(splats[1].mRaster, splats[1].mContrib);
+                            ts->nextSample();
+                        }
                     }
                 }
-            }
+            };
+            std::vector<std::thread> pool;
+            for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+            worker();
+            for (auto &th : pool) th.join();
         }
         paths = npix * r->mNumSpp;
         for (int y = 0; y < H; ++y)
@@ -255,7 +265,7 @@ int cmd_render(int argc, char **argv) {
         fclose(f);
     }
     printf("{\"seconds\": %.6f, \"paths\": %lld, \"load_seconds\": %.6f, \"threads\": %d, \"width\": %d, \"height\": %d}\n",
-           seconds, paths, loadSeconds, (serial || crop) ? 1 : Parallel::NumThreads(), W, H);
+           seconds, paths, loadSeconds, (serial || crop) ? threads : Parallel::NumThreads(), W, H);
     return 0;
 }
 

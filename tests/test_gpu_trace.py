@@ -1,0 +1,77 @@
+"""Traversal parity on the GPU: closest-hit triangle ids against the reference.
+
+The golden hits are the reference's own closest-hit answers
+(EmbreeAccel::intersectTriangleInfo through the oracle's restatement of Embree's
+triangle test). The B200 kernel uses a watertight test, so ids must agree
+exactly except on rays whose two candidate hits tie in distance within
+1e-5 relative, or that graze a triangle edge (barycentric within 1e-5 of an
+edge), where the two tests may legitimately pick different triangles.
+"""
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, GOLDEN, golden_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _tie_or_edge(t_ref, t_gpu, uv_ref):
+    tie = np.abs(t_ref - t_gpu) <= 1e-5 * np.maximum(np.abs(t_ref), 1.0)
+    edge = (uv_ref[:, 0] < 1e-5) | (uv_ref[:, 1] < 1e-5) | (1.0 - uv_ref[:, 0] - uv_ref[:, 1] < 1e-5)
+    return tie | edge
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_closest_hit_ids_match_reference(wr_lib, oracle_lib, name):
+    path, _ = golden_scene(name)
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name))
+    hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
+    with wr_lib.Scene.from_file(path) as sc:
+        g, p, t, uv = sc.trace_closest(rays)
+    _, _, _, uv_ref = oracle_lib.OracleScene(path).trace_closest(rays)
+    t_ref = hits[:, 2].view(np.float32)
+    same = (g == hits[:, 0]) & (p == hits[:, 1])
+    excused = _tie_or_edge(t_ref, t, uv_ref)
+    bad = ~same & ~excused
+    assert bad.sum() == 0, "mismatching rays: %s" % np.nonzero(bad)[0][:10]
+    assert same.mean() > 0.99
+    hit = same & (g >= 0)
+    assert np.allclose(t[hit], t_ref[hit], rtol=2e-5, atol=1e-6)
+    assert np.allclose(uv[hit], uv_ref[hit], atol=2e-4)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_occlusion_matches_oracle(wr_lib, oracle_lib, name):
+    path, _ = golden_scene(name)
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name)).copy()
+    hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
+    t_ref = hits[:, 2].view(np.float32)
+    # finite segments: half of them end before the closest hit, half after it
+    rng = np.random.default_rng(5)
+    tmax = np.where(hits[:, 0] >= 0, t_ref * np.where(rng.uniform(size=len(rays)) < 0.5, 0.5, 1.5), 10.0)
+    rays[:, 7] = tmax.astype(np.float32)
+    with wr_lib.Scene.from_file(path) as sc:
+        occ = sc.trace_occluded(rays)
+    occ_ref = oracle_lib.OracleScene(path).trace_occluded(rays)
+    assert (occ != occ_ref).mean() < 2e-3
+
+
+def test_empty_and_tiny_batches(wr_lib):
+    path, _ = golden_scene("cornell")
+    with wr_lib.Scene.from_file(path) as sc:
+        g, p, t, uv = sc.trace_closest(np.zeros((0, 8), np.float32))
+        assert g.shape == (0,)
+        r = np.array([[0, 1, 3.5, 1e-4, 0, 0, -1, np.inf]], np.float32)   # toward the back wall
+        g, p, t, uv = sc.trace_closest(r)
+        assert g[0] >= 0 and abs(t[0] - 4.5) < 1e-4
+        r = np.array([[0, 1, 3.5, 1e-4, 0, 0, 1, np.inf]], np.float32)    # out of the open front
+        g, p, t, uv = sc.trace_closest(r)
+        assert g[0] == -1 and p[0] == -1
+
+
+def test_traversal_statistics(wr_lib):
+    path, _ = golden_scene("hf")
+    rays = np.load("%s/hf_rays.npy" % GOLDEN)
+    with wr_lib.Scene.from_file(path) as sc:
+        nv, nt = sc.trace_stats(rays)
+    assert nv >= len(rays) and nt > 0

@@ -1,0 +1,129 @@
+"""Host-side logic of the B200 library, exercised without a GPU.
+
+Covers: the C ABI library loads and exports every function include/wurst_b200.h
+declares; scene loading (simple2 JSON, OBJ/MTL, PFM) and the BVH build agree
+with the oracle's reading of the same files; error statuses; the CLI flags.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, GOLDEN, ROOT, golden_scene
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "wurst_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char \*)\s*(wr_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol(wr_lib):
+    L = wr_lib.load_library()
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(wr_lib.EXPORTS)
+    assert L.wr_abi_version() == 1
+
+
+def test_symbols_visible_in_dynamic_table(wr_lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", wr_lib.LIB_PATH], capture_output=True, text=True).stdout
+    for n in declared_functions():
+        assert re.search(r"\bT %s\b" % n, out), n
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_inspect_matches_oracle_scene(wr_lib, oracle_lib, name):
+    path, _ = golden_scene(name)
+    info = wr_lib.inspect_scene(path)
+    sc = oracle_lib.OracleScene(path)
+    assert info["num_triangles"] == sc.num_triangles
+    assert info["num_meshes"] == sc.num_meshes
+    assert info["num_lights"] == sc.num_lights
+    assert (info["width"], info["height"]) == (sc.width, sc.height)
+    assert info["num_path_vertices"] == sc.num_path_vertices
+    assert 0 < info["bvh_depth"] <= 64
+    assert info["bvh_nodes"] >= 1
+    assert info["has_envmap"] == (1 if name == "env" else 0)
+
+
+def test_pfm_roundtrip_layout(wr_lib, tmp_path):
+    img = np.random.default_rng(1).uniform(size=(5, 7, 3))
+    p = str(tmp_path / "x.pfm")
+    wr_lib.write_pfm(p, img)
+    raw = open(p, "rb").read()
+    assert raw.startswith(b"PF\n7 5\n-1\n")
+    back = wr_lib.read_pfm(p)
+    assert np.array_equal(back, img.astype(np.float32))
+    # rows are stored bottom-to-top: the first stored row is the last image row
+    first = np.frombuffer(raw[len(b"PF\n7 5\n-1\n"):][:7 * 12], "<f4").reshape(7, 3)
+    assert np.array_equal(first, img[-1].astype(np.float32))
+
+
+def test_error_statuses(wr_lib, tmp_path):
+    with pytest.raises(wr_lib.WurstError) as e:
+        wr_lib.inspect_scene(str(tmp_path / "missing.json"))
+    assert e.value.status == 2
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"camera": [1, 2,')
+    with pytest.raises(wr_lib.WurstError) as e:
+        wr_lib.inspect_scene(str(bad))
+    assert e.value.status == 3
+    # emitters with Ns != 0 are SimpleMetal lights in the reference (assimpio.h:84-91): unsupported here
+    (tmp_path / "m.obj").write_text("mtllib m.mtl\no a\nusemtl e\nv 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
+    (tmp_path / "m.mtl").write_text("newmtl e\nKe 1 1 1\nNs 10\n")
+    (tmp_path / "s.json").write_text('{"meshes": [{"path": "m.obj"}]}')
+    with pytest.raises(wr_lib.WurstError) as e:
+        wr_lib.inspect_scene(str(tmp_path / "s.json"))
+    assert e.value.status == 4
+
+
+def test_obj_semantics(wr_lib, oracle_lib, tmp_path):
+    """Assimp-style reading: one mesh per object x material, a new object keeps the
+    current material (ObjFileParser::createObject), polygon fans, emitters attached
+    after the surfaces of their file."""
+    (tmp_path / "m.mtl").write_text("newmtl a\nKd 0.5 0.5 0.5\nnewmtl l\nKe 5 5 5\n")
+    (tmp_path / "m.obj").write_text(
+        "mtllib m.mtl\n"
+        "v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nv 0 0 1\n"
+        "o light\nusemtl l\nf 1 2 3\n"
+        "o quad\nusemtl a\nf 1 2 3 4\n"
+        "usemtl l\nf -1 -2 -3\n"
+        "o nomat\nf 1 3 5\n")
+    (tmp_path / "s.json").write_text(
+        '{"camera": {"pos": [0,0,5], "lookat": [0,0,0], "up": [0,1,0], "resolution": [8, 6]},'
+        ' "meshes": [{"path": "m.obj"}], "render": [{"integrator": "nextevent_path_tracer"}]}')
+    info = wr_lib.inspect_scene(str(tmp_path / "s.json"))
+    assert info["num_triangles"] == 1 + 2 + 1 + 1
+    assert info["num_meshes"] == 4
+    assert info["num_lights"] == 3
+    assert (info["num_spp"], info["num_path_vertices"]) == (16, 10)
+    sc = oracle_lib.OracleScene(str(tmp_path / "s.json"))
+    assert (sc.num_triangles, sc.num_meshes, sc.num_lights) == (5, 4, 3)
+
+
+def test_cli_reports_errors(wr_lib, tmp_path):
+    r = subprocess.run([wr_lib.CLI_PATH, "--simple2parse", str(tmp_path / "nope.json")], capture_output=True,
+                       text=True, cwd=str(tmp_path))
+    assert r.returncode == 1
+    assert "file not found" in r.stderr
+
+
+def test_cli_default_txt_created(wr_lib, tmp_path):
+    r = subprocess.run([wr_lib.CLI_PATH], capture_output=True, text=True, cwd=str(tmp_path))
+    assert r.returncode == 0
+    assert (tmp_path / "default.txt").exists()
+
+
+def test_heightfield_workload_size(wr_lib, tmp_path):
+    """The 1M-triangle workload: 511^2*2 floor + 2000 x 320-face spheres + 4 quad lights."""
+    from wurstrenderer_b200 import scenes
+    path = scenes.write_heightfield_spheres(str(tmp_path), spp=64)
+    info = wr_lib.inspect_scene(path)
+    assert info["num_triangles"] == 511 * 511 * 2 + 2000 * 320 + 4 * 2
+    assert info["num_lights"] == 4
+    assert (info["width"], info["height"], info["num_spp"], info["num_path_vertices"]) == (1024, 512, 64, 18)
+    assert info["bvh_depth"] <= 64

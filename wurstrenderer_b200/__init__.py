@@ -1,0 +1,273 @@
+"""B200-native `nextevent_path_tracer`: Python access to the C ABI.
+
+The product is ``libwurst_b200.so`` (host C++ + sm_100a CUDA, declared in
+``include/wurst_b200.h``) and the ``wurst_b200`` CLI, a drop-in for the
+reference's ``--simple2parse`` / ``--jsimple2parse`` flow. This module is a
+thin ctypes layer over that library for tests, the benchmark and scripting; it
+mirrors the reference's entry points:
+
+* :func:`Simple2Parser.Parse` -- ``Simple2Parser::Parse`` (src/sceneio/simple2parser.h:84-223):
+  load a scene JSON, render every ``nextevent_path_tracer`` entry, write its PFM;
+* :class:`Scene` -- a parsed, uploaded scene (``Simple2Parser::ParseScene`` + BVH build);
+* :meth:`Scene.render` -- ``PathNeeRenderer::render`` (src/renderer/pathnextevent.h:152-191)
+  returning the film image (base/spp + splat/(spp*W*H)) as an HxWx3 float64 array.
+
+There is no CPU fallback: every call runs the CUDA kernels, and loading fails
+loudly when the library has not been built or no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libwurst_b200.so")
+CLI_PATH = os.path.join(PKG_DIR, "wurst_b200")
+
+WR_OK = 0
+_STATUS = {1: "invalid argument", 2: "i/o error", 3: "parse error", 4: "unsupported", 5: "cuda error",
+           6: "out of memory", 7: "timeout"}
+
+
+class WurstError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s (status %d: %s)" % (message, status, _STATUS.get(status, "?")))
+        self.status = status
+
+
+class RenderDesc(ctypes.Structure):
+    _fields_ = [("num_spp", ctypes.c_int), ("num_path_vertices", ctypes.c_int), ("seed", ctypes.c_uint),
+                ("render_index", ctypes.c_int), ("queue_capacity", ctypes.c_int), ("grid_trace", ctypes.c_int),
+                ("grid_shade", ctypes.c_int), ("use_graph", ctypes.c_int), ("profile", ctypes.c_int),
+                ("reserved", ctypes.c_int * 7)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("render_ms", ctypes.c_double), ("paths", ctypes.c_ulonglong), ("iterations", ctypes.c_ulonglong),
+                ("max_shadow_queue", ctypes.c_uint), ("queue_capacity", ctypes.c_uint),
+                ("grid_trace", ctypes.c_int), ("grid_shade", ctypes.c_int),
+                ("kernel_launches", ctypes.c_ulonglong), ("kernel_ms", ctypes.c_double * 6),
+                ("kernel_count", ctypes.c_ulonglong * 6), ("kernel_items", ctypes.c_ulonglong * 6),
+                ("extend_node_visits", ctypes.c_ulonglong), ("extend_tri_tests", ctypes.c_ulonglong),
+                ("shadow_node_visits", ctypes.c_ulonglong), ("shadow_tri_tests", ctypes.c_ulonglong)]
+
+
+KERNELS = ["extend", "shade", "raygen", "shadow", "advance", "resolve"]
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("num_spp", ctypes.c_int),
+                ("num_path_vertices", ctypes.c_int), ("num_triangles", ctypes.c_ulonglong),
+                ("num_meshes", ctypes.c_int), ("num_lights", ctypes.c_int), ("has_envmap", ctypes.c_int),
+                ("bvh_nodes", ctypes.c_int), ("bvh_depth", ctypes.c_int), ("bvh_sah_cost", ctypes.c_double),
+                ("build_ms", ctypes.c_double), ("num_renders", ctypes.c_int)]
+
+
+# every function the C ABI exports (include/wurst_b200.h)
+EXPORTS = ["wr_scene_create", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
+           "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
+           "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
+           "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version"]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libwurst_b200.so (built by ``wurstrenderer_b200.build``); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise WurstError(4, "libwurst_b200.so is not built (run python -m wurstrenderer_b200.build)")
+    L = ctypes.CDLL(path)
+    vp, cp, ip, fp = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p
+    L.wr_last_error.restype = ctypes.c_char_p
+    L.wr_abi_version.restype = ctypes.c_int
+    L.wr_scene_create.argtypes = [cp, ctypes.POINTER(vp)]
+    L.wr_scene_create_from_json.argtypes = [cp, cp, ctypes.POINTER(vp)]
+    L.wr_scene_destroy.argtypes = [vp]
+    L.wr_scene_destroy.restype = None
+    L.wr_scene_get_info.argtypes = [vp, ctypes.POINTER(SceneInfo)]
+    L.wr_scene_inspect.argtypes = [cp, ctypes.POINTER(SceneInfo)]
+    L.wr_scene_set_camera_json.argtypes = [vp, cp]
+    L.wr_render.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
+    L.wr_render_device.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
+    L.wr_get_render_stats.argtypes = [vp, ctypes.POINTER(RenderStats)]
+    L.wr_trace_closest.argtypes = [vp, fp, ip, fp, fp, fp, fp]
+    L.wr_trace_occluded.argtypes = [vp, fp, ip, fp]
+    L.wr_trace_stats.argtypes = [vp, fp, ip, ip, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
+    L.wr_write_pfm.argtypes = [cp, fp, ip, ip]
+    L.wr_run_simple2.argtypes = [cp]
+    L.wr_run_jsimple2.argtypes = [cp]
+    L.wr_set_device.argtypes = [ip]
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != WR_OK:
+        raise WurstError(rc, load_library().wr_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else ctypes.c_void_p(int(a))
+
+
+class Scene:
+    """A simple2 scene parsed, BVH-built and uploaded to the current CUDA device."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_file(cls, json_path: str) -> "Scene":
+        L = load_library()
+        h = ctypes.c_void_p()
+        _check(L.wr_scene_create(os.fspath(json_path).encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_json(cls, json_text: str, base_dir: str = ".") -> "Scene":
+        L = load_library()
+        h = ctypes.c_void_p()
+        _check(L.wr_scene_create_from_json(json_text.encode(), base_dir.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            load_library().wr_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def info(self) -> dict:
+        inf = SceneInfo()
+        _check(load_library().wr_scene_get_info(self._h, ctypes.byref(inf)))
+        return {k: getattr(inf, k) for k, _ in SceneInfo._fields_}
+
+    def set_camera(self, camera_json: str) -> None:
+        _check(load_library().wr_scene_set_camera_json(self._h, camera_json.encode()))
+
+    @staticmethod
+    def _desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
+              profile=0):
+        d = RenderDesc()
+        d.num_spp = int(spp or 0)
+        d.num_path_vertices = int(num_path_vertices or 0)
+        d.seed = int(seed) & 0xFFFFFFFF
+        d.render_index = int(render_index)
+        d.queue_capacity = int(queue_capacity or 0)
+        d.grid_trace = int(grid_trace or 0)
+        d.grid_shade = int(grid_shade or 0)
+        d.use_graph = 1 if use_graph else 0
+        d.profile = int(profile)
+        return d
+
+    def render(self, spp=None, num_path_vertices=None, seed=0, render_index=0, queue_capacity=None,
+               grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0) -> np.ndarray:
+        """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top)."""
+        inf = self.info
+        if out is None:
+            out = np.empty((inf["height"], inf["width"], 3), np.float64)
+        d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
+                       profile)
+        _check(load_library().wr_render(self._h, ctypes.byref(d), _ptr(out)))
+        return out
+
+    def render_device(self, out_device_ptr: int, spp=None, num_path_vertices=None, seed=0, render_index=0,
+                      queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0) -> None:
+        """Renders into device memory at `out_device_ptr` (W*H*3 doubles)."""
+        d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
+                       profile)
+        _check(load_library().wr_render_device(self._h, ctypes.byref(d), ctypes.c_void_p(int(out_device_ptr))))
+
+    @property
+    def stats(self) -> dict:
+        st = RenderStats()
+        _check(load_library().wr_get_render_stats(self._h, ctypes.byref(st)))
+        out = {}
+        for k, _ in RenderStats._fields_:
+            v = getattr(st, k)
+            out[k] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
+
+    def trace_closest(self, rays: np.ndarray):
+        """rays (n, 8) float32 [ox, oy, oz, tnear, dx, dy, dz, tfar] -> (geom_id, prim_id, t, uv)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        g = np.empty(n, np.int32); p = np.empty(n, np.int32)
+        t = np.empty(n, np.float32); uv = np.empty((n, 2), np.float32)
+        _check(load_library().wr_trace_closest(self._h, _ptr(rays), n, _ptr(g), _ptr(p), _ptr(t), _ptr(uv)))
+        return g, p, t, uv
+
+    def trace_occluded(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, np.float32)
+        occ = np.empty(rays.shape[0], np.int32)
+        _check(load_library().wr_trace_occluded(self._h, _ptr(rays), rays.shape[0], _ptr(occ)))
+        return occ
+
+    def trace_stats(self, rays: np.ndarray, any_hit=False):
+        """Total inner-node visits and triangle tests for a ray batch."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        nv, nt = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+        _check(load_library().wr_trace_stats(self._h, _ptr(rays), rays.shape[0], 1 if any_hit else 0,
+                                             ctypes.byref(nv), ctypes.byref(nt)))
+        return int(nv.value), int(nt.value)
+
+
+def set_device(device: int) -> None:
+    """Selects the CUDA device the library uses on this thread."""
+    _check(load_library().wr_set_device(int(device)))
+
+
+def inspect_scene(json_path: str) -> dict:
+    """Host-only scene validation (parse + BVH build, no GPU): returns the scene info."""
+    inf = SceneInfo()
+    _check(load_library().wr_scene_inspect(os.fspath(json_path).encode(), ctypes.byref(inf)))
+    return {k: getattr(inf, k) for k, _ in SceneInfo._fields_}
+
+
+class Simple2Parser:
+    """The reference's scene-JSON entry point (src/sceneio/simple2parser.h)."""
+
+    @staticmethod
+    def Parse(scene_json_path: str) -> None:
+        _check(load_library().wr_run_simple2(os.fspath(scene_json_path).encode()))
+
+    @staticmethod
+    def ParseJson(json_text: str) -> None:
+        _check(load_library().wr_run_jsimple2(json_text.encode()))
+
+
+def write_pfm(path: str, image: np.ndarray) -> None:
+    """PFM in the reference's layout (rows bottom-to-top, little-endian float RGB)."""
+    img = np.ascontiguousarray(image, np.float64)
+    _check(load_library().wr_write_pfm(os.fspath(path).encode(), _ptr(img), img.shape[1], img.shape[0]))
+
+
+def read_pfm(path: str) -> np.ndarray:
+    """Reads a PFM into an (H, W, 3) float32 array, row 0 = top."""
+    with open(path, "rb") as f:
+        head = f.readline().strip()
+        dims = f.readline().split()
+        scale = float(f.readline())
+        w, h = int(dims[0]), int(dims[1])
+        nc = 3 if head == b"PF" else 1
+        data = np.frombuffer(f.read(), dtype="<f4" if scale < 0 else ">f4", count=w * h * nc)
+    img = data.reshape(h, w, nc)[::-1]
+    if nc == 1:
+        img = np.repeat(img, 3, axis=2)
+    return np.ascontiguousarray(img, np.float32)

@@ -1,0 +1,272 @@
+// Host binned-SAH BVH builder for the B200 traversal kernels (the role of
+// Embree's BVH8Triangle4 SAH build behind EmbreeAccel::commit,
+// src/accel/embreeaccel.h:466-469; the reference never exposes its tree, so
+// only the query results -- not the tree -- are part of the drop-in contract).
+//
+// Output layout (one node = 64 bytes = 4 x float4, loaded with 16-byte vector
+// loads on the device):
+//   float4 a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   float4 b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   float4 c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   float4 d = (child0, child1, 0, 0) as int bits
+// A child >= 0 is an inner node index; a child with bit 31 set is a leaf:
+// bits 0-26 first triangle (leaf order), bits 27-30 count - 1. An empty child
+// carries a box at +infinity so that it is never entered. Nodes are stored in
+// depth-first order (left child right after its parent) so that a traversal
+// descending to the near child mostly touches adjacent cache lines.
+// Top levels are built in parallel with std::thread.
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <thread>
+
+#include "wr_host.h"
+
+namespace wr {
+namespace {
+
+struct Aabb {
+    float lo[3] = {INFINITY, INFINITY, INFINITY};
+    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    void grow(const Aabb &b) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], b.lo[k]); hi[k] = std::max(hi[k], b.hi[k]); }
+    }
+    void grow(const float *p) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+    }
+    double half_area() const {
+        if (!(hi[0] >= lo[0])) return 0.0;
+        const double dx = double(hi[0]) - lo[0], dy = double(hi[1]) - lo[1], dz = double(hi[2]) - lo[2];
+        return dx * dy + dy * dz + dz * dx;
+    }
+};
+
+struct TmpNode {
+    Aabb box;
+    int child[2] = {-1, -1};
+    uint32_t start = 0, count = 0;   // leaf when child[0] < 0
+};
+
+constexpr int kBins = 32;
+constexpr uint32_t kMaxLeafHard = 16;   // 4-bit count field
+constexpr int kDepthBudget = 60;         // traversal stack holds 64 entries
+
+struct Builder {
+    const std::vector<float> &v;       // 9 floats per triangle
+    std::vector<Aabb> tbox;
+    std::vector<float> cen;            // 3 per triangle
+    std::vector<uint32_t> idx;
+    std::vector<TmpNode> nodes;
+    std::atomic<int> next_node{0};
+    int max_leaf;
+    int par_depth;
+
+    Builder(const std::vector<float> &verts, int ml, int threads) : v(verts), max_leaf(ml) {
+        const size_t n = v.size() / 9;
+        tbox.resize(n);
+        cen.resize(3 * n);
+        idx.resize(n);
+        nodes.resize(std::max<size_t>(2 * n + 1, 3));
+        par_depth = 0;
+        while ((1 << par_depth) < threads * 2) ++par_depth;
+        auto prep = [&](size_t a, size_t b) {
+            for (size_t i = a; i < b; ++i) {
+                Aabb bb;
+                for (int c = 0; c < 3; ++c) bb.grow(&v[9 * i + 3 * c]);
+                tbox[i] = bb;
+                for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5f * (bb.lo[k] + bb.hi[k]);
+                idx[i] = uint32_t(i);
+            }
+        };
+        std::vector<std::thread> th;
+        const size_t chunk = (n + threads - 1) / std::max(threads, 1);
+        for (int t = 0; t < threads; ++t) {
+            size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+            if (a < b) th.emplace_back(prep, a, b);
+        }
+        for (auto &x : th) x.join();
+    }
+
+    int alloc() { return next_node.fetch_add(1); }
+
+    // builds the subtree over idx[start, start+count) into node `ni`
+    void build(int ni, uint32_t start, uint32_t count, int depth) {
+        TmpNode &nd = nodes[ni];
+        Aabb box, cb;
+        for (uint32_t i = start; i < start + count; ++i) {
+            const uint32_t t = idx[i];
+            box.grow(tbox[t]);
+            cb.grow(&cen[3 * size_t(t)]);
+        }
+        nd.box = box;
+        if (count <= 1) { nd.start = start; nd.count = count; return; }
+
+        // binned SAH over the three axes
+        int best_axis = -1, best_split = -1;
+        double best_cost = INFINITY;
+        for (int ax = 0; ax < 3; ++ax) {
+            const float ext = cb.hi[ax] - cb.lo[ax];
+            if (!(ext > 0.f)) continue;
+            const float scale = kBins / ext;
+            Aabb bins[kBins];
+            uint32_t cnt[kBins] = {0};
+            for (uint32_t i = start; i < start + count; ++i) {
+                const uint32_t t = idx[i];
+                int b = int((cen[3 * size_t(t) + ax] - cb.lo[ax]) * scale);
+                b = std::min(std::max(b, 0), kBins - 1);
+                cnt[b]++;
+                bins[b].grow(tbox[t]);
+            }
+            double right_area[kBins];
+            uint32_t right_cnt[kBins];
+            Aabb acc;
+            uint32_t c = 0;
+            for (int b = kBins - 1; b > 0; --b) {
+                acc.grow(bins[b]);
+                c += cnt[b];
+                right_area[b] = acc.half_area();
+                right_cnt[b] = c;
+            }
+            acc = Aabb();
+            c = 0;
+            for (int b = 0; b < kBins - 1; ++b) {
+                acc.grow(bins[b]);
+                c += cnt[b];
+                if (c == 0 || right_cnt[b + 1] == 0) continue;
+                const double cost = acc.half_area() * c + right_area[b + 1] * right_cnt[b + 1];
+                if (cost < best_cost) { best_cost = cost; best_axis = ax; best_split = b; }
+            }
+        }
+        const double parent_area = box.half_area();
+        // SAH with traversal cost 1 and triangle cost 1 (relative to the parent's area)
+        const double split_cost = 1.0 + (parent_area > 0 ? best_cost / parent_area : double(count));
+        const double leaf_cost = double(count);
+        if (count <= uint32_t(max_leaf) && (best_axis < 0 || leaf_cost <= split_cost)) {
+            nd.start = start; nd.count = count; return;
+        }
+        uint32_t nl;
+        int log2c = 0;
+        while ((1u << log2c) < count) ++log2c;
+        if (best_axis >= 0 && depth + log2c >= kDepthBudget) {
+            // keep the tree shallower than the traversal stack: object median on the widest axis
+            int ax = 0;
+            for (int k = 1; k < 3; ++k) if (cb.hi[k] - cb.lo[k] > cb.hi[ax] - cb.lo[ax]) ax = k;
+            nl = count / 2;
+            std::nth_element(idx.begin() + start, idx.begin() + start + nl, idx.begin() + start + count,
+                             [&](uint32_t a, uint32_t b2) { return cen[3 * size_t(a) + ax] < cen[3 * size_t(b2) + ax]; });
+        } else if (best_axis < 0) {
+            nl = count / 2;   // coincident centroids: split the range
+        } else {
+            const float ext = cb.hi[best_axis] - cb.lo[best_axis];
+            const float scale = kBins / ext;
+            auto mid = std::partition(idx.begin() + start, idx.begin() + start + count, [&](uint32_t t) {
+                int b = int((cen[3 * size_t(t) + best_axis] - cb.lo[best_axis]) * scale);
+                b = std::min(std::max(b, 0), kBins - 1);
+                return b <= best_split;
+            });
+            nl = uint32_t(mid - (idx.begin() + start));
+            if (nl == 0 || nl == count) nl = count / 2;
+        }
+        const int l = alloc(), r = alloc();
+        nd.child[0] = l;
+        nd.child[1] = r;
+        if (depth < par_depth && count > 65536) {
+            auto fut = std::async(std::launch::async, [&, l, start, nl, depth] { build(l, start, nl, depth + 1); });
+            build(r, start + nl, count - nl, depth + 1);
+            fut.get();
+        } else {
+            build(l, start, nl, depth + 1);
+            build(r, start + nl, count - nl, depth + 1);
+        }
+    }
+};
+
+void put_child_box(float *out, int slot, const Aabb &b, bool empty) {
+    // slot 0 -> a.xyzw + c.xy, slot 1 -> b.xyzw + c.zw
+    float lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = empty ? INFINITY : b.lo[k];   // a box at +inf is missed by every ray
+        hi[k] = empty ? INFINITY : b.hi[k];
+    }
+    float *xy = out + (slot == 0 ? 0 : 4);
+    xy[0] = lo[0]; xy[1] = hi[0]; xy[2] = lo[1]; xy[3] = hi[1];
+    out[8 + 2 * slot] = lo[2];
+    out[9 + 2 * slot] = hi[2];
+}
+
+}  // namespace
+
+BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_leaf, int threads) {
+    BvhBuildResult res;
+    const uint32_t n = uint32_t(tri_vertices.size() / 9);
+    if (threads <= 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    max_leaf = std::max(1, std::min(max_leaf, int(kMaxLeafHard)));
+    if (n >= (1u << 27)) throw Error(WR_ERR_UNSUPPORTED, "more than 2^27 triangles");
+    Builder b(tri_vertices, max_leaf, threads);
+    const int root = b.alloc();
+    if (n > 0) b.build(root, 0, n, 0);
+    else b.nodes[root].count = 0;
+
+    // depth-first linearisation; the device root is always an inner node
+    std::vector<std::pair<int, int>> order;   // (tmp node, device slot)
+    std::vector<int> dev_of(size_t(b.next_node.load()), -1);
+    res.tri_order.reserve(n);
+    std::vector<float> &out = res.nodes;
+    struct Item { int tmp; int depth; };
+    // assign device indices to inner nodes in DFS preorder
+    std::vector<int> inner_order;
+    {
+        std::vector<Item> st{{root, 0}};
+        while (!st.empty()) {
+            Item it = st.back(); st.pop_back();
+            const TmpNode &nd = b.nodes[it.tmp];
+            if (nd.child[0] < 0 && it.tmp != root) continue;
+            dev_of[it.tmp] = int(inner_order.size());
+            inner_order.push_back(it.tmp);
+            res.depth = std::max(res.depth, it.depth + 1);
+            if (nd.child[0] >= 0) {
+                st.push_back({nd.child[1], it.depth + 1});
+                st.push_back({nd.child[0], it.depth + 1});
+            }
+        }
+    }
+    out.assign(inner_order.size() * 16, 0.f);
+    const double root_area = std::max(b.nodes[root].box.half_area(), 1e-30);
+    for (size_t di = 0; di < inner_order.size(); ++di) {
+        const TmpNode &nd = b.nodes[inner_order[di]];
+        float *o = &out[di * 16];
+        int32_t child_code[2];
+        if (nd.child[0] < 0) {
+            // the whole scene is one leaf: child 0 holds it, child 1 is empty
+            const uint32_t first = uint32_t(res.tri_order.size());
+            for (uint32_t i = nd.start; i < nd.start + nd.count; ++i) res.tri_order.push_back(b.idx[i]);
+            put_child_box(o, 0, nd.box, nd.count == 0);
+            put_child_box(o, 1, nd.box, true);
+            child_code[0] = int32_t(0x80000000u | (uint32_t(std::max<uint32_t>(nd.count, 1) - 1) << 27) | first);
+            child_code[1] = int32_t(0x80000000u);
+            res.sah_cost += nd.box.half_area() / root_area * nd.count;
+        } else {
+            res.sah_cost += nd.box.half_area() / root_area;
+            for (int s = 0; s < 2; ++s) {
+                const TmpNode &c = b.nodes[nd.child[s]];
+                put_child_box(o, s, c.box, false);
+                if (c.child[0] >= 0) {
+                    child_code[s] = dev_of[nd.child[s]];
+                } else {
+                    const uint32_t first = uint32_t(res.tri_order.size());
+                    for (uint32_t i = c.start; i < c.start + c.count; ++i) res.tri_order.push_back(b.idx[i]);
+                    child_code[s] = int32_t(0x80000000u | ((c.count - 1) << 27) | first);
+                    res.sah_cost += c.box.half_area() / root_area * c.count;
+                }
+            }
+        }
+        memcpy(&o[12], &child_code[0], 4);
+        memcpy(&o[13], &child_code[1], 4);
+    }
+    return res;
+}
+
+}  // namespace wr

@@ -1,0 +1,807 @@
+// C ABI of the B200 renderer (include/wurst_b200.h): scene upload, the
+// wavefront render loop, ray-batch queries and the simple2 CLI flow.
+//
+// Scene creation mirrors Simple2Parser::ParseScene + the GeneralSubpathSampler
+// constructor (src/sceneio/simple2parser.h:27-68,
+// src/pathsampler/generalsubpathsampler.h:162-183): meshes are flattened in
+// Embree attach order, the BVH is built, and the light-selection CDF
+// (|average Ke| per emitter, 1.23 for the environment, src/light/diffusearealight.h:21-24,
+// src/light/envmap.h:22-26), the per-emitter triangle-area CDFs
+// (src/geometry/trianglemesh.h:110-129) and the environment's sin-weighted
+// luminance CDF (src/sphericalrepresentation/equirectangular.h:33-64) are
+// built as FP64 prefix sums on the device.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/wurst_b200.h"
+#include "wr_host.h"
+#include "wr_kernels.h"
+
+using wr::Error;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define WR_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            throw Error(e_ == cudaErrorMemoryAllocation ? WR_ERR_OUT_OF_MEMORY : WR_ERR_CUDA,  \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() {}
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t n) {
+        if (n <= bytes && p) return;
+        release();
+        WR_CUDA(cudaMalloc(&p, std::max<size_t>(n, 16)));
+        bytes = n;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+template <typename T> void upload(DevBuf &b, const std::vector<T> &v, cudaStream_t st) {
+    b.alloc(v.size() * sizeof(T));
+    if (!v.empty()) WR_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+}  // namespace
+
+struct wr_scene {
+    wr::Scene host;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    // scene data
+    DevBuf nodes, tris, tri_mat, materials, lights, light_tris, light_tri_cdf, light_tri_pdf, light_cdf, light_pdf;
+    DevBuf env_texels, env_pixel_pdf, env_row_cdf, env_row_pdf, env_col_cdf, env_col_pdf;
+    wrd::DevScene dev{};
+    int bvh_nodes = 0, bvh_depth = 0;
+    double sah_cost = 0.0, build_ms = 0.0;
+    // wavefront buffers
+    DevBuf w_o[2], w_d[2], w_thr[2], w_meta[2], w_hit, w_sho, w_shd, w_shc, w_film, w_ctr, w_sample, w_out, w_prof;
+    std::vector<cudaEvent_t> kev;
+    uint32_t w_capacity = 0;
+    size_t w_npix = 0;
+    uint32_t *pinned = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    wr_render_stats stats{};
+    ~wr_scene() {
+        if (pinned) cudaFreeHost(pinned);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto e : kev) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int fail(const Error &e) {
+    g_last_error = e.what();
+    return e.code;
+}
+
+// ------------------------------------------------------------ scene upload ----
+void build_device_scene(wr_scene &s) {
+    const auto t0 = std::chrono::steady_clock::now();
+    wr::Scene &h = s.host;
+    WR_CUDA(cudaGetDevice(&s.device));
+    WR_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    WR_CUDA(cudaEventCreate(&s.ev0));
+    WR_CUDA(cudaEventCreate(&s.ev1));
+    WR_CUDA(cudaMallocHost(reinterpret_cast<void **>(&s.pinned), 64));
+    cudaStream_t st = s.stream;
+
+    // flatten triangles in attach order
+    const uint64_t ntri64 = h.num_triangles();
+    if (ntri64 >= (1ull << 27)) throw Error(WR_ERR_UNSUPPORTED, "scene has more than 2^27 triangles");
+    const uint32_t ntri = uint32_t(ntri64);
+    std::vector<float> verts(size_t(ntri) * 9);
+    std::vector<uint32_t> tri_mesh(ntri), tri_prim(ntri), tri_code(ntri);
+    {
+        size_t g = 0;
+        for (size_t mi = 0; mi < h.meshes.size(); ++mi) {
+            const wr::Mesh &m = h.meshes[mi];
+            const uint32_t code = m.light >= 0 ? (wrd::LIGHT_BIT | uint32_t(m.light)) : uint32_t(m.material);
+            for (uint32_t t = 0; t < m.num_triangles(); ++t, ++g) {
+                for (int c = 0; c < 3; ++c) {
+                    const uint32_t vi = m.indices[3 * t + c];
+                    if (size_t(vi) * 3 + 2 >= m.positions.size()) throw Error(WR_ERR_PARSE, "mesh index out of range");
+                    for (int k = 0; k < 3; ++k) verts[9 * g + 3 * c + k] = m.positions[3 * size_t(vi) + k];
+                }
+                tri_mesh[g] = uint32_t(mi);
+                tri_prim[g] = t;
+                tri_code[g] = code;
+            }
+        }
+    }
+    wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, 4, 0);
+    s.bvh_nodes = int(bvh.nodes.size() / 16);
+    s.bvh_depth = bvh.depth;
+    s.sah_cost = bvh.sah_cost;
+    if (bvh.depth > wrd::kMaxStack) throw Error(WR_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
+    std::vector<float> trisf(size_t(ntri) * 12);
+    std::vector<uint32_t> leaf_mat(ntri);
+    for (uint32_t i = 0; i < ntri; ++i) {
+        const uint32_t g = bvh.tri_order[i];
+        float *o = &trisf[12 * size_t(i)];
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) o[4 * c + k] = verts[9 * size_t(g) + 3 * c + k];
+        memcpy(&o[3], &g, 4);
+        memcpy(&o[7], &tri_mesh[g], 4);
+        memcpy(&o[11], &tri_prim[g], 4);
+        leaf_mat[i] = tri_code[g];
+    }
+    upload(s.nodes, bvh.nodes, st);
+    upload(s.tris, trisf, st);
+    upload(s.tri_mat, leaf_mat, st);
+
+    // materials
+    std::vector<wrd::DevMaterial> mats(std::max<size_t>(h.materials.size(), 1));
+    for (size_t i = 0; i < h.materials.size(); ++i) {
+        const wr::Material &m = h.materials[i];
+        wrd::DevMaterial d{};
+        for (int k = 0; k < 3; ++k) { d.kd[k] = m.kd[k]; d.ks[k] = m.ks[k]; }
+        d.exponent = m.exponent;
+        d.flags = (m.has_diffuse ? wrd::MAT_DIFFUSE : 0) | (m.has_glossy ? wrd::MAT_GLOSSY : 0);
+        if (m.sigma >= 0.f && m.has_diffuse) {
+            const double s2 = double(m.sigma) * m.sigma;
+            d.on_a = float(1.0 - s2 / (2 * (s2 + 0.33)));
+            d.on_b = float(0.45 * s2 / (s2 + 0.09));
+            d.flags |= wrd::MAT_OREN_NAYAR;
+        } else {
+            d.on_a = 1.f;
+            d.on_b = 0.f;
+        }
+        mats[i] = d;
+    }
+    upload(s.materials, mats, st);
+
+    // emitters: triangles in mesh order, FP64 area CDF per emitter, FP64 selection CDF
+    const int nl = int(h.lights.size());
+    std::vector<float> ltris;
+    std::vector<double> areas;
+    std::vector<uint32_t> offsets{0};
+    std::vector<wrd::DevLight> lights(std::max(nl, 1));
+    for (int li = 0; li < nl; ++li) {
+        const wr::Mesh &m = h.meshes[h.lights[li].mesh];
+        lights[li].tri_offset = uint32_t(areas.size());
+        lights[li].tri_count = m.num_triangles();
+        for (int k = 0; k < 3; ++k) lights[li].intensity[k] = h.lights[li].intensity[k];
+        for (uint32_t t = 0; t < m.num_triangles(); ++t) {
+            double p[3][3];
+            for (int c = 0; c < 3; ++c) {
+                for (int k = 0; k < 3; ++k) {
+                    p[c][k] = m.positions[3 * size_t(m.indices[3 * t + c]) + k];
+                    ltris.push_back(float(p[c][k]));
+                }
+                ltris.push_back(0.f);
+            }
+            const double e1[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+            const double e2[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+            const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+            areas.push_back(std::sqrt(cx * cx + cy * cy + cz * cz) / 2.0);
+        }
+        offsets.push_back(uint32_t(areas.size()));
+    }
+    // selection weights: emitters then the environment
+    std::vector<double> sel;
+    for (int li = 0; li < nl; ++li) {
+        const float *I = h.lights[li].intensity;
+        sel.push_back(std::sqrt(double(I[0]) * I[0] + double(I[1]) * I[1] + double(I[2]) * I[2]));
+    }
+    if (h.has_env) sel.push_back(1.23);
+    const int nsel = int(sel.size());
+    std::vector<double> tri_sums(std::max(nl, 1), 0.0);
+    std::vector<float> sel_pdf(std::max(nsel, 1), 0.f);
+    {
+        DevBuf w, off, sums;
+        upload(w, areas, st);
+        upload(off, offsets, st);
+        s.light_tri_cdf.alloc(std::max<size_t>(areas.size(), 1) * 4);
+        s.light_tri_pdf.alloc(std::max<size_t>(areas.size(), 1) * 4);
+        sums.alloc(std::max(nl, 1) * 8);
+        wrk::launch_cdf_build(w.as<double>(), off.as<uint32_t>(), uint32_t(nl), s.light_tri_cdf.as<float>(),
+                              s.light_tri_pdf.as<float>(), sums.as<double>(), st);
+        WR_CUDA(cudaGetLastError());
+        if (nl) WR_CUDA(cudaMemcpyAsync(tri_sums.data(), sums.p, nl * 8, cudaMemcpyDeviceToHost, st));
+        DevBuf w2, off2;
+        upload(w2, sel, st);
+        std::vector<uint32_t> o2{0, uint32_t(nsel)};
+        upload(off2, o2, st);
+        s.light_cdf.alloc(std::max(nsel, 1) * 4);
+        s.light_pdf.alloc(std::max(nsel, 1) * 4);
+        wrk::launch_cdf_build(w2.as<double>(), off2.as<uint32_t>(), nsel ? 1u : 0u, s.light_cdf.as<float>(),
+                              s.light_pdf.as<float>(), nullptr, st);
+        WR_CUDA(cudaGetLastError());
+        if (nsel) WR_CUDA(cudaMemcpyAsync(sel_pdf.data(), s.light_pdf.p, nsel * 4, cudaMemcpyDeviceToHost, st));
+        WR_CUDA(cudaStreamSynchronize(st));
+    }
+    for (int li = 0; li < nl; ++li) {
+        lights[li].inv_area = float(1.0 / tri_sums[li]);
+        lights[li].select_pdf = sel_pdf[li];
+    }
+    upload(s.lights, lights, st);
+    if (ltris.empty()) ltris.assign(12, 0.f);
+    upload(s.light_tris, ltris, st);
+
+    wrd::DevScene &d = s.dev;
+    d.nodes = s.nodes.as<float4>();
+    d.tris = s.tris.as<float4>();
+    d.tri_mat = s.tri_mat.as<uint32_t>();
+    d.materials = s.materials.as<wrd::DevMaterial>();
+    d.lights = s.lights.as<wrd::DevLight>();
+    d.light_tris = s.light_tris.as<float4>();
+    d.light_tri_cdf = s.light_tri_cdf.as<float>();
+    d.light_cdf = s.light_cdf.as<float>();
+    d.num_lights = nl;
+    d.num_select = nsel;
+    d.has_env = h.has_env ? 1 : 0;
+    d.env_select_pdf = h.has_env ? sel_pdf[nsel - 1] : 0.f;
+
+    if (h.has_env) {
+        const int W = h.env.width, H = h.env.height;
+        const size_t N = size_t(W) * H;
+        std::vector<float> tex(N * 4);
+        for (size_t i = 0; i < N; ++i) {
+            for (int k = 0; k < 3; ++k) tex[4 * i + k] = h.env.rgb[3 * i + k];
+            tex[4 * i + 3] = 0.f;
+        }
+        upload(s.env_texels, tex, st);
+        DevBuf wts, off, rowsum, off2;
+        wts.alloc(N * 8);
+        wrk::launch_env_weights(s.env_texels.as<float4>(), W, H, wts.as<double>(), st);
+        std::vector<uint32_t> offs(H + 1);
+        for (int y = 0; y <= H; ++y) offs[y] = uint32_t(size_t(y) * W);
+        upload(off, offs, st);
+        s.env_col_cdf.alloc(N * 4);
+        s.env_col_pdf.alloc(N * 4);
+        rowsum.alloc(size_t(H) * 8);
+        wrk::launch_cdf_build(wts.as<double>(), off.as<uint32_t>(), uint32_t(H), s.env_col_cdf.as<float>(),
+                              s.env_col_pdf.as<float>(), rowsum.as<double>(), st);
+        std::vector<uint32_t> o2{0, uint32_t(H)};
+        upload(off2, o2, st);
+        s.env_row_cdf.alloc(size_t(H) * 4);
+        s.env_row_pdf.alloc(size_t(H) * 4);
+        DevBuf total;
+        total.alloc(8);
+        wrk::launch_cdf_build(rowsum.as<double>(), off2.as<uint32_t>(), 1u, s.env_row_cdf.as<float>(),
+                              s.env_row_pdf.as<float>(), total.as<double>(), st);
+        double tot = 0.0;
+        WR_CUDA(cudaMemcpyAsync(&tot, total.p, 8, cudaMemcpyDeviceToHost, st));
+        WR_CUDA(cudaStreamSynchronize(st));
+        s.env_pixel_pdf.alloc(N * 4);
+        wrk::launch_scale_pdf(wts.as<double>(), tot, s.env_pixel_pdf.as<float>(), N, st);
+        WR_CUDA(cudaGetLastError());
+        WR_CUDA(cudaStreamSynchronize(st));
+        d.env_w = W;
+        d.env_h = H;
+        d.env_texels = s.env_texels.as<float4>();
+        d.env_pixel_pdf = s.env_pixel_pdf.as<float>();
+        d.env_row_cdf = s.env_row_cdf.as<float>();
+        d.env_row_pdf = s.env_row_pdf.as<float>();
+        d.env_col_cdf = s.env_col_cdf.as<float>();
+        d.env_col_pdf = s.env_col_pdf.as<float>();
+    }
+    WR_CUDA(cudaStreamSynchronize(st));
+    s.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// camera constants of ThinlensCamera (src/camera/thinlens.h:40-61, src/common/camera.h:9-18), in FP64
+wrd::DevCamera make_camera(const wr::Camera &c) {
+    auto sub = [](const double *a, const double *b, double *o) { for (int k = 0; k < 3; ++k) o[k] = a[k] - b[k]; };
+    auto crs = [](const double *a, const double *b, double *o) {
+        o[0] = a[1] * b[2] - a[2] * b[1]; o[1] = a[2] * b[0] - a[0] * b[2]; o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    auto nrm = [](double *a) { double l = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); for (int k = 0; k < 3; ++k) a[k] /= l; };
+    double z[3], x[3], y[3];
+    sub(c.lookat, c.pos, z); nrm(z);
+    crs(c.up, z, x); nrm(x);
+    crs(z, x, y); nrm(y);
+    const double fov = c.fovy_deg * 3.141592653589793238462643 / 180.0;
+    const double dist = double(c.height) * 0.5 / std::tan(fov * 0.5);
+    wrd::DevCamera d{};
+    for (int k = 0; k < 3; ++k) {
+        d.origin[k] = float(c.pos[k]); d.fx[k] = float(x[k]); d.fy[k] = float(y[k]); d.fz[k] = float(z[k]);
+    }
+    d.dist = float(dist);
+    d.per_film = float(dist * dist);
+    d.per_pixel = float(dist * dist / (double(c.width) * double(c.height)));
+    d.focal = float(c.focal);
+    d.aperture = float(c.aperture);
+    d.inv_lens_area = c.aperture > 0 ? float(1.0 / (3.141592653589793 * c.aperture * c.aperture)) : 1.f;
+    d.width = c.width;
+    d.height = c.height;
+    return d;
+}
+
+void ensure_wave(wr_scene &s, uint32_t capacity, size_t npix) {
+    if (s.w_capacity != capacity) {
+        for (int p = 0; p < 2; ++p) {
+            s.w_o[p].alloc(size_t(capacity) * 16);
+            s.w_d[p].alloc(size_t(capacity) * 16);
+            s.w_thr[p].alloc(size_t(capacity) * 16);
+            s.w_meta[p].alloc(size_t(capacity) * 4);
+        }
+        s.w_hit.alloc(size_t(capacity) * 16);
+        s.w_sho.alloc(size_t(capacity) * 2 * 16);
+        s.w_shd.alloc(size_t(capacity) * 2 * 16);
+        s.w_shc.alloc(size_t(capacity) * 2 * 16);
+        s.w_ctr.alloc(wrd::CTR_COUNT * 4);
+        s.w_sample.alloc(8);
+        s.w_capacity = capacity;
+    }
+    if (s.w_npix != npix) {
+        s.w_film.alloc(npix * 6 * 8);
+        s.w_out.alloc(npix * 3 * 8);
+        s.w_npix = npix;
+    }
+}
+
+void render(wr_scene &s, const wr_render_desc *desc_in, double *out, bool out_on_host) {
+    wr_render_desc desc{};
+    if (desc_in) desc = *desc_in;
+    const wr::Scene &h = s.host;
+    if (!h.has_camera) throw Error(WR_ERR_INVALID_ARGUMENT, "scene has no camera");
+    wr::RenderEntry re;
+    if (desc.render_index < 0) throw Error(WR_ERR_INVALID_ARGUMENT, "render_index must be >= 0");
+    if (size_t(desc.render_index) < h.renders.size()) re = h.renders[desc.render_index];
+    const int spp = desc.num_spp > 0 ? desc.num_spp : re.num_spp;
+    const int nverts = desc.num_path_vertices > 0 ? desc.num_path_vertices : re.num_path_vertices;
+    if (spp <= 0) throw Error(WR_ERR_INVALID_ARGUMENT, "num_spp must be positive");
+    const wr::Camera &cam = h.camera;
+    const size_t npix = size_t(cam.width) * cam.height;
+    if (npix >= (1ull << 31)) throw Error(WR_ERR_UNSUPPORTED, "film too large");
+    int sms = 148;
+    WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
+    uint32_t capacity = desc.queue_capacity > 0 ? uint32_t(desc.queue_capacity) : (1u << 21);
+    const unsigned long long total = (unsigned long long)npix * unsigned(spp);
+    capacity = uint32_t(std::min<unsigned long long>(capacity, std::max<unsigned long long>(total, 1024ull)));
+    ensure_wave(s, capacity, npix);
+
+    wrk::WaveBuffers b{};
+    for (int p = 0; p < 2; ++p) {
+        b.o[p] = s.w_o[p].as<float4>();
+        b.d[p] = s.w_d[p].as<float4>();
+        b.thr[p] = s.w_thr[p].as<float4>();
+        b.meta[p] = s.w_meta[p].as<uint32_t>();
+    }
+    b.hit = s.w_hit.as<float4>();
+    b.sh_o = s.w_sho.as<float4>();
+    b.sh_d = s.w_shd.as<float4>();
+    b.sh_c = s.w_shc.as<float4>();
+    b.film = s.w_film.as<double>();
+    b.ctr = s.w_ctr.as<uint32_t>();
+    b.sample_next = s.w_sample.as<unsigned long long>();
+    b.capacity = capacity;
+    b.shadow_capacity = 2 * capacity;
+
+    wrk::RenderLaunch r{};
+    r.cam = make_camera(cam);
+    r.spp = spp;
+    r.nverts = nverts;
+    r.seed = desc.seed;
+    r.total_samples = total;
+    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0));
+    r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * std::max(1, wrk::occupancy_blocks(1));
+
+    cudaStream_t st = s.stream;
+    const int profile = desc.profile;
+    s.w_prof.alloc(16 * 8);
+    r.prof = profile >= 2 ? s.w_prof.as<unsigned long long>() : nullptr;
+    s.stats = wr_render_stats{};
+    WR_CUDA(cudaMemsetAsync(b.film, 0, npix * 6 * 8, st));
+    WR_CUDA(cudaMemsetAsync(b.ctr, 0, wrd::CTR_COUNT * 4, st));
+    WR_CUDA(cudaMemsetAsync(b.sample_next, 0, 8, st));
+    WR_CUDA(cudaMemsetAsync(s.w_prof.p, 0, 16 * 8, st));
+    WR_CUDA(cudaEventRecord(s.ev0, st));
+    unsigned long long iterations = 0, launches = 0;
+    if (nverts > 1) {
+        // upper bound on iterations: every sample needs at most nverts extensions
+        const unsigned long long waves = (total + capacity - 1) / capacity;
+        const unsigned long long limit = (waves + 2) * (unsigned long long)(nverts + 2) + 64;
+        if (profile) {
+            // one kernel at a time, bracketed by events, to attribute device time per kernel
+            if (s.kev.empty()) {
+                s.kev.resize(2);
+                for (auto &e : s.kev) WR_CUDA(cudaEventCreate(&e));
+            }
+            auto timed = [&](int which, int parity) {
+                WR_CUDA(cudaEventRecord(s.kev[0], st));
+                wrk::launch_kernel(which, s.dev, b, r, parity, st);
+                WR_CUDA(cudaGetLastError());
+                WR_CUDA(cudaEventRecord(s.kev[1], st));
+                WR_CUDA(cudaEventSynchronize(s.kev[1]));
+                float ms = 0.f;
+                WR_CUDA(cudaEventElapsedTime(&ms, s.kev[0], s.kev[1]));
+                s.stats.kernel_ms[which] += ms;
+                s.stats.kernel_count[which] += 1;
+                launches += 1;
+            };
+            timed(wrk::KERNEL_RAYGEN, 1);
+            timed(wrk::KERNEL_SHADOW, 1);
+            timed(wrk::KERNEL_ADVANCE, 1);
+            bool done = false;
+            int parity = 0;
+            while (!done) {
+                for (int k : {wrk::KERNEL_EXTEND, wrk::KERNEL_SHADE, wrk::KERNEL_RAYGEN, wrk::KERNEL_SHADOW,
+                              wrk::KERNEL_ADVANCE})
+                    timed(k, parity);
+                parity ^= 1;
+                ++iterations;
+                WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
+                WR_CUDA(cudaStreamSynchronize(st));
+                done = s.pinned[wrd::CTR_DONE] != 0;
+                if (!done && iterations > limit) throw Error(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
+            }
+        } else {
+            wrk::launch_prime(s.dev, b, r, st);
+            WR_CUDA(cudaGetLastError());
+            launches += 3;
+            cudaGraphExec_t exec = nullptr;
+            if (desc.use_graph) {
+                cudaGraph_t g;
+                WR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                wrk::launch_iteration(s.dev, b, r, 0, st);
+                wrk::launch_iteration(s.dev, b, r, 1, st);
+                WR_CUDA(cudaStreamEndCapture(st, &g));
+                WR_CUDA(cudaGraphInstantiate(&exec, g, 0));
+                cudaGraphDestroy(g);
+            }
+            bool done = false;
+            while (!done) {
+                if (exec) {
+                    WR_CUDA(cudaGraphLaunch(exec, st));
+                } else {
+                    wrk::launch_iteration(s.dev, b, r, 0, st);
+                    wrk::launch_iteration(s.dev, b, r, 1, st);
+                }
+                iterations += 2;
+                launches += 10;
+                WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
+                WR_CUDA(cudaStreamSynchronize(st));
+                done = s.pinned[wrd::CTR_DONE] != 0;
+                if (!done && iterations > limit) {
+                    if (exec) cudaGraphExecDestroy(exec);
+                    throw Error(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
+                }
+            }
+            if (exec) WR_CUDA(cudaGraphExecDestroy(exec));
+        }
+        if (s.pinned[wrd::CTR_OVERFLOW]) throw Error(WR_ERR_CUDA, "shadow queue overflow");
+        s.stats.max_shadow_queue = s.pinned[wrd::CTR_SHADOW_MAX];
+    }
+    double *dst = out_on_host ? s.w_out.as<double>() : out;
+    if (profile) WR_CUDA(cudaEventRecord(s.kev[0], st));
+    wrk::launch_resolve(b.film, dst, uint32_t(npix), spp, st);
+    WR_CUDA(cudaGetLastError());
+    launches += 1;
+    WR_CUDA(cudaEventRecord(s.ev1, st));
+    if (out_on_host) WR_CUDA(cudaMemcpyAsync(out, dst, npix * 3 * 8, cudaMemcpyDeviceToHost, st));
+    WR_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    WR_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
+    if (profile) {
+        float rms = 0.f;
+        WR_CUDA(cudaEventElapsedTime(&rms, s.kev[0], s.ev1));
+        s.stats.kernel_ms[wrk::KERNEL_RESOLVE] += rms;
+        s.stats.kernel_count[wrk::KERNEL_RESOLVE] += 1;
+        s.stats.kernel_items[wrk::KERNEL_RESOLVE] += npix;
+        unsigned long long prof[16];
+        WR_CUDA(cudaMemcpy(prof, s.w_prof.p, sizeof(prof), cudaMemcpyDeviceToHost));
+        if (profile >= 2) {
+            for (int k = 0; k < 4; ++k) s.stats.kernel_items[k] = prof[k];
+            s.stats.extend_node_visits = prof[6];
+            s.stats.extend_tri_tests = prof[7];
+            s.stats.shadow_node_visits = prof[8];
+            s.stats.shadow_tri_tests = prof[9];
+        }
+    }
+    s.stats.render_ms = ms;
+    s.stats.paths = total;
+    s.stats.iterations = iterations;
+    s.stats.queue_capacity = capacity;
+    s.stats.grid_trace = r.grid_trace;
+    s.stats.grid_shade = r.grid_shade;
+    s.stats.kernel_launches = launches;
+}
+
+wrd::DevScene scene_for_queries(wr_scene &s) { return s.dev; }
+
+void trace_batch(wr_scene &s, const float *rays, int n, int any_hit, std::vector<float> &out, unsigned long long *nv,
+                 unsigned long long *nt) {
+    if (n < 0 || (n > 0 && !rays)) throw Error(WR_ERR_INVALID_ARGUMENT, "bad ray batch");
+    out.assign(size_t(n) * 8, 0.f);
+    if (n == 0) return;
+    DevBuf dr, dout, dvis;
+    dr.alloc(size_t(n) * 32);
+    dout.alloc(size_t(n) * 32);
+    dvis.alloc(8);
+    cudaStream_t st = s.stream;
+    WR_CUDA(cudaMemcpyAsync(dr.p, rays, size_t(n) * 32, cudaMemcpyHostToDevice, st));
+    WR_CUDA(cudaMemsetAsync(dvis.p, 0, 8, st));
+    int sms = 148;
+    WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
+    const int grid = std::max(1, std::min(sms * 8, (n + wrd::kTraceBlock - 1) / wrd::kTraceBlock));
+    wrk::launch_trace_batch(scene_for_queries(s), dr.as<float4>(), uint32_t(n), any_hit, dout.as<float4>(),
+                            (nv || nt) ? dvis.as<uint32_t>() : nullptr, grid, st);
+    WR_CUDA(cudaGetLastError());
+    WR_CUDA(cudaMemcpyAsync(out.data(), dout.p, size_t(n) * 32, cudaMemcpyDeviceToHost, st));
+    uint32_t vis[2] = {0, 0};
+    WR_CUDA(cudaMemcpyAsync(vis, dvis.p, 8, cudaMemcpyDeviceToHost, st));
+    WR_CUDA(cudaStreamSynchronize(st));
+    if (nv) *nv = vis[0];
+    if (nt) *nt = vis[1];
+}
+
+std::unique_ptr<wr_scene> create(wr::Scene &&host) {
+    std::unique_ptr<wr_scene> s(new wr_scene());
+    s->host = std::move(host);
+    build_device_scene(*s);
+    return s;
+}
+
+void run_scene(wr_scene &s) {
+    const wr::Scene &h = s.host;
+    for (size_t i = 0; i < h.renders.size(); ++i) {
+        const wr::RenderEntry &re = h.renders[i];
+        if (re.integrator != "nextevent_path_tracer")
+            throw Error(WR_ERR_UNSUPPORTED, "integrator '" + re.integrator + "' is not provided by this build");
+        wr_render_desc d{};
+        d.render_index = int(i);
+        d.use_graph = 1;
+        std::vector<double> img(size_t(h.camera.width) * h.camera.height * 3);
+        render(s, &d, img.data(), true);
+        if (!re.output.empty()) {
+            const std::string out = re.output[0] == '/' ? re.output : h.base_dir + "/" + re.output;
+            wr::write_pfm(out, img.data(), h.camera.width, h.camera.height);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *wr_last_error(void) { return g_last_error.c_str(); }
+
+int wr_set_device(int device) {
+    const cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+        return WR_ERR_CUDA;
+    }
+    return WR_OK;
+}
+int wr_abi_version(void) { return WR_ABI_VERSION; }
+
+int wr_scene_create(const char *path, wr_scene **out) {
+    if (!path || !out) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    try {
+        *out = create(wr::load_simple2_file(path)).release();
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return WR_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int wr_scene_create_from_json(const char *json_text, const char *base_dir, wr_scene **out) {
+    if (!json_text || !out) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    try {
+        *out = create(wr::load_simple2_text(json_text, base_dir ? base_dir : ".")).release();
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return WR_ERR_INVALID_ARGUMENT;
+    }
+}
+
+void wr_scene_destroy(wr_scene *s) { delete s; }
+
+int wr_scene_inspect(const char *path, wr_scene_info *info) {
+    if (!path || !info) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        const auto t0 = std::chrono::steady_clock::now();
+        wr::Scene h = wr::load_simple2_file(path);
+        std::vector<float> verts;
+        verts.reserve(size_t(h.num_triangles()) * 9);
+        for (const wr::Mesh &m : h.meshes)
+            for (uint32_t i : m.indices)
+                for (int k = 0; k < 3; ++k) verts.push_back(m.positions[3 * size_t(i) + k]);
+        wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, 4, 0);
+        memset(info, 0, sizeof(*info));
+        info->width = h.has_camera ? h.camera.width : 0;
+        info->height = h.has_camera ? h.camera.height : 0;
+        info->num_spp = h.renders.empty() ? 16 : h.renders[0].num_spp;
+        info->num_path_vertices = h.renders.empty() ? 10 : h.renders[0].num_path_vertices;
+        info->num_triangles = h.num_triangles();
+        info->num_meshes = int(h.meshes.size());
+        info->num_lights = int(h.lights.size());
+        info->has_envmap = h.has_env ? 1 : 0;
+        info->bvh_nodes = int(bvh.nodes.size() / 16);
+        info->bvh_depth = bvh.depth;
+        info->bvh_sah_cost = bvh.sah_cost;
+        info->num_renders = int(h.renders.size());
+        info->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (bvh.depth > wrd::kMaxStack) throw Error(WR_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return WR_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int wr_scene_get_info(const wr_scene *s, wr_scene_info *info) {
+    if (!s || !info) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    memset(info, 0, sizeof(*info));
+    const wr::Scene &h = s->host;
+    info->width = h.has_camera ? h.camera.width : 0;
+    info->height = h.has_camera ? h.camera.height : 0;
+    info->num_spp = h.renders.empty() ? 16 : h.renders[0].num_spp;
+    info->num_path_vertices = h.renders.empty() ? 10 : h.renders[0].num_path_vertices;
+    info->num_triangles = h.num_triangles();
+    info->num_meshes = int(h.meshes.size());
+    info->num_lights = int(h.lights.size());
+    info->has_envmap = h.has_env ? 1 : 0;
+    info->bvh_nodes = s->bvh_nodes;
+    info->bvh_depth = s->bvh_depth;
+    info->bvh_sah_cost = s->sah_cost;
+    info->build_ms = s->build_ms;
+    info->num_renders = int(h.renders.size());
+    return WR_OK;
+}
+
+int wr_scene_set_camera_json(wr_scene *s, const char *camera_json) {
+    if (!s || !camera_json) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        s->host.camera = wr::parse_camera_json(camera_json);
+        s->host.has_camera = true;
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_render(wr_scene *s, const wr_render_desc *desc, double *out_rgb) {
+    if (!s || !out_rgb) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        render(*s, desc, out_rgb, true);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_render_device(wr_scene *s, const wr_render_desc *desc, double *out_rgb_device) {
+    if (!s || !out_rgb_device) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        render(*s, desc, out_rgb_device, false);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_get_render_stats(const wr_scene *s, wr_render_stats *st) {
+    if (!s || !st) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    *st = s->stats;
+    return WR_OK;
+}
+
+int wr_trace_closest(wr_scene *s, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *uv) {
+    if (!s || (n > 0 && (!geom_id || !prim_id || !t))) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        std::vector<float> out;
+        trace_batch(*s, rays, n, 0, out, nullptr, nullptr);
+        for (int i = 0; i < n; ++i) {
+            const float *o = &out[8 * size_t(i)];
+            uint32_t g, p;
+            memcpy(&g, &o[0], 4);
+            memcpy(&p, &o[1], 4);
+            geom_id[i] = g == wrd::MISS ? -1 : int(g);
+            prim_id[i] = p == wrd::MISS ? -1 : int(p);
+            t[i] = o[2];
+            if (uv) { uv[2 * i] = o[4]; uv[2 * i + 1] = o[5]; }
+        }
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_trace_occluded(wr_scene *s, const float *rays, int n, int *occluded) {
+    if (!s || (n > 0 && !occluded)) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        std::vector<float> out;
+        trace_batch(*s, rays, n, 1, out, nullptr, nullptr);
+        for (int i = 0; i < n; ++i) {
+            uint32_t g;
+            memcpy(&g, &out[8 * size_t(i)], 4);
+            occluded[i] = g == wrd::MISS ? 0 : 1;
+        }
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_trace_stats(wr_scene *s, const float *rays, int n, int any_hit, unsigned long long *node_visits,
+                   unsigned long long *tri_tests) {
+    if (!s || !node_visits || !tri_tests) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        std::vector<float> out;
+        trace_batch(*s, rays, n, any_hit, out, node_visits, tri_tests);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_write_pfm(const char *path, const double *rgb, int width, int height) {
+    if (!path || !rgb || width <= 0 || height <= 0) { g_last_error = "bad argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        wr::write_pfm(path, rgb, width, height);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_run_simple2(const char *path) {
+    wr_scene *s = nullptr;
+    int rc = wr_scene_create(path, &s);
+    if (rc != WR_OK) return rc;
+    try {
+        run_scene(*s);
+        wr_scene_destroy(s);
+        return WR_OK;
+    } catch (const Error &e) {
+        wr_scene_destroy(s);
+        return fail(e);
+    }
+}
+
+int wr_run_jsimple2(const char *json_text) {
+    wr_scene *s = nullptr;
+    int rc = wr_scene_create_from_json(json_text, ".", &s);
+    if (rc != WR_OK) return rc;
+    try {
+        run_scene(*s);
+        wr_scene_destroy(s);
+        return WR_OK;
+    } catch (const Error &e) {
+        wr_scene_destroy(s);
+        return fail(e);
+    }
+}
+
+}  // extern "C"

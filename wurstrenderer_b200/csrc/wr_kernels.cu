@@ -1,0 +1,804 @@
+// sm_100a kernels of the wavefront NEE+MIS path tracer.
+//
+// The reference integrator (src/renderer/pathnextevent.h:41-191 driving
+// src/pathsampler/generalsubpathsampler.h:13-323) is recursive per pixel
+// sample. Here every sample is a slot in a wavefront; one iteration of the
+// bounce loop is five persistent, grid-stride kernels:
+//   extend  closest hit for every live path                       (Scene::intersect)
+//   shade   emitter hit (strategy B) or NEE at a surface (strategy A, emits a
+//           shadow ray), then BSDF sampling; surviving paths are compacted into
+//           the next wavefront by warp ballot/popc + one atomic per warp
+//   raygen  fills the freed slots with new camera samples: light vertex,
+//           camera vertex, light->camera connection (strategy C, emits a shadow
+//           ray into the splat film), primary ray
+//   shadow  any-hit test of every queued shadow ray; unoccluded contributions
+//           are added to the FP64 film with FP64 atomics
+//   advance one thread: queue bookkeeping for the next iteration
+// Counters live on the device, so an iteration needs no host round trip and a
+// pair of iterations is captured once into a CUDA graph by the host.
+// Arithmetic is FP32; FP64 is used for the film and for building the light /
+// environment CDF tables (the prefix sums at the end of this file).
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "wr_device.cuh"
+#include "wr_kernels.h"
+#include "wr_trace.cuh"
+
+namespace wrd {
+
+// ------------------------------------------------------------------ BSDFs ----
+// TwoSided(inner) of src/bsdf/twosided.h:25-63 with inner one of Lambert
+// (lambertdiffuse.h:16-51), Oren-Nayar (orennayar.h:14-83), modified Phong
+// (phong.h:22-93) or Mixed(diffuse, Phong) (mixed.h:20-60). Directions are in
+// the local frame with y = normal.
+
+__device__ __forceinline__ f3 lambert_or_on_eval(const DevMaterial &m, f3 in, f3 out) {
+    if (in.y <= 0.f || out.y <= 0.f) return mk(0.f, 0.f, 0.f);
+    const f3 kd = mk(m.kd[0], m.kd[1], m.kd[2]);
+    if (!(m.flags & MAT_OREN_NAYAR)) return kd * kInvPi;
+    const float sinI = sqrtf(fminf(fmaxf(1.f - in.y * in.y, 0.f), 1.f));
+    const float sinO = sqrtf(fminf(fmaxf(1.f - out.y * out.y, 0.f), 1.f));
+    float maxCos = 0.f, sinAlpha = 0.f, tanBeta = 0.f;
+    if (sinI > 1e-4f && sinO > 1e-4f) {
+        const float cI = in.x / sinI, sI = in.z / sinI, cO = out.x / sinO, sO = out.z / sinO;
+        maxCos = fmaxf(0.f, cI * cO + sI * sO);
+        if (fabsf(in.y) > fabsf(out.y)) { sinAlpha = sinO; tanBeta = sinI / in.y; }
+        else { sinAlpha = sinI; tanBeta = sinO / out.y; }
+    }
+    return kd * (kInvPi * (m.on_a + m.on_b * maxCos * sinAlpha * tanBeta));
+}
+
+__device__ __forceinline__ float diffuse_pdf(f3 in, f3 out) {
+    if (in.y <= 0.f || out.y <= 0.f) return 0.f;
+    return out.y * kInvPi;
+}
+
+__device__ __forceinline__ f3 phong_eval(const DevMaterial &m, f3 in, f3 out) {
+    if (in.y <= 0.f || out.y <= 0.f) return mk(0.f, 0.f, 0.f);
+    const f3 refl = mk(-in.x, in.y, -in.z);   // Local3::Reflect(-in)
+    const float cr = dot(refl, out);
+    if (cr <= 0.f) return mk(0.f, 0.f, 0.f);
+    const float n = m.exponent;
+    return mk(m.ks[0], m.ks[1], m.ks[2]) * ((n + 2.f) * __powf(cr, n) * (kInvPi * 0.5f));
+}
+
+__device__ __forceinline__ float phong_pdf(const DevMaterial &m, f3 in, f3 out) {
+    if (in.y <= 0.f && out.y <= 0.f) return 0.f;
+    const f3 refl = mk(-in.x, in.y, -in.z);
+    const float cr = dot(refl, out);
+    if (cr <= 0.f) return 0.f;
+    const float n = m.exponent;
+    return (n + 1.f) * __powf(cr, n) * (kInvPi * 0.5f);
+}
+
+__device__ __forceinline__ f3 inner_eval(const DevMaterial &m, f3 in, f3 out) {
+    f3 r = mk(0.f, 0.f, 0.f);
+    if (m.flags & MAT_DIFFUSE) r = lambert_or_on_eval(m, in, out);
+    if (m.flags & MAT_GLOSSY) r = r + phong_eval(m, in, out);
+    return r;
+}
+
+__device__ __forceinline__ float inner_pdf(const DevMaterial &m, f3 in, f3 out) {
+    const int both = (m.flags & MAT_DIFFUSE) && (m.flags & MAT_GLOSSY);
+    float p = 0.f;
+    if (m.flags & MAT_DIFFUSE) p = diffuse_pdf(in, out);
+    if (m.flags & MAT_GLOSSY) p += phong_pdf(m, in, out);
+    return both ? p * 0.5f : p;
+}
+
+__device__ __forceinline__ f3 cosine_hemisphere(float s0, float s1) {
+    float sn, cs;
+    __sincosf(2.f * kPi * s1, &sn, &cs);
+    const float sinPhi = sqrtf(fmaxf(1.f - s0, 0.f));
+    return mk(cs * sinPhi, sqrtf(s0), sn * sinPhi);
+}
+
+// lobe about the mirror direction (phong.h:58-72)
+__device__ __forceinline__ f3 phong_direction(float n, f3 in, float s0, float s1) {
+    const f3 refl = mk(-in.x, in.y, -in.z);
+    const float cosT = __powf(s0, 1.f / (n + 1.f));
+    const float sinT = sqrtf(fmaxf(1.f - cosT * cosT, 0.f));
+    float sn, cs;
+    __sincosf(2.f * kPi * s1, &sn, &cs);
+    const Frame rf(refl);
+    return rf.to_world(mk(sinT * cs, cosT, sinT * sn));
+}
+
+// Bsdf::sampleBsdfCosByPdf on the inner BSDF (front side): returns bsdf*cos/pdf
+// (zero terminates the path) and writes the direction and its pdf.
+__device__ __forceinline__ f3 inner_sample(const DevMaterial &m, f3 in, float s0, float s1, f3 &out, float &pdf) {
+    const bool dif = m.flags & MAT_DIFFUSE, gl = m.flags & MAT_GLOSSY;
+    pdf = 0.f;
+    if (dif && gl) {
+        // MixedBsdf: pick a component with s0, evaluate the mixture at the result
+        const int k = s0 < 0.5f ? 0 : 1;
+        const float r0 = fminf(s0 * 2.f - float(k), 0.99999994f);
+        out = mk(0.f, 0.f, 0.f);
+        if (k == 0) {
+            if ((m.flags & MAT_OREN_NAYAR) ? in.y >= 0.f : in.y > 0.f) out = cosine_hemisphere(r0, s1);
+        } else {
+            if (in.y > 0.f) out = phong_direction(m.exponent, in, r0, s1);
+        }
+        const f3 f = inner_eval(m, in, out);
+        pdf = inner_pdf(m, in, out);
+        if (pdf == 0.f) return mk(0.f, 0.f, 0.f);
+        return f * (out.y / pdf);
+    }
+    if (dif) {
+        if (m.flags & MAT_OREN_NAYAR) {
+            if (in.y < 0.f) return mk(0.f, 0.f, 0.f);
+            out = cosine_hemisphere(s0, s1);
+            pdf = out.y * kInvPi;
+            return lambert_or_on_eval(m, out, in) * kPi;
+        }
+        if (in.y <= 0.f) return mk(0.f, 0.f, 0.f);
+        out = cosine_hemisphere(s0, s1);
+        pdf = fmaxf(out.y, 0.f) * kInvPi;
+        if (out.y <= 0.f) return mk(0.f, 0.f, 0.f);
+        return mk(m.kd[0], m.kd[1], m.kd[2]);
+    }
+    // Phong only
+    if (in.y <= 0.f) return mk(0.f, 0.f, 0.f);
+    const float n = m.exponent;
+    const f3 refl = mk(-in.x, in.y, -in.z);
+    out = phong_direction(n, in, s0, s1);
+    const float cr = dot(out, refl);
+    pdf = (n + 1.f) * 0.5f * kInvPi * __powf(fmaxf(cr, 0.f), n);
+    if (refl.y <= 0.f || out.y <= 0.f || cr <= 0.f) return mk(0.f, 0.f, 0.f);
+    return mk(m.ks[0], m.ks[1], m.ks[2]) * ((n + 2.f) / (n + 1.f) * out.y);
+}
+
+__device__ __forceinline__ f3 flip_y(f3 v) { return mk(v.x, -v.y, v.z); }
+
+__device__ __forceinline__ f3 bsdf_eval(const DevMaterial &m, f3 in, f3 out) {
+    if (in.y > 0.f && out.y > 0.f) return inner_eval(m, in, out);
+    if (in.y <= 0.f && out.y <= 0.f) return inner_eval(m, flip_y(in), flip_y(out));
+    return mk(0.f, 0.f, 0.f);
+}
+
+__device__ __forceinline__ float bsdf_pdf(const DevMaterial &m, f3 in, f3 out) {
+    if (in.y > 0.f && out.y > 0.f) return inner_pdf(m, in, out);
+    if (in.y <= 0.f && out.y <= 0.f) return inner_pdf(m, flip_y(in), flip_y(out));
+    return 0.f;
+}
+
+__device__ __forceinline__ f3 bsdf_sample(const DevMaterial &m, f3 in, float s0, float s1, f3 &out, float &pdf) {
+    if (in.y > 0.f) return inner_sample(m, in, s0, s1, out, pdf);
+    f3 o;
+    const f3 w = inner_sample(m, flip_y(in), s0, s1, o, pdf);
+    out = flip_y(o);
+    return w;
+}
+
+// ------------------------------------------------------------ environment ----
+// EnvmapLight + EquiRectRep (src/light/envmap.h:22-101,
+// src/sphericalrepresentation/equirectangular.h:66-123, mapping.h:91-96,302-323)
+__device__ __forceinline__ void panorama(f3 d, float &u, float &v) {
+    u = atan2f(-d.z, -d.x) * (kInvPi * 0.5f) + 0.5f;
+    v = acosf(fminf(fmaxf(d.y, -1.f), 1.f)) * kInvPi;
+}
+
+__device__ __forceinline__ f3 env_texel(const DevScene &s, int x, int y) {
+    x %= s.env_w;
+    if (x < 0) x += s.env_w;
+    y = min(max(y, 0), s.env_h - 1);
+    return xyz(__ldg(s.env_texels + size_t(y) * s.env_w + x));
+}
+
+__device__ __forceinline__ f3 env_eval(const DevScene &s, f3 d) {
+    float u, v;
+    panorama(d, u, v);
+    const float su = u * float(s.env_w) - 0.5f, sv = v * float(s.env_h) - 0.5f;
+    const float fx = floorf(su), fy = floorf(sv);
+    const int x = int(fx), y = int(fy);
+    const float dx1 = su - fx, dy1 = sv - fy, dx2 = 1.f - dx1, dy2 = 1.f - dy1;
+    return env_texel(s, x, y) * (dx2 * dy2) + env_texel(s, x, y + 1) * (dx2 * dy1) +
+           env_texel(s, x + 1, y) * (dx1 * dy2) + env_texel(s, x + 1, y + 1) * (dx1 * dy1);
+}
+
+// directional pdf (solid angle) of EquiRectRep::pdfA
+__device__ __forceinline__ float env_pdf(const DevScene &s, f3 d) {
+    float u, v;
+    panorama(d, u, v);
+    if (!(u >= 0.f && v >= 0.f)) return 0.f;   // non-finite direction
+    const int px = min(int(u * float(s.env_w)), s.env_w - 1), py = min(int(v * float(s.env_h)), s.env_h - 1);
+    const float sine = sqrtf(fminf(fmaxf(1.f - d.y * d.y, 0.f), 1.f));
+    if (sine <= 1e-12f) return 0.f;
+    return __ldg(s.env_pixel_pdf + size_t(py) * s.env_w + px) * float(s.env_w * s.env_h) / sine * (kInvPi * kInvPi * 0.5f);
+}
+
+// ------------------------------------------------------------ light vertex ----
+struct LightVtx {
+    f3 pos;       // area: point; environment: direction toward the environment
+    f3 n;
+    f3 contrib;   // Le0 / pdf of the light subpath (mPathContrib)
+    float pdfA;   // lPdfA
+    bool env;
+};
+
+// GeneralSubpathSampler::createLightSubpath with one vertex (generalsubpathsampler.h:185-268)
+__device__ __forceinline__ LightVtx sample_light(const DevScene &s, float u0, float u1) {
+    LightVtx l;
+    if (s.num_select == 0) {   // no emitter and no environment: nothing to connect to
+        l.env = false;
+        l.pos = mk(0.f, 0.f, 0.f);
+        l.n = mk(0.f, 1.f, 0.f);
+        l.contrib = mk(0.f, 0.f, 0.f);
+        l.pdfA = 0.f;
+        return l;
+    }
+    const int li = cdf_lower_bound(s.light_cdf, s.num_select, u0);
+    const float pl = li < s.num_lights ? __ldg(&s.lights[li].select_pdf) : s.env_select_pdf;
+    float r0 = cdf_remap(s.light_cdf, li, pl, u0);
+    if (li >= s.num_lights) {
+        // environment: pixel by the row / column tables, uniform within the pixel
+        const int row = cdf_lower_bound(s.env_row_cdf, s.env_h, r0);
+        const float rp = __ldg(s.env_row_pdf + row);
+        const float r1 = cdf_remap(s.env_row_cdf, row, rp, r0);
+        const float *ccdf = s.env_col_cdf + size_t(row) * s.env_w;
+        const int col = cdf_lower_bound(ccdf, s.env_w, r1);
+        const float cp = __ldg(s.env_col_pdf + size_t(row) * s.env_w + col);
+        const float r2 = cdf_remap(ccdf, col, cp, r1);
+        const float uu = (float(col) + r2) / float(s.env_w), vv = (float(row) + u1) / float(s.env_h);
+        float st, ct, sp, cp2;
+        sincosf(uu * 2.f * kPi, &st, &ct);
+        sincosf(vv * kPi, &sp, &cp2);
+        const f3 d = mk(ct * sp, cp2, st * sp);
+        const float sine = sqrtf(fminf(fmaxf(1.f - d.y * d.y, 0.f), 1.f));
+        const float pix = __ldg(s.env_pixel_pdf + size_t(row) * s.env_w + col);
+        const float pdfDir = sine <= 1e-12f ? 0.f : pix * float(s.env_w * s.env_h) / sine * (kInvPi * kInvPi * 0.5f);
+        l.env = true;
+        l.pos = d;
+        l.n = mk(0.f, 1.f, 0.f);
+        l.contrib = pdfDir > 0.f ? env_eval(s, d) * (1.f / (pdfDir * pl)) : mk(0.f, 0.f, 0.f);
+        l.pdfA = pl * pdfDir;
+        return l;
+    }
+    const DevLight &L = s.lights[li];
+    const float *tcdf = s.light_tri_cdf + L.tri_offset;
+    const int ti = cdf_lower_bound(tcdf, int(L.tri_count), r0);
+    const float tp = __ldg(tcdf + ti) - (ti == 0 ? 0.f : __ldg(tcdf + ti - 1));
+    const float r1 = cdf_remap(tcdf, ti, tp, r0);
+    const float4 *lt = s.light_tris + 3 * size_t(L.tri_offset + ti);
+    const f3 p0 = xyz(__ldg(lt)), p1 = xyz(__ldg(lt + 1)), p2 = xyz(__ldg(lt + 2));
+    const float sq = sqrtf(r1);
+    const float b1 = sq * (1.f - u1), b2 = u1 * sq;   // BarycentricFromSquare (mapping.h:21-27)
+    l.env = false;
+    l.pos = p0 * (1.f - b1 - b2) + p1 * b1 + p2 * b2;
+    l.n = normalize(cross(p1 - p0, p2 - p0));
+    l.contrib = mk(L.intensity[0], L.intensity[1], L.intensity[2]) * (kPi / (L.inv_area * pl));
+    l.pdfA = pl * L.inv_area;
+    return l;
+}
+
+// ----------------------------------------------------------------- kernels ----
+struct PathState {
+    float4 *o, *d, *thr;
+    uint32_t *meta;
+};
+
+struct ShadowQueue {
+    float4 *o, *d, *c;
+};
+
+struct WaveArgs {
+    PathState cur, nxt;
+    float4 *hit;
+    ShadowQueue sq;
+    double *film;          // base film (W*H*3) followed by the splat film (W*H*3)
+    uint32_t *ctr;         // device counters (wr_kernels.h)
+    unsigned long long *sample_next;
+    unsigned long long total_samples;
+    uint32_t capacity;
+    uint32_t shadow_capacity;
+    DevCamera cam;
+    int spp, nverts;
+    uint32_t seed;
+    uint32_t npix;
+    unsigned long long *prof;   // profiling totals (nullptr when off): items[6], extend nv/nt, shadow nv/nt
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// warp-aggregated append: one atomic per warp, lane offsets from ballot/popc
+__device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred, uint32_t &total_out) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    const uint32_t n = __popc(mask);
+    uint32_t base = 0;
+    const uint32_t leader = mask ? (__ffs(mask) - 1) : 0;
+    if (n && lane_id() == leader) base = atomicAdd(counter, n);
+    base = __shfl_sync(0xffffffffu, base, leader);
+    total_out = n;
+    return base + __popc(mask & ((1u << lane_id()) - 1u));
+}
+
+__device__ __forceinline__ void push_shadow(const WaveArgs &w, bool pred, f3 o, f3 d, float tmax, uint32_t slot, f3 c) {
+    uint32_t n;
+    const uint32_t idx = warp_append(w.ctr + CTR_SHADOW, pred, n);
+    if (pred && idx < w.shadow_capacity) {
+        w.sq.o[idx] = make_float4(o.x, o.y, o.z, tmax);
+        w.sq.d[idx] = make_float4(d.x, d.y, d.z, __uint_as_float(slot));
+        w.sq.c[idx] = make_float4(c.x, c.y, c.z, 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_extend(DevScene s, WaveArgs w) {
+    __shared__ uint32_t stack[kSmemStack * kTraceBlock];
+    const uint32_t n = w.ctr[CTR_ACTIVE];
+    uint32_t nv = 0, nt = 0;
+    uint32_t *pv = w.prof ? &nv : nullptr, *pt = w.prof ? &nt : nullptr;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = w.cur.o[i], d = w.cur.d[i];
+        float t, bu = 0.f, bv = 0.f;
+        uint32_t tri;
+        traverse<false>(s.nodes, s.tris, xyz(o), xyz(d), kRayEps, __int_as_float(0x7f800000), stack, t, tri, bu, bv,
+                        pv, pt);
+        w.hit[i] = make_float4(t, bu, bv, __uint_as_float(tri));
+    }
+    if (w.prof) {
+        atomicAdd(w.prof + 6, (unsigned long long)nv);
+        atomicAdd(w.prof + 7, (unsigned long long)nt);
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 0, (unsigned long long)n);
+    }
+}
+
+__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
+    const uint32_t n = w.ctr[CTR_ACTIVE];
+    if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 1, (unsigned long long)n);
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp_global * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t i = base + lane_id();
+        const bool valid = i < n;
+        bool alive = false, shadow = false;
+        f3 so = mk(0, 0, 0), sd = mk(0, 0, 1), sc = mk(0, 0, 0);
+        float stmax = 0.f;
+        f3 no = mk(0, 0, 0), nd = mk(0, 0, 1), nthr = mk(0, 0, 0);
+        float npdf = 0.f;
+        uint32_t pixel = 0, sample = 0, depth = 0;
+        if (valid) {
+            const float4 o4 = w.cur.o[i], d4 = w.cur.d[i], t4 = w.cur.thr[i];
+            depth = w.cur.meta[i];
+            const float4 h = w.hit[i];
+            const f3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
+            const float prevPdfW = o4.w;
+            pixel = __float_as_uint(d4.w);
+            sample = __float_as_uint(t4.w);
+            const uint32_t tri = __float_as_uint(h.w);
+            const float t = h.x;
+            if (tri == MISS) {
+                if (s.has_env) {
+                    // strategy B on the environment (pathnextevent.h:128-146)
+                    const float cPdfA = prevPdfW;   // ConvertToArea to an environment vertex: 1/|d|^2
+                    const float lPdfA = s.env_select_pdf * env_pdf(s, d);
+                    const float mis = cPdfA / (lPdfA + cPdfA);
+                    const f3 c = thr * env_eval(s, d) * mis;
+                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                        double *f = w.film + 3 * size_t(pixel);
+                        atomicAdd(f + 0, double(c.x)); atomicAdd(f + 1, double(c.y)); atomicAdd(f + 2, double(c.z));
+                    }
+                }
+            } else {
+                const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
+                const f3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(cc);
+                const f3 ng = normalize(cross(p1 - p0, p2 - p0));
+                const f3 pos = o + d * t;
+                const uint32_t mat = __ldg(s.tri_mat + tri);
+                if (mat & LIGHT_BIT) {
+                    // strategy B: BSDF-sampled hit on an emitter
+                    const uint32_t li = mat & ~LIGHT_BIT;
+                    const float cosl = dot(ng, d);
+                    if (cosl < 0.f) {   // front face: evalLe1 (diffusearealight.h:48-53)
+                        const float cPdfA = prevPdfW * fabsf(cosl) / (t * t);
+                        const float lPdfA = __ldg(&s.lights[li].select_pdf) * __ldg(&s.lights[li].inv_area);
+                        const float mis = cPdfA / (lPdfA + cPdfA);
+                        const f3 c = thr * mk(__ldg(&s.lights[li].intensity[0]), __ldg(&s.lights[li].intensity[1]),
+                                              __ldg(&s.lights[li].intensity[2])) * mis;
+                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                            double *f = w.film + 3 * size_t(pixel);
+                            atomicAdd(f + 0, double(c.x)); atomicAdd(f + 1, double(c.y)); atomicAdd(f + 2, double(c.z));
+                        }
+                    }
+                } else if (int(depth) + 2 < w.nverts) {
+                    const DevMaterial &m = s.materials[mat];
+                    DevMaterial mm;
+                    mm = m;
+                    const Frame fr(ng);
+                    const f3 wi = -d;
+                    const f3 inL = fr.to_local(wi);
+                    // strategy A: next-event estimation toward this sample's light vertex
+                    const Rand4 r0 = rand4(pixel, sample, 0, w.seed);
+                    const LightVtx l = sample_light(s, r0.a, r0.b);
+                    f3 wo;
+                    float G, convA, dist = 0.f;
+                    if (l.env) {
+                        wo = l.pos;
+                        G = fabsf(dot(ng, wo));
+                        convA = 1.f;
+                    } else {
+                        const f3 uv = l.pos - pos;
+                        const float d2 = len2(uv);
+                        dist = sqrtf(d2);
+                        wo = uv / dist;
+                        const float cl = fabsf(dot(l.n, wo));
+                        convA = cl / d2;
+                        G = fabsf(dot(ng, wo)) * convA;
+                    }
+                    const bool front = l.env || dot(l.n, wo) <= 0.f;   // light emits toward -wo
+                    if (G > 0.f && front && l.pdfA > 0.f) {
+                        const f3 outL = fr.to_local(wo);
+                        const f3 f = bsdf_eval(mm, inL, outL);
+                        if (!is_zero(f)) {
+                            const float bsdfPdfA = bsdf_pdf(mm, inL, outL) * convA;
+                            const float mis = l.pdfA / (l.pdfA + bsdfPdfA);
+                            const float le1 = l.env ? 1.f : kInvPi;
+                            const f3 c = thr * f * (le1 * G * mis) * l.contrib;
+                            if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                                shadow = true;
+                                so = pos; sd = wo; sc = c;
+                                stmax = l.env ? __int_as_float(0x7f800000) : dist - kRayEps;
+                            }
+                        }
+                    }
+                    // BSDF sampling continues the path
+                    const Rand4 rb = rand4(pixel, sample, 2 + depth, w.seed);
+                    f3 outL;
+                    float pdfW;
+                    const f3 wgt = bsdf_sample(mm, inL, rb.a, rb.b, outL, pdfW);
+                    if (!is_zero(wgt) && isfinite(wgt.x + wgt.y + wgt.z)) {
+                        alive = true;
+                        no = pos;
+                        nd = normalize(fr.to_world(outL));
+                        nthr = thr * wgt;
+                        npdf = pdfW;
+                    }
+                }
+            }
+        }
+        push_shadow(w, shadow, so, sd, stmax, pixel, sc);
+        uint32_t cnt;
+        const uint32_t j = warp_append(w.ctr + CTR_NEXT, alive, cnt);
+        if (alive) {
+            w.nxt.o[j] = make_float4(no.x, no.y, no.z, npdf);
+            w.nxt.d[j] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel));
+            w.nxt.thr[j] = make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample));
+            w.nxt.meta[j] = depth + 1;
+        }
+    }
+}
+
+// new camera samples into the free tail of the next wavefront
+__global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) {
+    const uint32_t filled = w.ctr[CTR_NEXT];
+    const unsigned long long issued = *w.sample_next;
+    const unsigned long long remaining = w.total_samples - issued;
+    const uint32_t room = w.capacity > filled ? w.capacity - filled : 0u;
+    const uint32_t n_new = uint32_t(remaining < room ? remaining : room);
+    if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 2, (unsigned long long)n_new);
+    const DevCamera &cam = w.cam;
+    const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), cfz = ld3(cam.fz), corg = ld3(cam.origin);
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp_global * 32u; base < n_new; base += nwarps * 32u) {
+        const uint32_t k = base + lane_id();
+        const bool valid = k < n_new;
+        bool shadow = false;
+        f3 so = mk(0, 0, 0), sd = mk(0, 0, 1), sc = mk(0, 0, 0);
+        float stmax = 0.f;
+        uint32_t slot = 0;
+        if (valid) {
+            const unsigned long long id = issued + k;
+            const uint32_t pixel = uint32_t(id % w.npix);
+            const uint32_t sample = uint32_t(id / w.npix);
+            const uint32_t px = pixel % uint32_t(cam.width), py = pixel / uint32_t(cam.width);
+            const Rand4 r0 = rand4(pixel, sample, 0, w.seed);
+            const LightVtx l = sample_light(s, r0.a, r0.b);
+            // camera vertex: lens point (pinhole when the aperture is zero)
+            f3 c0 = corg;
+            if (cam.aperture > 0.f) {
+                const Rand4 r1 = rand4(pixel, sample, 1, w.seed);
+                const float ax = 2.f * r1.a - 1.f, ay = 2.f * r1.b - 1.f;
+                float rr = 0.f, phi = 0.f;
+                if (ax != 0.f || ay != 0.f) {
+                    if (ax * ax > ay * ay) { rr = ax; phi = (kPi / 4.f) * (ay / ax); }
+                    else { rr = ay; phi = (kPi / 2.f) - (kPi / 4.f) * (ax / ay); }
+                }
+                float sn, cs;
+                sincosf(phi, &sn, &cs);
+                c0 = corg + cfx * (rr * cs * cam.aperture) + cfy * (rr * sn * cam.aperture);
+            }
+            // strategy C: connect the light vertex to the camera (pathnextevent.h:75-99)
+            if (l.pdfA > 0.f) {
+                f3 wl;          // direction camera -> light
+                float G, conv, len = 0.f;
+                if (l.env) {
+                    wl = l.pos;
+                    G = fabsf(dot(cfz, wl));
+                    conv = 1.f;
+                } else {
+                    const f3 uv = l.pos - c0;
+                    const float d2 = len2(uv);
+                    len = sqrtf(d2);
+                    wl = uv / len;
+                    conv = fabsf(dot(l.n, wl)) / d2;
+                    G = fabsf(dot(cfz, wl)) * conv;
+                }
+                const bool front = l.env || dot(l.n, wl) <= 0.f;
+                const float cosT = dot(wl, cfz);
+                if (G > 0.f && front && cosT > 0.f) {
+                    // evalWe1 (thinlens.h:63-80): project through the lens onto the film
+                    const f3 cp = c0 - corg;
+                    const f3 pl = mk(dot(cp, cfx), dot(cp, cfy), dot(cp, cfz));
+                    const f3 dl = mk(dot(wl, cfx), dot(wl, cfy), cosT);
+                    const f3 fpp = dl * (cam.focal / cosT) + pl;
+                    const float fxp = -fpp.x / cam.focal * cam.dist, fyp = -fpp.y / cam.focal * cam.dist;
+                    const float rx = (fxp / float(cam.width) + 0.5f) * float(cam.width);
+                    const float ry = (fyp / float(cam.height) + 0.5f) * float(cam.height);
+                    if (rx >= 0.f && rx < float(cam.width) && ry >= 0.f && ry < float(cam.height)) {
+                        const float c2 = cosT * cosT;
+                        const float we = cam.per_film / (c2 * c2);
+                        const float camPdfA = cam.per_pixel / (c2 * cosT) * conv;
+                        const float mis = l.pdfA / (l.pdfA + camPdfA);
+                        const float le1 = l.env ? 1.f : kInvPi;
+                        const f3 c = l.contrib * (mis * we * G * le1);
+                        const uint32_t sx = min(uint32_t(rx), uint32_t(cam.width - 1));
+                        const uint32_t sy = min(uint32_t(ry), uint32_t(cam.height - 1));
+                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                            shadow = true;
+                            slot = (sy * uint32_t(cam.width) + sx) | SPLAT_BIT;
+                            sc = c;
+                            if (l.env) { so = c0; sd = wl; stmax = __int_as_float(0x7f800000); }
+                            else { so = l.pos; sd = -wl; stmax = len - kRayEps; }
+                        }
+                    }
+                }
+            }
+            // primary ray through the jittered pixel position (thinlens.h:138-165)
+            const float nsx = (float(px) + r0.c) / float(cam.width), nsy = (float(py) + r0.d) / float(cam.height);
+            const f3 film = mk((nsx - 0.5f) * float(cam.width), (nsy - 0.5f) * float(cam.height), -cam.dist);
+            const f3 fpp = film * (cam.focal / film.z);
+            const f3 cpl = mk(dot(c0 - corg, cfx), dot(c0 - corg, cfy), dot(c0 - corg, cfz));
+            const f3 dir = normalize(fpp - cpl);
+            const float ct = dir.z;
+            const float pdfW = cam.per_film / (ct * ct * ct) / float(w.npix);
+            const f3 dw = normalize(cfx * dir.x + cfy * dir.y + cfz * dir.z);
+            const uint32_t j = filled + k;
+            w.nxt.o[j] = make_float4(c0.x, c0.y, c0.z, pdfW);
+            w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(pixel));
+            w.nxt.thr[j] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sample));
+            w.nxt.meta[j] = 0u;
+        }
+        push_shadow(w, shadow, so, sd, stmax, slot, sc);
+    }
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_shadow(DevScene s, WaveArgs w) {
+    __shared__ uint32_t stack[kSmemStack * kTraceBlock];
+    const uint32_t n = min(w.ctr[CTR_SHADOW], w.shadow_capacity);
+    uint32_t nv = 0, nt = 0;
+    uint32_t *pv = w.prof ? &nv : nullptr, *pt = w.prof ? &nt : nullptr;
+    if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 3, (unsigned long long)n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = w.sq.o[i], d = w.sq.d[i];
+        float t, bu, bv;
+        uint32_t tri;
+        const bool occ = traverse<true>(s.nodes, s.tris, xyz(o), xyz(d), kRayEps, o.w, stack, t, tri, bu, bv, pv, pt);
+        if (!occ) {
+            const float4 c = w.sq.c[i];
+            const uint32_t slot = __float_as_uint(d.w);
+            double *f = w.film + ((slot & SPLAT_BIT) ? 3 * size_t(w.npix) : size_t(0)) + 3 * size_t(slot & ~SPLAT_BIT);
+            atomicAdd(f + 0, double(c.x));
+            atomicAdd(f + 1, double(c.y));
+            atomicAdd(f + 2, double(c.z));
+        }
+    }
+    if (w.prof) {
+        atomicAdd(w.prof + 8, (unsigned long long)nv);
+        atomicAdd(w.prof + 9, (unsigned long long)nt);
+    }
+}
+
+// queue bookkeeping between iterations (one thread)
+__global__ void k_advance(WaveArgs w) {
+    const uint32_t filled = w.ctr[CTR_NEXT];
+    const unsigned long long issued = *w.sample_next;
+    const unsigned long long remaining = w.total_samples - issued;
+    const uint32_t room = w.capacity > filled ? w.capacity - filled : 0u;
+    const uint32_t n_new = uint32_t(remaining < room ? remaining : room);
+    if (w.ctr[CTR_SHADOW] > w.ctr[CTR_SHADOW_MAX]) w.ctr[CTR_SHADOW_MAX] = w.ctr[CTR_SHADOW];
+    if (w.ctr[CTR_SHADOW] > w.shadow_capacity) w.ctr[CTR_OVERFLOW] = 1;
+    w.ctr[CTR_ACTIVE] = filled + n_new;
+    w.ctr[CTR_NEXT] = 0;
+    w.ctr[CTR_SHADOW] = 0;
+    w.ctr[CTR_ITER] += 1;
+    *w.sample_next = issued + n_new;
+    w.ctr[CTR_DONE] = (filled + n_new == 0u) ? 1u : 0u;
+}
+
+// final image = base / spp + splat / (spp * W * H)   (film.h:70-90)
+__global__ void k_resolve(const double *film, double *out, uint32_t npix, int spp) {
+    const double bs = 1.0 / double(spp), as = 1.0 / double(spp) / double(npix);
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 3 * size_t(npix); i += size_t(gridDim.x) * blockDim.x) {
+        double c = 0.0;
+        c += film[i] * bs;
+        c += film[3 * size_t(npix) + i] * as;
+        out[i] = c;
+    }
+}
+
+// ----------------------------------------------------------- ray batches ----
+// rays: n x 8 floats (ox, oy, oz, tnear, dx, dy, dz, tfar)
+__global__ void __launch_bounds__(kTraceBlock) k_trace_batch(DevScene s, const float4 *rays, uint32_t n, int any_hit,
+                                                           float4 *out, uint32_t *visits) {
+    __shared__ uint32_t stack[kSmemStack * kTraceBlock];
+    uint32_t nv = 0, nt = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = rays[2 * i], b = rays[2 * i + 1];
+        float t, bu = 0.f, bv = 0.f;
+        uint32_t tri;
+        bool hit;
+        if (any_hit) hit = traverse<true>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt);
+        else hit = traverse<false>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt);
+        uint32_t gid = MISS, pid = MISS;
+        if (hit) {
+            gid = __float_as_uint(__ldg(s.tris + 3 * tri + 1).w);
+            pid = __float_as_uint(__ldg(s.tris + 3 * tri + 2).w);
+        }
+        out[2 * i] = make_float4(__uint_as_float(gid), __uint_as_float(pid), hit ? t : __int_as_float(0x7f800000), 0.f);
+        out[2 * i + 1] = make_float4(bu, bv, __uint_as_float(tri), 0.f);
+    }
+    if (visits) {
+        atomicAdd(visits, nv);
+        atomicAdd(visits + 1, nt);
+    }
+}
+
+// ------------------------------------------------------ FP64 CDF builders ----
+// CdfTable construction (src/common/cdftable.h:10-30) as FP64 prefix sums on
+// the device, one block per table; the tables are stored as float for
+// sampling. pdf_i = |w_i| / sum, cdf_i = sum_{j<=i} pdf_j, cdf_last = 1.
+__global__ void k_cdf_build(const double *weights, const uint32_t *offsets, uint32_t ntables, float *cdf_out,
+                            float *pdf_out, double *sums_out) {
+    __shared__ double part[1024];
+    __shared__ double carry;
+    const uint32_t tb = blockIdx.x;
+    if (tb >= ntables) return;
+    const uint32_t b0 = offsets[tb], b1 = offsets[tb + 1], n = b1 - b0;
+    // total
+    double acc = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) acc += fabs(weights[b0 + i]);
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double total = part[0];
+    __syncthreads();
+    if (threadIdx.x == 0) { carry = 0.0; if (sums_out) sums_out[tb] = total; }
+    __syncthreads();
+    const double inv = total > 0.0 ? 1.0 / total : 0.0;
+    // chunked inclusive scan of the pdfs
+    for (uint32_t c0 = 0; c0 < n; c0 += blockDim.x) {
+        const uint32_t i = c0 + threadIdx.x;
+        const double p = i < n ? fabs(weights[b0 + i]) * inv : 0.0;
+        part[threadIdx.x] = p;
+        __syncthreads();
+        for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+            const double v = threadIdx.x >= off ? part[threadIdx.x - off] : 0.0;
+            __syncthreads();
+            part[threadIdx.x] += v;
+            __syncthreads();
+        }
+        if (i < n) {
+            const double c = carry + part[threadIdx.x];
+            cdf_out[b0 + i] = (i == n - 1) ? 1.0f : float(c);
+            pdf_out[b0 + i] = float(p);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += part[blockDim.x - 1];
+        __syncthreads();
+    }
+}
+
+// environment weights sin(theta_row) * |L| (equirectangular.h:40-61)
+__global__ void k_env_weights(const float4 *texels, int w, int h, double *out) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < size_t(w) * h; i += size_t(gridDim.x) * blockDim.x) {
+        const int y = int(i / w);
+        const double v = (double(y) + 0.5) / double(h);
+        const double sine = sin(v * 3.14159265358979323846);
+        const float4 t = texels[i];
+        out[i] = sine * sqrt(double(t.x) * t.x + double(t.y) * t.y + double(t.z) * t.z);
+    }
+}
+
+__global__ void k_scale_pdf(const double *weights, double total, float *pdf, size_t n) {
+    const double inv = total > 0.0 ? 1.0 / total : 0.0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        pdf[i] = float(fabs(weights[i]) * inv);
+}
+
+}  // namespace wrd
+
+// ------------------------------------------------------------ launch API ----
+namespace wrk {
+
+using namespace wrd;
+
+static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &r) {
+    WaveArgs w;
+    const int c = parity & 1, n = c ^ 1;
+    w.cur = {b.o[c], b.d[c], b.thr[c], b.meta[c]};
+    w.nxt = {b.o[n], b.d[n], b.thr[n], b.meta[n]};
+    w.hit = b.hit;
+    w.sq = {b.sh_o, b.sh_d, b.sh_c};
+    w.film = b.film;
+    w.ctr = b.ctr;
+    w.sample_next = b.sample_next;
+    w.total_samples = r.total_samples;
+    w.capacity = b.capacity;
+    w.shadow_capacity = b.shadow_capacity;
+    w.cam = r.cam;
+    w.spp = r.spp;
+    w.nverts = r.nverts;
+    w.seed = r.seed;
+    w.npix = uint32_t(r.cam.width) * uint32_t(r.cam.height);
+    w.prof = r.prof;
+    return w;
+}
+
+void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
+                   cudaStream_t st) {
+    const WaveArgs w = make_args(b, parity, r);
+    switch (which) {
+        case KERNEL_EXTEND: k_extend<<<r.grid_trace, kTraceBlock, 0, st>>>(s, w); break;
+        case KERNEL_SHADE: k_shade<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
+        case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
+        case KERNEL_SHADOW: k_shadow<<<r.grid_trace, kTraceBlock, 0, st>>>(s, w); break;
+        case KERNEL_ADVANCE: k_advance<<<1, 1, 0, st>>>(w); break;
+        default: break;
+    }
+}
+
+void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity, cudaStream_t st) {
+    for (int k : {KERNEL_EXTEND, KERNEL_SHADE, KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE})
+        launch_kernel(k, s, b, r, parity, st);
+}
+
+void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st) {
+    // the first wavefront: raygen into buffer 0 (parity 1 makes buffer 0 the "next" one), then bookkeeping
+    for (int k : {KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE}) launch_kernel(k, s, b, r, 1, st);
+}
+
+void launch_resolve(const double *film, double *out, uint32_t npix, int spp, cudaStream_t st) {
+    k_resolve<<<592, 256, 0, st>>>(film, out, npix, spp);
+}
+
+void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,
+                        int grid, cudaStream_t st) {
+    k_trace_batch<<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+}
+
+void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t ntables, float *cdf, float *pdf,
+                      double *sums, cudaStream_t st) {
+    if (ntables) k_cdf_build<<<ntables, 1024, 0, st>>>(weights, offsets, ntables, cdf, pdf, sums);
+}
+
+void launch_env_weights(const float4 *texels, int w, int h, double *out, cudaStream_t st) {
+    k_env_weights<<<592, 256, 0, st>>>(texels, w, h, out);
+}
+
+void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n, cudaStream_t st) {
+    k_scale_pdf<<<592, 256, 0, st>>>(weights, total, pdf, n);
+}
+
+int occupancy_blocks(int which) {
+    int nb = 0;
+    if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend, kTraceBlock, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeBlock, 0);
+    return nb;
+}
+
+}  // namespace wrk

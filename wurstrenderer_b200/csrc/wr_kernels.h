@@ -1,0 +1,49 @@
+// Host-side launch interface of the wavefront kernels (wr_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "wr_device.cuh"
+
+namespace wrk {
+
+using namespace wrd;
+
+struct WaveBuffers {
+    float4 *o[2], *d[2], *thr[2];
+    uint32_t *meta[2];
+    float4 *hit;
+    float4 *sh_o, *sh_d, *sh_c;
+    double *film;                      // base (npix*3) then splat (npix*3)
+    uint32_t *ctr;                     // CTR_COUNT counters
+    unsigned long long *sample_next;
+    uint32_t capacity, shadow_capacity;
+};
+
+struct RenderLaunch {
+    wrd::DevCamera cam;
+    int spp, nverts;
+    uint32_t seed;
+    unsigned long long total_samples;
+    int grid_trace, grid_shade;
+    unsigned long long *prof;   // device profiling totals or nullptr
+};
+
+enum KernelId { KERNEL_EXTEND = 0, KERNEL_SHADE = 1, KERNEL_RAYGEN = 2, KERNEL_SHADOW = 3, KERNEL_ADVANCE = 4,
+                KERNEL_RESOLVE = 5 };
+
+void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
+                   cudaStream_t st);
+void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st);
+void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity, cudaStream_t st);
+void launch_resolve(const double *film, double *out, uint32_t npix, int spp, cudaStream_t st);
+void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,
+                        int grid, cudaStream_t st);
+void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t ntables, float *cdf, float *pdf,
+                      double *sums, cudaStream_t st);
+void launch_env_weights(const float4 *texels, int w, int h, double *out, cudaStream_t st);
+void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n, cudaStream_t st);
+int occupancy_blocks(int which);
+
+}  // namespace wrk
