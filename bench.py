@@ -204,6 +204,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queue-capacity", type=int, default=0)
+    ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs only)")
+    ap.add_argument("--quick", action="store_true", help="skip e2e, profile and CPU baseline (profiling runs)")
     args = ap.parse_args()
 
     world = env_int("WORLD_SIZE", 1)
@@ -233,12 +235,14 @@ def main():
     info = scene.info
     W, H = info["width"], info["height"]
     spp, nverts = info["num_spp"], info["num_path_vertices"]
+    if args.spp:
+        spp = args.spp
     film = torch.empty((H, W, 3), dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
     qc = args.queue_capacity or None
 
     def step(seed):
-        scene.render_device(film.data_ptr(), seed=seed, queue_capacity=qc)
+        scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc)
         st = scene.stats
         if world > 1:
             dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
@@ -274,13 +278,22 @@ def main():
     paths_per_rank = W * H * spp
     value = paths_per_rank * world * args.steps / (max_ms / 1e3) / 1e6
 
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                              "ms_per_step": max_ms / args.steps, "spp": spp, "quick": True}), flush=True)
+        scene.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
     # end to end through the public C ABI with host output (device->host copy of the film inside)
     host = np.empty((H, W, 3), np.float64)
     e2e_ms = 0.0
     for i in range(args.steps):
         torch.cuda.synchronize()
         a = time.perf_counter()
-        scene.render(seed=424242 + i, out=host, queue_capacity=qc)
+        scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc)
         e2e_ms += (time.perf_counter() - a) * 1e3
     e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -288,7 +301,7 @@ def main():
     e2e_value = paths_per_rank * world * args.steps / (float(e2e_t.item()) / 1e3) / 1e6
 
     # one profiled render (per-kernel events + traversal counters) for the roofline, outside the timed region
-    scene.render_device(film.data_ptr(), seed=99, queue_capacity=qc, profile=2)
+    scene.render_device(film.data_ptr(), spp=spp, seed=99, queue_capacity=qc, profile=2)
     prof = scene.stats
     kn = wr.KERNELS
     k_ms = dict(zip(kn, prof["kernel_ms"]))

@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _tie_or_edge(t_ref, t_gpu, uv_ref):
-    tie = np.abs(t_ref - t_gpu) <= 1e-5 * np.maximum(np.abs(t_ref), 1.0)
+    with np.errstate(invalid="ignore"):
+        tie = np.abs(t_ref - t_gpu) <= 1e-5 * np.maximum(np.abs(t_ref), 1.0)
     edge = (uv_ref[:, 0] < 1e-5) | (uv_ref[:, 1] < 1e-5) | (1.0 - uv_ref[:, 0] - uv_ref[:, 1] < 1e-5)
     return tie | edge
 
@@ -56,17 +57,21 @@ def test_occlusion_matches_oracle(wr_lib, oracle_lib, name):
     assert (occ != occ_ref).mean() < 2e-3
 
 
-def test_empty_and_tiny_batches(wr_lib):
+def test_empty_and_tiny_batches(wr_lib, oracle_lib):
     path, _ = golden_scene("cornell")
     with wr_lib.Scene.from_file(path) as sc:
         g, p, t, uv = sc.trace_closest(np.zeros((0, 8), np.float32))
         assert g.shape == (0,)
-        r = np.array([[0, 1, 3.5, 1e-4, 0, 0, -1, np.inf]], np.float32)   # toward the back wall
+        r = np.array([[0.6, 1.5, 3.5, 1e-4, 0, 0, -1, np.inf],      # over the short box to the back wall
+                      [0, 1, 3.5, 1e-4, 0, 0, -1, np.inf],          # onto the tall box
+                      [0, 1, 3.5, 1e-4, 0, 0, 1, np.inf],           # out of the open front: miss
+                      [0, 1, 0.5, 1e-4, 0, 1, 0, 0.5]], np.float32)  # segment ending below the ceiling: miss
         g, p, t, uv = sc.trace_closest(r)
-        assert g[0] >= 0 and abs(t[0] - 4.5) < 1e-4
-        r = np.array([[0, 1, 3.5, 1e-4, 0, 0, 1, np.inf]], np.float32)    # out of the open front
-        g, p, t, uv = sc.trace_closest(r)
-        assert g[0] == -1 and p[0] == -1
+    go, po, to, _ = oracle_lib.OracleScene(path).trace_closest(r)
+    assert g[0] >= 0 and abs(t[0] - 4.5) < 1e-4
+    assert np.array_equal(g, go) and np.array_equal(p, po)
+    assert (g[2], p[2], g[3]) == (-1, -1, -1)
+    assert np.allclose(t[:2], to[:2], rtol=1e-5)
 
 
 def test_traversal_statistics(wr_lib):
