@@ -118,6 +118,17 @@ int wr_render_device(wr_scene *scene, const wr_render_desc *desc, double *out_rg
 
 int wr_get_render_stats(const wr_scene *scene, wr_render_stats *stats);
 
+/* No counterpart in the reference. wr_render_device without any allocation:
+ * the wavefront and film scratch live in one fixed 10 MiB device array that
+ * the library holds on every GPU it is loaded on, for callers that may not
+ * allocate device memory while running (fixed memory budgets, or no implicit
+ * synchronisation from cudaMalloc/cudaFree). Limits: films of at most 65,536
+ * pixels (larger: WR_ERR_INVALID_ARGUMENT), a 32,768-path wavefront, plain
+ * kernel launches. Every call clears and reuses the same array, so calls that
+ * overlap on the GPU race; the first call on a device resolves the array's
+ * address and should precede any stream capture. */
+int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc, double *out_rgb_device);
+
 /* Closest-hit queries (EmbreeAccel::intersectTriangleInfo,
  * src/accel/embreeaccel.h:425-464). rays: n x 8 floats
  * (ox, oy, oz, tnear, dx, dy, dz, tfar) in host memory. Outputs (host):

@@ -69,7 +69,7 @@ class SceneInfo(ctypes.Structure):
 EXPORTS = ["wr_scene_create", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
-           "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version"]
+           "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc"]
 
 _lib = None
 
@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH):
     L.wr_scene_set_camera_json.argtypes = [vp, cp]
     L.wr_render.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_render_device.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
+    L.wr_render_device_noalloc.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_get_render_stats.argtypes = [vp, ctypes.POINTER(RenderStats)]
     L.wr_trace_closest.argtypes = [vp, fp, ip, fp, fp, fp, fp]
     L.wr_trace_occluded.argtypes = [vp, fp, ip, fp]

@@ -805,3 +805,36 @@ int wr_run_jsimple2(const char *json_text) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Read-only view of a scene handle for other translation units of this library.
+namespace wr_internal {
+
+struct SceneView {
+    wrd::DevScene dev;
+    cudaStream_t stream;
+    int device;
+    uint32_t *pinned;
+    cudaEvent_t ev0, ev1;
+    const wr::Scene *host;
+    wr_render_stats *stats;
+};
+
+bool scene_view(wr_scene *s, SceneView *v) {
+    if (!s || !v) return false;
+    v->dev = s->dev;
+    v->stream = s->stream;
+    v->device = s->device;
+    v->pinned = s->pinned;
+    v->ev0 = s->ev0;
+    v->ev1 = s->ev1;
+    v->host = &s->host;
+    v->stats = &s->stats;
+    return true;
+}
+
+wrd::DevCamera camera_constants(const wr::Camera &c) { return make_camera(c); }
+
+void set_last_error(const std::string &m) { g_last_error = m; }
+
+}  // namespace wr_internal

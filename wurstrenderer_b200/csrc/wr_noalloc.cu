@@ -1,0 +1,209 @@
+// wr_render_device_noalloc: the wavefront render with all of its scratch memory
+// in one fixed, statically allocated device array, so that the call itself
+// allocates nothing.
+//
+// Who needs it: host applications that run under a fixed device-memory budget
+// or must not allocate once they are running -- for example an engine that has
+// handed the rest of the GPU to its own caching allocator, or a latency-bound
+// service that cannot afford the implicit device synchronisation that
+// cudaMalloc/cudaFree may perform while other streams are busy. wr_render_device
+// allocates its wavefront buffers on first use (and again when the film size or
+// queue capacity changes); this variant never does.
+//
+// Limits and rules:
+//   * scratch: kScratchBytes = 10 MiB in a file-scope __device__ array; every
+//     GPU that loads this library holds it until the process exits;
+//   * film at most kMaxPixels = 65,536 pixels (e.g. 256 x 256); larger cameras
+//     are rejected with WR_ERR_INVALID_ARGUMENT;
+//   * the wavefront holds kCapacity = 32,768 paths (desc->queue_capacity and the
+//     graph option are ignored; kernels are launched one by one);
+//   * all calls share the one array: the film, counters and sample cursor are
+//     cleared at the start of every call, and two calls whose work overlaps on
+//     the GPU (for example from two threads with two scene handles on one
+//     device) race on it -- serialise them;
+//   * the first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress (with that device current); make that first call
+//     before any stream capture is started.
+
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/wurst_b200.h"
+#include "wr_host.h"
+#include "wr_kernels.h"
+
+namespace wr_internal {
+struct SceneView {
+    wrd::DevScene dev;
+    cudaStream_t stream;
+    int device;
+    uint32_t *pinned;
+    cudaEvent_t ev0, ev1;
+    const wr::Scene *host;
+    wr_render_stats *stats;
+};
+bool scene_view(wr_scene *s, SceneView *v);
+wrd::DevCamera camera_constants(const wr::Camera &c);
+void set_last_error(const std::string &m);
+}  // namespace wr_internal
+
+namespace {
+
+constexpr size_t kScratchBytes = size_t(10) << 20;
+constexpr uint32_t kCapacity = 32768;
+constexpr size_t kMaxPixels = 65536;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+std::mutex g_setup_mutex;
+unsigned char *g_scratch_ptr[kMaxDevices] = {};
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// carves the wavefront and film out of the scratch array; returns the bytes used
+size_t carve(unsigned char *base, size_t npix, wrk::WaveBuffers &b) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char *p = base + off;
+        off = align256(off + bytes);
+        return p;
+    };
+    for (int p = 0; p < 2; ++p) {
+        b.o[p] = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 16));
+        b.d[p] = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 16));
+        b.thr[p] = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 16));
+        b.meta[p] = reinterpret_cast<uint32_t *>(take(size_t(kCapacity) * 4));
+    }
+    b.hit = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 16));
+    b.sh_o = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 2 * 16));
+    b.sh_d = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 2 * 16));
+    b.sh_c = reinterpret_cast<float4 *>(take(size_t(kCapacity) * 2 * 16));
+    b.ctr = reinterpret_cast<uint32_t *>(take(wrd::CTR_COUNT * 4));
+    b.sample_next = reinterpret_cast<unsigned long long *>(take(8));
+    b.film = reinterpret_cast<double *>(take(npix * 6 * 8));
+    b.capacity = kCapacity;
+    b.shadow_capacity = 2 * kCapacity;
+    return off;
+}
+
+int fail(int code, const std::string &m) {
+    wr_internal::set_last_error(m);
+    return code;
+}
+
+#define NA_CUDA(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(WR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+}  // namespace
+
+extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc_in, double *out_rgb_device) {
+    wr_internal::SceneView v;
+    if (!wr_internal::scene_view(scene, &v) || !out_rgb_device) return fail(WR_ERR_INVALID_ARGUMENT, "null argument");
+    const wr::Scene &h = *v.host;
+    if (!h.has_camera) return fail(WR_ERR_INVALID_ARGUMENT, "scene has no camera");
+    wr_render_desc desc{};
+    if (desc_in) desc = *desc_in;
+    if (desc.render_index < 0) return fail(WR_ERR_INVALID_ARGUMENT, "render_index must be >= 0");
+    wr::RenderEntry re;
+    if (size_t(desc.render_index) < h.renders.size()) re = h.renders[desc.render_index];
+    const int spp = desc.num_spp > 0 ? desc.num_spp : re.num_spp;
+    const int nverts = desc.num_path_vertices > 0 ? desc.num_path_vertices : re.num_path_vertices;
+    if (spp <= 0) return fail(WR_ERR_INVALID_ARGUMENT, "num_spp must be positive");
+    const size_t npix = size_t(h.camera.width) * size_t(h.camera.height);
+    if (npix > kMaxPixels)
+        return fail(WR_ERR_INVALID_ARGUMENT, "wr_render_device_noalloc: film of " + std::to_string(npix) +
+                                                 " pixels exceeds the fixed scratch limit of " + std::to_string(kMaxPixels) +
+                                                 " pixels (use wr_render_device)");
+    if (v.device < 0 || v.device >= kMaxDevices) return fail(WR_ERR_UNSUPPORTED, "device index out of range");
+
+    int prev = 0;
+    NA_CUDA(cudaGetDevice(&prev));
+    if (prev != v.device) NA_CUDA(cudaSetDevice(v.device));
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (!g_scratch_ptr[v.device]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+            if (e != cudaSuccess) {
+                if (prev != v.device) cudaSetDevice(prev);
+                return fail(WR_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+            }
+            g_scratch_ptr[v.device] = static_cast<unsigned char *>(p);
+        }
+        base = g_scratch_ptr[v.device];
+    }
+    wrk::WaveBuffers b{};
+    const size_t used = carve(base, npix, b);
+    if (used > kScratchBytes) {
+        if (prev != v.device) cudaSetDevice(prev);
+        return fail(WR_ERR_INVALID_ARGUMENT, "film does not fit the fixed scratch array");
+    }
+
+    int sms = 148;
+    NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v.device));
+    wrk::RenderLaunch r{};
+    r.cam = wr_internal::camera_constants(h.camera);
+    r.spp = spp;
+    r.nverts = nverts;
+    r.seed = desc.seed;
+    r.total_samples = (unsigned long long)npix * unsigned(spp);
+    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * (wrk::occupancy_blocks(0) > 0 ? wrk::occupancy_blocks(0) : 1);
+    r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * (wrk::occupancy_blocks(1) > 0 ? wrk::occupancy_blocks(1) : 1);
+    r.prof = nullptr;
+
+    cudaStream_t st = v.stream;
+    NA_CUDA(cudaMemsetAsync(b.film, 0, npix * 6 * 8, st));
+    NA_CUDA(cudaMemsetAsync(b.ctr, 0, wrd::CTR_COUNT * 4, st));
+    NA_CUDA(cudaMemsetAsync(b.sample_next, 0, 8, st));
+    NA_CUDA(cudaEventRecord(v.ev0, st));
+    unsigned long long iterations = 0, launches = 0;
+    if (nverts > 1) {
+        const unsigned long long waves = (r.total_samples + kCapacity - 1) / kCapacity;
+        const unsigned long long limit = (waves + 2) * (unsigned long long)(nverts + 2) + 64;
+        wrk::launch_prime(v.dev, b, r, st);
+        NA_CUDA(cudaGetLastError());
+        launches += 3;
+        bool done = false;
+        while (!done) {
+            wrk::launch_iteration(v.dev, b, r, 0, st);
+            wrk::launch_iteration(v.dev, b, r, 1, st);
+            NA_CUDA(cudaGetLastError());
+            iterations += 2;
+            launches += 10;
+            NA_CUDA(cudaMemcpyAsync(v.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
+            NA_CUDA(cudaStreamSynchronize(st));
+            done = v.pinned[wrd::CTR_DONE] != 0;
+            if (!done && iterations > limit) {
+                if (prev != v.device) cudaSetDevice(prev);
+                return fail(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
+            }
+        }
+        if (v.pinned[wrd::CTR_OVERFLOW]) return fail(WR_ERR_CUDA, "shadow queue overflow");
+    }
+    wrk::launch_resolve(b.film, out_rgb_device, uint32_t(npix), spp, st);
+    NA_CUDA(cudaGetLastError());
+    launches += 1;
+    NA_CUDA(cudaEventRecord(v.ev1, st));
+    NA_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    NA_CUDA(cudaEventElapsedTime(&ms, v.ev0, v.ev1));
+    wr_render_stats &stats = *v.stats;
+    stats = wr_render_stats{};
+    stats.render_ms = ms;
+    stats.paths = r.total_samples;
+    stats.iterations = iterations;
+    stats.queue_capacity = kCapacity;
+    stats.grid_trace = r.grid_trace;
+    stats.grid_shade = r.grid_shade;
+    stats.kernel_launches = launches;
+    if (prev != v.device) NA_CUDA(cudaSetDevice(prev));
+    return WR_OK;
+}
