@@ -117,11 +117,19 @@ struct TraceStack {
 
 // Traverses the BVH. ANY_HIT: returns at the first accepted hit.
 // On return `t` holds the closest accepted distance; `tri` the leaf-order triangle (or MISS).
+//
+// Loop structure after Aila & Laine ("Understanding the Efficiency of Ray
+// Traversal on GPUs", HPG 2009): inner nodes and leaves are handled in two
+// separate loops, and a lane that reaches a leaf postpones it and keeps
+// descending inner nodes until every converged lane of the warp holds a leaf,
+// so that the triangle tests run with most lanes active. The warp vote only
+// steers scheduling; each lane's result does not depend on other lanes.
 template <bool ANY_HIT>
 __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const float4 *__restrict__ tris, f3 o,
                                          f3 d, float tmin, float tmax, uint32_t *smem_stack, float &t, uint32_t &tri,
                                          float &bu, float &bv, uint32_t *node_visits = nullptr,
                                          uint32_t *tri_tests = nullptr) {
+    constexpr int kDone = 0x7fffffff;   // traversal finished (stack empty)
     const RayPre r = ray_setup(o, d);
     TraceStack st;
     st.smem = smem_stack + threadIdx.x;
@@ -129,10 +137,11 @@ __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const
     st.sp = 0;
     tri = MISS;
     t = tmax;
-    int node = 0;
+    int node = 0;    // next inner node (>= 0), a leaf code (< 0) or kDone
+    int leaf = 0;    // postponed leaf code (< 0), 0 when none
     uint32_t nv = 0, nt = 0;
-    while (true) {
-        while (node >= 0) {
+    while (node != kDone) {
+        while (node >= 0 && node != kDone) {
             const float4 n0 = __ldg(nodes + 4 * node + 0);
             const float4 n1 = __ldg(nodes + 4 * node + 1);
             const float4 n2 = __ldg(nodes + 4 * node + 2);
@@ -152,32 +161,39 @@ __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const
             } else if (h1) {
                 node = c1;
             } else {
-                if (st.sp == 0) { node = 0x7fffffff; break; }
-                node = st.pop();
+                node = st.sp ? st.pop() : kDone;
             }
+            if (node < 0 && leaf == 0) {   // postpone the first leaf found, keep descending
+                leaf = node;
+                node = st.sp ? st.pop() : kDone;
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;
         }
-        if (node == 0x7fffffff) break;
-        // leaf
-        const uint32_t code = uint32_t(node);
-        const uint32_t first = code & 0x07ffffffu;
-        const uint32_t count = ((code >> 27) & 0xfu) + 1u;
-        for (uint32_t i = first; i < first + count; ++i) {
-            const float4 a = __ldg(tris + 3 * i + 0);
-            const float4 b = __ldg(tris + 3 * i + 1);
-            const float4 c = __ldg(tris + 3 * i + 2);
-            ++nt;
-            float th, uh, vh;
-            if (tri_test(r, a, b, c, tmin, t, th, uh, vh)) {
-                if (ANY_HIT) {
-                    t = th; tri = i; bu = uh; bv = vh;
-                    if (node_visits) { *node_visits += nv; *tri_tests += nt; }
-                    return true;
+        while (leaf < 0) {
+            const uint32_t code = uint32_t(leaf);
+            const uint32_t first = code & 0x07ffffffu;
+            const uint32_t count = ((code >> 27) & 0xfu) + 1u;
+            for (uint32_t i = first; i < first + count; ++i) {
+                const float4 a = __ldg(tris + 3 * i + 0);
+                const float4 b = __ldg(tris + 3 * i + 1);
+                const float4 c = __ldg(tris + 3 * i + 2);
+                ++nt;
+                float th, uh, vh;
+                if (tri_test(r, a, b, c, tmin, t, th, uh, vh)) {
+                    if (ANY_HIT) {
+                        t = th; tri = i; bu = uh; bv = vh;
+                        if (node_visits) { *node_visits += nv; *tri_tests += nt; }
+                        return true;
+                    }
+                    if (th < t || tri == MISS) { t = th; tri = i; bu = uh; bv = vh; }
                 }
-                if (th < t || tri == MISS) { t = th; tri = i; bu = uh; bv = vh; }
+            }
+            leaf = 0;
+            if (node < 0 && node != kDone) {   // the traversal is sitting on another leaf
+                leaf = node;
+                node = st.sp ? st.pop() : kDone;
             }
         }
-        if (st.sp == 0) break;
-        node = st.pop();
     }
     if (node_visits) { *node_visits += nv; *tri_tests += nt; }
     return tri != MISS;
