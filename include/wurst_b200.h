@@ -44,7 +44,8 @@ typedef struct wr_render_desc {
     int queue_capacity;      /* wavefront slots; 0 = default (tuned) */
     int grid_trace;          /* persistent blocks of the traversal kernels; 0 = occupancy-derived */
     int grid_shade;          /* persistent blocks of shade / raygen; 0 = occupancy-derived */
-    int use_graph;           /* 1: replay captured CUDA graphs of the bounce loop; 0: plain launches */
+    int use_graph;           /* 1: the whole render is one CUDA-graph launch (while-loop node over the
+                                bounce iterations); 0: host-driven launches */
     int profile;             /* 0: off; 1: per-kernel CUDA-event timing (plain launches);
                                 2: timing + traversal counters (node visits, triangle tests) */
     int reserved[7];
@@ -115,6 +116,25 @@ int wr_render(wr_scene *scene, const wr_render_desc *desc, double *out_rgb);
 /* Same, writing the image to device memory (W*H*3 doubles on the scene's
  * device); no host copy. */
 int wr_render_device(wr_scene *scene, const wr_render_desc *desc, double *out_rgb_device);
+
+/* One render job of a batch (many cameras / resolutions / sample counts over one scene). */
+typedef struct wr_job {
+    const char *camera_json;   /* simple2 "camera" object of this job; NULL: the scene's camera */
+    int num_spp;               /* <= 0: "num_spp" of the render entry */
+    int num_path_vertices;     /* <= 0: "num_path_vertices" of the render entry */
+    unsigned int seed;         /* random streams of this job (mixed with its index) */
+    int reserved[3];
+} wr_job;
+
+/* Renders n jobs over the scene in one wavefront: every job is an independent
+ * PathNeeRenderer::render with its own camera (src/renderer/pathnextevent.h:152-191),
+ * but all their samples share the same queues, and with desc->use_graph the whole
+ * bounce loop of all jobs is one CUDA-graph launch. desc supplies the wavefront
+ * settings (its num_spp / num_path_vertices / seed are ignored). out_rgb receives the
+ * images concatenated in job order (job j: W_j*H_j*3 doubles). */
+int wr_render_batch(wr_scene *scene, const wr_job *jobs, int n, const wr_render_desc *desc, double *out_rgb);
+int wr_render_batch_device(wr_scene *scene, const wr_job *jobs, int n, const wr_render_desc *desc,
+                           double *out_rgb_device);
 
 int wr_get_render_stats(const wr_scene *scene, wr_render_stats *stats);
 

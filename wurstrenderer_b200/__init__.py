@@ -44,6 +44,11 @@ class RenderDesc(ctypes.Structure):
                 ("reserved", ctypes.c_int * 7)]
 
 
+class Job(ctypes.Structure):
+    _fields_ = [("camera_json", ctypes.c_char_p), ("num_spp", ctypes.c_int), ("num_path_vertices", ctypes.c_int),
+                ("seed", ctypes.c_uint), ("reserved", ctypes.c_int * 3)]
+
+
 class RenderStats(ctypes.Structure):
     _fields_ = [("render_ms", ctypes.c_double), ("paths", ctypes.c_ulonglong), ("iterations", ctypes.c_ulonglong),
                 ("max_shadow_queue", ctypes.c_uint), ("queue_capacity", ctypes.c_uint),
@@ -69,7 +74,8 @@ class SceneInfo(ctypes.Structure):
 EXPORTS = ["wr_scene_create", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
-           "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc"]
+           "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
+           "wr_render_batch_device"]
 
 _lib = None
 
@@ -95,6 +101,8 @@ def load_library(path: str = LIB_PATH):
     L.wr_render.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_render_device.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_render_device_noalloc.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
+    L.wr_render_batch.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), fp]
+    L.wr_render_batch_device.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), fp]
     L.wr_get_render_stats.argtypes = [vp, ctypes.POINTER(RenderStats)]
     L.wr_trace_closest.argtypes = [vp, fp, ip, fp, fp, fp, fp]
     L.wr_trace_occluded.argtypes = [vp, fp, ip, fp]
@@ -194,6 +202,39 @@ class Scene:
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
                        profile)
         _check(load_library().wr_render_device(self._h, ctypes.byref(d), ctypes.c_void_p(int(out_device_ptr))))
+
+    def render_batch(self, jobs, queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0):
+        """jobs: list of dicts {camera (dict or JSON text), num_spp, num_path_vertices, seed}.
+        Returns one (H, W, 3) float64 image per job, rendered in one wavefront."""
+        import json as _json
+        n = len(jobs)
+        arr = (Job * n)()
+        keep = []
+        shapes = []
+        for i, j in enumerate(jobs):
+            cam = j.get("camera")
+            if isinstance(cam, dict):
+                cam = _json.dumps(cam)
+            if cam is not None:
+                keep.append(cam.encode())
+                arr[i].camera_json = keep[-1]
+                c = _json.loads(cam)
+                shapes.append((int(c["resolution"][1]), int(c["resolution"][0])))
+            else:
+                inf = self.info
+                shapes.append((inf["height"], inf["width"]))
+            arr[i].num_spp = int(j.get("num_spp", 0))
+            arr[i].num_path_vertices = int(j.get("num_path_vertices", 0))
+            arr[i].seed = int(j.get("seed", 0)) & 0xFFFFFFFF
+        total = sum(h * w for h, w in shapes)
+        out = np.empty(total * 3, np.float64)
+        d = self._desc(None, None, 0, 0, queue_capacity, grid_trace, grid_shade, use_graph, profile)
+        _check(load_library().wr_render_batch(self._h, arr, n, ctypes.byref(d), _ptr(out)))
+        imgs, off = [], 0
+        for h, w in shapes:
+            imgs.append(out[off * 3:(off + h * w) * 3].reshape(h, w, 3))
+            off += h * w
+        return imgs
 
     @property
     def stats(self) -> dict:

@@ -78,7 +78,8 @@ struct wr_scene {
     int bvh_nodes = 0, bvh_depth = 0;
     double sah_cost = 0.0, build_ms = 0.0;
     // wavefront buffers
-    DevBuf w_o[2], w_d[2], w_thr[2], w_meta[2], w_hit, w_sho, w_shd, w_shc, w_film, w_ctr, w_sample, w_out, w_prof;
+    DevBuf w_o[2], w_d[2], w_thr[2], w_meta[2], w_hit, w_sho, w_shd, w_shc, w_film, w_ctr, w_sample, w_out, w_prof,
+        w_jobs;
     std::vector<cudaEvent_t> kev;
     uint32_t w_capacity = 0;
     size_t w_npix = 0;
@@ -358,26 +359,46 @@ void ensure_wave(wr_scene &s, uint32_t capacity, size_t npix) {
     }
 }
 
-void render(wr_scene &s, const wr_render_desc *desc_in, double *out, bool out_on_host) {
-    wr_render_desc desc{};
-    if (desc_in) desc = *desc_in;
-    const wr::Scene &h = s.host;
-    if (!h.has_camera) throw Error(WR_ERR_INVALID_ARGUMENT, "scene has no camera");
-    wr::RenderEntry re;
-    if (desc.render_index < 0) throw Error(WR_ERR_INVALID_ARGUMENT, "render_index must be >= 0");
-    if (size_t(desc.render_index) < h.renders.size()) re = h.renders[desc.render_index];
-    const int spp = desc.num_spp > 0 ? desc.num_spp : re.num_spp;
-    const int nverts = desc.num_path_vertices > 0 ? desc.num_path_vertices : re.num_path_vertices;
-    if (spp <= 0) throw Error(WR_ERR_INVALID_ARGUMENT, "num_spp must be positive");
-    const wr::Camera &cam = h.camera;
-    const size_t npix = size_t(cam.width) * cam.height;
-    if (npix >= (1ull << 31)) throw Error(WR_ERR_UNSUPPORTED, "film too large");
+struct HostJob {
+    wr::Camera cam;
+    int spp = 16, nverts = 10;
+    uint32_t seed = 0;
+};
+
+// Renders a batch of jobs (one camera, spp and depth each) over the scene in one wavefront.
+// The images land in `out` (host or device) concatenated in job order.
+void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_desc &desc, double *out,
+                 bool out_on_host) {
+    if (jobs.empty()) throw Error(WR_ERR_INVALID_ARGUMENT, "no jobs");
+    std::vector<wrd::DevJob> table(jobs.size());
+    unsigned long long total = 0;
+    size_t total_pix = 0;
+    int max_nverts = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const HostJob &hj = jobs[j];
+        if (hj.spp <= 0) throw Error(WR_ERR_INVALID_ARGUMENT, "num_spp must be positive");
+        if (hj.cam.width <= 0 || hj.cam.height <= 0) throw Error(WR_ERR_INVALID_ARGUMENT, "resolution must be positive");
+        wrd::DevJob &d = table[j];
+        d = wrd::DevJob{};
+        d.cam = make_camera(hj.cam);
+        d.spp = hj.spp;
+        d.nverts = hj.nverts;
+        d.npix = uint32_t(size_t(hj.cam.width) * hj.cam.height);
+        d.pix_offset = uint32_t(total_pix);
+        d.sample_begin = total;
+        d.seed = hj.seed;
+        total += (unsigned long long)d.npix * unsigned(hj.spp);
+        total_pix += d.npix;
+        max_nverts = std::max(max_nverts, hj.nverts);
+        if (total_pix >= (1ull << 31)) throw Error(WR_ERR_UNSUPPORTED, "batch film larger than 2^31 pixels");
+        if (jobs.size() >= (1u << 24)) throw Error(WR_ERR_UNSUPPORTED, "more than 2^24 jobs");
+    }
     int sms = 148;
     WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
     uint32_t capacity = desc.queue_capacity > 0 ? uint32_t(desc.queue_capacity) : (1u << 21);
-    const unsigned long long total = (unsigned long long)npix * unsigned(spp);
     capacity = uint32_t(std::min<unsigned long long>(capacity, std::max<unsigned long long>(total, 1024ull)));
-    ensure_wave(s, capacity, npix);
+    ensure_wave(s, capacity, total_pix);
+    cudaStream_t st = s.stream;
 
     wrk::WaveBuffers b{};
     for (int p = 0; p < 2; ++p) {
@@ -397,133 +418,221 @@ void render(wr_scene &s, const wr_render_desc *desc_in, double *out, bool out_on
     b.shadow_capacity = 2 * capacity;
 
     wrk::RenderLaunch r{};
-    r.cam = make_camera(cam);
-    r.spp = spp;
-    r.nverts = nverts;
-    r.seed = desc.seed;
+    r.num_jobs = int(table.size());
+    r.job0 = table[0];
+    if (table.size() > 1) {
+        upload(s.w_jobs, table, st);
+        r.jobs = s.w_jobs.as<wrd::DevJob>();
+    }
+    r.total_pix = uint32_t(total_pix);
     r.total_samples = total;
+    const unsigned long long waves = (total + capacity - 1) / capacity;
+    r.iter_limit = uint32_t(std::min<unsigned long long>((waves + 2) * (unsigned long long)(max_nverts + 2) + 64,
+                                                         0xffffffffull));
     r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0));
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * std::max(1, wrk::occupancy_blocks(1));
 
-    cudaStream_t st = s.stream;
     const int profile = desc.profile;
     s.w_prof.alloc(16 * 8);
     r.prof = profile >= 2 ? s.w_prof.as<unsigned long long>() : nullptr;
     s.stats = wr_render_stats{};
-    WR_CUDA(cudaMemsetAsync(b.film, 0, npix * 6 * 8, st));
-    WR_CUDA(cudaMemsetAsync(b.ctr, 0, wrd::CTR_COUNT * 4, st));
-    WR_CUDA(cudaMemsetAsync(b.sample_next, 0, 8, st));
-    WR_CUDA(cudaMemsetAsync(s.w_prof.p, 0, 16 * 8, st));
-    WR_CUDA(cudaEventRecord(s.ev0, st));
-    unsigned long long iterations = 0, launches = 0;
-    if (nverts > 1) {
-        // upper bound on iterations: every sample needs at most nverts extensions
-        const unsigned long long waves = (total + capacity - 1) / capacity;
-        const unsigned long long limit = (waves + 2) * (unsigned long long)(nverts + 2) + 64;
-        if (profile) {
-            // one kernel at a time, bracketed by events, to attribute device time per kernel
-            if (s.kev.empty()) {
-                s.kev.resize(2);
-                for (auto &e : s.kev) WR_CUDA(cudaEventCreate(&e));
-            }
-            auto timed = [&](int which, int parity) {
-                WR_CUDA(cudaEventRecord(s.kev[0], st));
-                wrk::launch_kernel(which, s.dev, b, r, parity, st);
-                WR_CUDA(cudaGetLastError());
-                WR_CUDA(cudaEventRecord(s.kev[1], st));
-                WR_CUDA(cudaEventSynchronize(s.kev[1]));
-                float ms = 0.f;
-                WR_CUDA(cudaEventElapsedTime(&ms, s.kev[0], s.kev[1]));
-                s.stats.kernel_ms[which] += ms;
-                s.stats.kernel_count[which] += 1;
-                launches += 1;
-            };
+    double *dst = out_on_host ? s.w_out.as<double>() : out;
+    unsigned long long launches = 0;
+
+    auto clear = [&]() {
+        WR_CUDA(cudaMemsetAsync(b.film, 0, total_pix * 6 * 8, st));
+        WR_CUDA(cudaMemsetAsync(b.ctr, 0, wrd::CTR_COUNT * 4, st));
+        WR_CUDA(cudaMemsetAsync(b.sample_next, 0, 8, st));
+    };
+    const bool trace = max_nverts > 1;
+    if (profile) {
+        // one kernel at a time, bracketed by events, to attribute device time per kernel
+        WR_CUDA(cudaMemsetAsync(s.w_prof.p, 0, 16 * 8, st));
+        clear();
+        WR_CUDA(cudaEventRecord(s.ev0, st));
+        if (s.kev.empty()) {
+            s.kev.resize(2);
+            for (auto &e : s.kev) WR_CUDA(cudaEventCreate(&e));
+        }
+        auto timed = [&](int which, int parity) {
+            WR_CUDA(cudaEventRecord(s.kev[0], st));
+            if (which == wrk::KERNEL_RESOLVE) wrk::launch_resolve(b.film, dst, r, st);
+            else wrk::launch_kernel(which, s.dev, b, r, parity, st);
+            WR_CUDA(cudaGetLastError());
+            WR_CUDA(cudaEventRecord(s.kev[1], st));
+            WR_CUDA(cudaEventSynchronize(s.kev[1]));
+            float ms = 0.f;
+            WR_CUDA(cudaEventElapsedTime(&ms, s.kev[0], s.kev[1]));
+            s.stats.kernel_ms[which] += ms;
+            s.stats.kernel_count[which] += 1;
+            launches += 1;
+        };
+        if (trace) {
             timed(wrk::KERNEL_RAYGEN, 1);
             timed(wrk::KERNEL_SHADOW, 1);
             timed(wrk::KERNEL_ADVANCE, 1);
-            bool done = false;
             int parity = 0;
-            while (!done) {
+            while (true) {
                 for (int k : {wrk::KERNEL_EXTEND, wrk::KERNEL_SHADE, wrk::KERNEL_RAYGEN, wrk::KERNEL_SHADOW,
                               wrk::KERNEL_ADVANCE})
                     timed(k, parity);
                 parity ^= 1;
-                ++iterations;
                 WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
                 WR_CUDA(cudaStreamSynchronize(st));
-                done = s.pinned[wrd::CTR_DONE] != 0;
-                if (!done && iterations > limit) throw Error(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
+                if (s.pinned[wrd::CTR_DONE]) break;
             }
-        } else {
+        }
+        timed(wrk::KERNEL_RESOLVE, 0);
+        s.stats.kernel_items[wrk::KERNEL_RESOLVE] += total_pix;
+    } else if (desc.use_graph) {
+        // the whole render as one graph: clears, first wavefront, a while-loop node whose body is two
+        // bounce iterations (the bookkeeping kernel clears the condition when the wavefront drains
+        // or the iteration bound is reached), and the resolve
+        cudaGraph_t g = nullptr, gp = nullptr, gs = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        auto cleanup = [&]() {
+            if (ex) cudaGraphExecDestroy(ex);
+            if (g) cudaGraphDestroy(g);
+            if (gp) cudaGraphDestroy(gp);
+            if (gs) cudaGraphDestroy(gs);
+        };
+        try {
+            WR_CUDA(cudaGraphCreate(&g, 0));
+            cudaGraphConditionalHandle h{};
+            if (trace) {   // a handle must belong to a conditional node of the graph
+                WR_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+                r.cond = h;
+                r.has_cond = 1;
+            }
+            WR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            clear();
+            if (trace) wrk::launch_prime(s.dev, b, r, st);
+            WR_CUDA(cudaStreamEndCapture(st, &gp));
+            cudaGraphNode_t np, nw, ns;
+            WR_CUDA(cudaGraphAddChildGraphNode(&np, g, nullptr, 0, gp));
+            cudaGraphNode_t last = np;
+            if (trace) {
+                cudaGraphNodeParams cp{};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = h;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                WR_CUDA(cudaGraphAddNode(&nw, g, &np, 1, &cp));
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                WR_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+                wrk::launch_iteration(s.dev, b, r, 0, st);
+                wrk::launch_iteration(s.dev, b, r, 1, st);
+                WR_CUDA(cudaStreamEndCapture(st, &body));
+                last = nw;
+            }
+            WR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            wrk::launch_resolve(b.film, dst, r, st);
+            WR_CUDA(cudaStreamEndCapture(st, &gs));
+            WR_CUDA(cudaGraphAddChildGraphNode(&ns, g, &last, 1, gs));
+            WR_CUDA(cudaGraphInstantiate(&ex, g, 0));
+            WR_CUDA(cudaEventRecord(s.ev0, st));
+            WR_CUDA(cudaGraphLaunch(ex, st));
+            launches += 1;
+        } catch (...) {
+            cudaStreamCaptureStatus cs;
+            if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(st, &junk);
+                if (junk) cudaGraphDestroy(junk);
+            }
+            cleanup();
+            throw;
+        }
+        WR_CUDA(cudaEventRecord(s.ev1, st));
+        WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
+        const cudaError_t e = cudaStreamSynchronize(st);
+        cleanup();
+        if (e != cudaSuccess) throw Error(WR_ERR_CUDA, std::string("render graph: ") + cudaGetErrorString(e));
+    } else {
+        clear();
+        WR_CUDA(cudaEventRecord(s.ev0, st));
+        if (trace) {
             wrk::launch_prime(s.dev, b, r, st);
             WR_CUDA(cudaGetLastError());
             launches += 3;
-            cudaGraphExec_t exec = nullptr;
-            if (desc.use_graph) {
-                cudaGraph_t g;
-                WR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            while (true) {
                 wrk::launch_iteration(s.dev, b, r, 0, st);
                 wrk::launch_iteration(s.dev, b, r, 1, st);
-                WR_CUDA(cudaStreamEndCapture(st, &g));
-                WR_CUDA(cudaGraphInstantiate(&exec, g, 0));
-                cudaGraphDestroy(g);
-            }
-            bool done = false;
-            while (!done) {
-                if (exec) {
-                    WR_CUDA(cudaGraphLaunch(exec, st));
-                } else {
-                    wrk::launch_iteration(s.dev, b, r, 0, st);
-                    wrk::launch_iteration(s.dev, b, r, 1, st);
-                }
-                iterations += 2;
+                WR_CUDA(cudaGetLastError());
                 launches += 10;
                 WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
                 WR_CUDA(cudaStreamSynchronize(st));
-                done = s.pinned[wrd::CTR_DONE] != 0;
-                if (!done && iterations > limit) {
-                    if (exec) cudaGraphExecDestroy(exec);
-                    throw Error(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
-                }
+                if (s.pinned[wrd::CTR_DONE]) break;
             }
-            if (exec) WR_CUDA(cudaGraphExecDestroy(exec));
         }
-        if (s.pinned[wrd::CTR_OVERFLOW]) throw Error(WR_ERR_CUDA, "shadow queue overflow");
-        s.stats.max_shadow_queue = s.pinned[wrd::CTR_SHADOW_MAX];
+        wrk::launch_resolve(b.film, dst, r, st);
+        WR_CUDA(cudaGetLastError());
+        launches += 1;
     }
-    double *dst = out_on_host ? s.w_out.as<double>() : out;
-    if (profile) WR_CUDA(cudaEventRecord(s.kev[0], st));
-    wrk::launch_resolve(b.film, dst, uint32_t(npix), spp, st);
-    WR_CUDA(cudaGetLastError());
-    launches += 1;
-    WR_CUDA(cudaEventRecord(s.ev1, st));
-    if (out_on_host) WR_CUDA(cudaMemcpyAsync(out, dst, npix * 3 * 8, cudaMemcpyDeviceToHost, st));
+    if (!desc.use_graph || profile) WR_CUDA(cudaEventRecord(s.ev1, st));
+    WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
+    if (out_on_host) WR_CUDA(cudaMemcpyAsync(out, dst, total_pix * 3 * 8, cudaMemcpyDeviceToHost, st));
     WR_CUDA(cudaStreamSynchronize(st));
+    if (trace && s.pinned[wrd::CTR_TIMEOUT]) throw Error(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
+    if (trace && s.pinned[wrd::CTR_OVERFLOW]) throw Error(WR_ERR_CUDA, "shadow queue overflow");
     float ms = 0.f;
     WR_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
-    if (profile) {
-        float rms = 0.f;
-        WR_CUDA(cudaEventElapsedTime(&rms, s.kev[0], s.ev1));
-        s.stats.kernel_ms[wrk::KERNEL_RESOLVE] += rms;
-        s.stats.kernel_count[wrk::KERNEL_RESOLVE] += 1;
-        s.stats.kernel_items[wrk::KERNEL_RESOLVE] += npix;
+    if (profile >= 2) {
         unsigned long long prof[16];
         WR_CUDA(cudaMemcpy(prof, s.w_prof.p, sizeof(prof), cudaMemcpyDeviceToHost));
-        if (profile >= 2) {
-            for (int k = 0; k < 4; ++k) s.stats.kernel_items[k] = prof[k];
-            s.stats.extend_node_visits = prof[6];
-            s.stats.extend_tri_tests = prof[7];
-            s.stats.shadow_node_visits = prof[8];
-            s.stats.shadow_tri_tests = prof[9];
-        }
+        for (int k = 0; k < 4; ++k) s.stats.kernel_items[k] = prof[k];
+        s.stats.extend_node_visits = prof[6];
+        s.stats.extend_tri_tests = prof[7];
+        s.stats.shadow_node_visits = prof[8];
+        s.stats.shadow_tri_tests = prof[9];
     }
     s.stats.render_ms = ms;
     s.stats.paths = total;
-    s.stats.iterations = iterations;
+    s.stats.iterations = trace ? s.pinned[wrd::CTR_ITER] : 0;
+    // kernels per render: prime 3 + 5 per iteration + resolve (a graph launch runs the same kernels)
+    s.stats.kernel_launches = trace ? 3ull + 5ull * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
+    s.stats.max_shadow_queue = s.pinned[wrd::CTR_SHADOW_MAX];
     s.stats.queue_capacity = capacity;
     s.stats.grid_trace = r.grid_trace;
     s.stats.grid_shade = r.grid_shade;
-    s.stats.kernel_launches = launches;
+    (void)launches;
+}
+
+HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
+    if (!h.has_camera) throw Error(WR_ERR_INVALID_ARGUMENT, "scene has no camera");
+    if (desc.render_index < 0) throw Error(WR_ERR_INVALID_ARGUMENT, "render_index must be >= 0");
+    wr::RenderEntry re;
+    if (size_t(desc.render_index) < h.renders.size()) re = h.renders[desc.render_index];
+    HostJob j;
+    j.cam = h.camera;
+    j.spp = desc.num_spp > 0 ? desc.num_spp : re.num_spp;
+    j.nverts = desc.num_path_vertices > 0 ? desc.num_path_vertices : re.num_path_vertices;
+    j.seed = desc.seed;
+    return j;
+}
+
+void render(wr_scene &s, const wr_render_desc *desc_in, double *out, bool out_on_host) {
+    wr_render_desc desc{};
+    if (desc_in) desc = *desc_in;
+    render_jobs(s, {scene_job(s.host, desc)}, desc, out, out_on_host);
+}
+
+void render_batch(wr_scene &s, const wr_job *jobs, int n, const wr_render_desc *desc_in, double *out, bool on_host) {
+    if (n <= 0 || !jobs) throw Error(WR_ERR_INVALID_ARGUMENT, "empty job list");
+    wr_render_desc desc{};
+    if (desc_in) desc = *desc_in;
+    std::vector<HostJob> hj;
+    hj.reserve(size_t(n));
+    for (int i = 0; i < n; ++i) {
+        wr_render_desc d = desc;
+        d.num_spp = jobs[i].num_spp;
+        d.num_path_vertices = jobs[i].num_path_vertices;
+        d.seed = jobs[i].seed;
+        HostJob j = scene_job(s.host, d);
+        if (jobs[i].camera_json) j.cam = wr::parse_camera_json(jobs[i].camera_json);
+        hj.push_back(j);
+    }
+    render_jobs(s, hj, desc, out, on_host);
 }
 
 wrd::DevScene scene_for_queries(wr_scene &s) { return s.dev; }
@@ -705,6 +814,26 @@ int wr_render_device(wr_scene *s, const wr_render_desc *desc, double *out_rgb_de
     if (!s || !out_rgb_device) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
     try {
         render(*s, desc, out_rgb_device, false);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_render_batch(wr_scene *s, const wr_job *jobs, int n, const wr_render_desc *desc, double *out_rgb) {
+    if (!s || !out_rgb) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        render_batch(*s, jobs, n, desc, out_rgb, true);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_render_batch_device(wr_scene *s, const wr_job *jobs, int n, const wr_render_desc *desc, double *out_rgb_device) {
+    if (!s || !out_rgb_device) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        render_batch(*s, jobs, n, desc, out_rgb_device, false);
         return WR_OK;
     } catch (const Error &e) {
         return fail(e);

@@ -42,6 +42,7 @@ enum Counter {
     CTR_ITER = 4,        // iterations executed
     CTR_SHADOW_MAX = 5,  // largest shadow queue seen
     CTR_OVERFLOW = 6,    // shadow queue overflowed (not expected: its capacity is 2x the wavefront)
+    CTR_TIMEOUT = 7,     // the iteration bound was reached before the wavefront drained
     CTR_COUNT = 8
 };
 
@@ -70,6 +71,17 @@ struct DevCamera {
     float per_film, per_pixel;   // mPerFilmNormFactor, mPerPixelNormFactor
     float focal, aperture, inv_lens_area;
     int width, height;
+};
+
+// one render job of a batch: its camera, sample count and film slice
+struct DevJob {
+    DevCamera cam;
+    int spp, nverts;
+    uint32_t pix_offset;              // first pixel of this job in the batch film
+    uint32_t npix;
+    unsigned long long sample_begin;  // first global sample id of this job
+    uint32_t seed;
+    uint32_t pad;
 };
 
 struct DevScene {

@@ -276,7 +276,7 @@ __device__ __forceinline__ LightVtx sample_light(const DevScene &s, float u0, fl
 // ----------------------------------------------------------------- kernels ----
 struct PathState {
     float4 *o, *d, *thr;
-    uint32_t *meta;
+    uint32_t *meta;     // depth (bits 0-7) | job (bits 8-31)
 };
 
 struct ShadowQueue {
@@ -287,18 +287,45 @@ struct WaveArgs {
     PathState cur, nxt;
     float4 *hit;
     ShadowQueue sq;
-    double *film;          // base film (W*H*3) followed by the splat film (W*H*3)
-    uint32_t *ctr;         // device counters (wr_kernels.h)
+    double *film;          // base film (total_pix*3) followed by the splat film (total_pix*3)
+    uint32_t *ctr;         // device counters (Counter)
     unsigned long long *sample_next;
     unsigned long long total_samples;
     uint32_t capacity;
     uint32_t shadow_capacity;
-    DevCamera cam;
-    int spp, nverts;
-    uint32_t seed;
-    uint32_t npix;
+    const DevJob *jobs;    // job table in device memory, or nullptr: the single job `job0`
+    DevJob job0;
+    int num_jobs;
+    uint32_t total_pix;
+    uint32_t iter_limit;   // bookkeeping stops the loop after this many iterations
+    cudaGraphConditionalHandle cond;   // while-loop condition of the captured graph (0: none)
+    int has_cond;
     unsigned long long *prof;   // profiling totals (nullptr when off): items[6], extend nv/nt, shadow nv/nt
 };
+
+__device__ __forceinline__ const DevJob &job_at(const WaveArgs &w, uint32_t j) { return w.jobs ? w.jobs[j] : w.job0; }
+
+// job owning global sample `id`: last job whose sample_begin <= id
+__device__ __forceinline__ uint32_t job_of_sample(const WaveArgs &w, unsigned long long id) {
+    if (!w.jobs) return 0;
+    int lo = 0, hi = w.num_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&w.jobs[mid].sample_begin) <= id) lo = mid; else hi = mid - 1;
+    }
+    return uint32_t(lo);
+}
+
+__device__ __forceinline__ uint32_t job_of_pixel(const DevJob *jobs, int n, uint32_t pix) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&jobs[mid].pix_offset) <= pix) lo = mid; else hi = mid - 1;
+    }
+    return uint32_t(lo);
+}
+
+__device__ __forceinline__ uint32_t job_seed(const DevJob &J, uint32_t job) { return J.seed + job * 0x9E3779B9u; }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
@@ -322,6 +349,13 @@ __device__ __forceinline__ void push_shadow(const WaveArgs &w, bool pred, f3 o, 
         w.sq.d[idx] = make_float4(d.x, d.y, d.z, __uint_as_float(slot));
         w.sq.c[idx] = make_float4(c.x, c.y, c.z, 0.f);
     }
+}
+
+__device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c) {
+    double *f = w.film + ((slot & SPLAT_BIT) ? 3 * size_t(w.total_pix) : size_t(0)) + 3 * size_t(slot & ~SPLAT_BIT);
+    atomicAdd(f + 0, double(c.x));
+    atomicAdd(f + 1, double(c.y));
+    atomicAdd(f + 2, double(c.z));
 }
 
 __global__ void __launch_bounds__(kTraceBlock) k_extend(DevScene s, WaveArgs w) {
@@ -357,14 +391,16 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
         float stmax = 0.f;
         f3 no = mk(0, 0, 0), nd = mk(0, 0, 1), nthr = mk(0, 0, 0);
         float npdf = 0.f;
-        uint32_t pixel = 0, sample = 0, depth = 0;
+        uint32_t pixel = 0, sample = 0, meta = 0;
         if (valid) {
             const float4 o4 = w.cur.o[i], d4 = w.cur.d[i], t4 = w.cur.thr[i];
-            depth = w.cur.meta[i];
+            meta = w.cur.meta[i];
+            const uint32_t depth = meta & 0xffu, job = meta >> 8;
+            const DevJob &J = job_at(w, job);
             const float4 h = w.hit[i];
             const f3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
             const float prevPdfW = o4.w;
-            pixel = __float_as_uint(d4.w);
+            pixel = __float_as_uint(d4.w);   // global film pixel
             sample = __float_as_uint(t4.w);
             const uint32_t tri = __float_as_uint(h.w);
             const float t = h.x;
@@ -375,10 +411,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
                     const float lPdfA = s.env_select_pdf * env_pdf(s, d);
                     const float mis = cPdfA / (lPdfA + cPdfA);
                     const f3 c = thr * env_eval(s, d) * mis;
-                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
-                        double *f = w.film + 3 * size_t(pixel);
-                        atomicAdd(f + 0, double(c.x)); atomicAdd(f + 1, double(c.y)); atomicAdd(f + 2, double(c.z));
-                    }
+                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) film_add(w, pixel, c);
                 }
             } else {
                 const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
@@ -390,26 +423,22 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
                     // strategy B: BSDF-sampled hit on an emitter
                     const uint32_t li = mat & ~LIGHT_BIT;
                     const float cosl = dot(ng, d);
-                    if (cosl < 0.f) {   // front face: evalLe1 (diffusearealight.h:48-53)
+                    if (cosl <= 0.f) {   // front face: evalLe1 (diffusearealight.h:48-53)
                         const float cPdfA = prevPdfW * fabsf(cosl) / (t * t);
                         const float lPdfA = __ldg(&s.lights[li].select_pdf) * __ldg(&s.lights[li].inv_area);
                         const float mis = cPdfA / (lPdfA + cPdfA);
                         const f3 c = thr * mk(__ldg(&s.lights[li].intensity[0]), __ldg(&s.lights[li].intensity[1]),
                                               __ldg(&s.lights[li].intensity[2])) * mis;
-                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
-                            double *f = w.film + 3 * size_t(pixel);
-                            atomicAdd(f + 0, double(c.x)); atomicAdd(f + 1, double(c.y)); atomicAdd(f + 2, double(c.z));
-                        }
+                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) film_add(w, pixel, c);
                     }
-                } else if (int(depth) + 2 < w.nverts) {
-                    const DevMaterial &m = s.materials[mat];
-                    DevMaterial mm;
-                    mm = m;
+                } else if (int(depth) + 2 < J.nverts) {
+                    const DevMaterial mm = s.materials[mat];
                     const Frame fr(ng);
                     const f3 wi = -d;
                     const f3 inL = fr.to_local(wi);
+                    const uint32_t lpix = pixel - J.pix_offset, seed = job_seed(J, job);
                     // strategy A: next-event estimation toward this sample's light vertex
-                    const Rand4 r0 = rand4(pixel, sample, 0, w.seed);
+                    const Rand4 r0 = rand4(lpix, sample, 0, seed);
                     const LightVtx l = sample_light(s, r0.a, r0.b);
                     f3 wo;
                     float G, convA, dist = 0.f;
@@ -443,7 +472,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
                         }
                     }
                     // BSDF sampling continues the path
-                    const Rand4 rb = rand4(pixel, sample, 2 + depth, w.seed);
+                    const Rand4 rb = rand4(lpix, sample, 2 + depth, seed);
                     f3 outL;
                     float pdfW;
                     const f3 wgt = bsdf_sample(mm, inL, rb.a, rb.b, outL, pdfW);
@@ -464,21 +493,23 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
             w.nxt.o[j] = make_float4(no.x, no.y, no.z, npdf);
             w.nxt.d[j] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel));
             w.nxt.thr[j] = make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample));
-            w.nxt.meta[j] = depth + 1;
+            w.nxt.meta[j] = meta + 1u;
         }
     }
+}
+
+__device__ __forceinline__ uint32_t new_samples(const WaveArgs &w, uint32_t filled, unsigned long long issued) {
+    const unsigned long long remaining = w.total_samples > issued ? w.total_samples - issued : 0ull;
+    const uint32_t room = w.capacity > filled ? w.capacity - filled : 0u;
+    return uint32_t(remaining < room ? remaining : room);
 }
 
 // new camera samples into the free tail of the next wavefront
 __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) {
     const uint32_t filled = w.ctr[CTR_NEXT];
     const unsigned long long issued = *w.sample_next;
-    const unsigned long long remaining = w.total_samples - issued;
-    const uint32_t room = w.capacity > filled ? w.capacity - filled : 0u;
-    const uint32_t n_new = uint32_t(remaining < room ? remaining : room);
+    const uint32_t n_new = new_samples(w, filled, issued);
     if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 2, (unsigned long long)n_new);
-    const DevCamera &cam = w.cam;
-    const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), cfz = ld3(cam.fz), corg = ld3(cam.origin);
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t base = warp_global * 32u; base < n_new; base += nwarps * 32u) {
@@ -490,15 +521,21 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
         uint32_t slot = 0;
         if (valid) {
             const unsigned long long id = issued + k;
-            const uint32_t pixel = uint32_t(id % w.npix);
-            const uint32_t sample = uint32_t(id / w.npix);
-            const uint32_t px = pixel % uint32_t(cam.width), py = pixel / uint32_t(cam.width);
-            const Rand4 r0 = rand4(pixel, sample, 0, w.seed);
+            const uint32_t job = job_of_sample(w, id);
+            const DevJob &J = job_at(w, job);
+            const DevCamera &cam = J.cam;
+            const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), cfz = ld3(cam.fz), corg = ld3(cam.origin);
+            const unsigned long long lid = id - J.sample_begin;
+            const uint32_t lpix = uint32_t(lid % J.npix);
+            const uint32_t sample = uint32_t(lid / J.npix);
+            const uint32_t seed = job_seed(J, job);
+            const uint32_t px = lpix % uint32_t(cam.width), py = lpix / uint32_t(cam.width);
+            const Rand4 r0 = rand4(lpix, sample, 0, seed);
             const LightVtx l = sample_light(s, r0.a, r0.b);
             // camera vertex: lens point (pinhole when the aperture is zero)
             f3 c0 = corg;
             if (cam.aperture > 0.f) {
-                const Rand4 r1 = rand4(pixel, sample, 1, w.seed);
+                const Rand4 r1 = rand4(lpix, sample, 1, seed);
                 const float ax = 2.f * r1.a - 1.f, ay = 2.f * r1.b - 1.f;
                 float rr = 0.f, phi = 0.f;
                 if (ax != 0.f || ay != 0.f) {
@@ -547,7 +584,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
                         const uint32_t sy = min(uint32_t(ry), uint32_t(cam.height - 1));
                         if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
                             shadow = true;
-                            slot = (sy * uint32_t(cam.width) + sx) | SPLAT_BIT;
+                            slot = (J.pix_offset + sy * uint32_t(cam.width) + sx) | SPLAT_BIT;
                             sc = c;
                             if (l.env) { so = c0; sd = wl; stmax = __int_as_float(0x7f800000); }
                             else { so = l.pos; sd = -wl; stmax = len - kRayEps; }
@@ -562,13 +599,13 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
             const f3 cpl = mk(dot(c0 - corg, cfx), dot(c0 - corg, cfy), dot(c0 - corg, cfz));
             const f3 dir = normalize(fpp - cpl);
             const float ct = dir.z;
-            const float pdfW = cam.per_film / (ct * ct * ct) / float(w.npix);
+            const float pdfW = cam.per_film / (ct * ct * ct) / float(J.npix);
             const f3 dw = normalize(cfx * dir.x + cfy * dir.y + cfz * dir.z);
             const uint32_t j = filled + k;
             w.nxt.o[j] = make_float4(c0.x, c0.y, c0.z, pdfW);
-            w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(pixel));
+            w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(J.pix_offset + lpix));
             w.nxt.thr[j] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sample));
-            w.nxt.meta[j] = 0u;
+            w.nxt.meta[j] = job << 8;
         }
         push_shadow(w, shadow, so, sd, stmax, slot, sc);
     }
@@ -587,11 +624,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shadow(DevScene s, WaveArgs w) 
         const bool occ = traverse<true>(s.nodes, s.tris, xyz(o), xyz(d), kRayEps, o.w, stack, t, tri, bu, bv, pv, pt);
         if (!occ) {
             const float4 c = w.sq.c[i];
-            const uint32_t slot = __float_as_uint(d.w);
-            double *f = w.film + ((slot & SPLAT_BIT) ? 3 * size_t(w.npix) : size_t(0)) + 3 * size_t(slot & ~SPLAT_BIT);
-            atomicAdd(f + 0, double(c.x));
-            atomicAdd(f + 1, double(c.y));
-            atomicAdd(f + 2, double(c.z));
+            film_add(w, __float_as_uint(d.w), mk(c.x, c.y, c.z));
         }
     }
     if (w.prof) {
@@ -600,30 +633,39 @@ __global__ void __launch_bounds__(kTraceBlock) k_shadow(DevScene s, WaveArgs w) 
     }
 }
 
-// queue bookkeeping between iterations (one thread)
+// queue bookkeeping between iterations (one thread); also drives the graph's while loop
 __global__ void k_advance(WaveArgs w) {
     const uint32_t filled = w.ctr[CTR_NEXT];
     const unsigned long long issued = *w.sample_next;
-    const unsigned long long remaining = w.total_samples - issued;
-    const uint32_t room = w.capacity > filled ? w.capacity - filled : 0u;
-    const uint32_t n_new = uint32_t(remaining < room ? remaining : room);
+    const uint32_t n_new = new_samples(w, filled, issued);
     if (w.ctr[CTR_SHADOW] > w.ctr[CTR_SHADOW_MAX]) w.ctr[CTR_SHADOW_MAX] = w.ctr[CTR_SHADOW];
     if (w.ctr[CTR_SHADOW] > w.shadow_capacity) w.ctr[CTR_OVERFLOW] = 1;
     w.ctr[CTR_ACTIVE] = filled + n_new;
     w.ctr[CTR_NEXT] = 0;
     w.ctr[CTR_SHADOW] = 0;
-    w.ctr[CTR_ITER] += 1;
+    const uint32_t iter = w.ctr[CTR_ITER] + 1;
+    w.ctr[CTR_ITER] = iter;
     *w.sample_next = issued + n_new;
-    w.ctr[CTR_DONE] = (filled + n_new == 0u) ? 1u : 0u;
+    bool done = filled + n_new == 0u;
+    if (!done && iter >= w.iter_limit) {   // never loop unbounded: stop and report
+        w.ctr[CTR_TIMEOUT] = 1;
+        done = true;
+    }
+    w.ctr[CTR_DONE] = done ? 1u : 0u;
+    if (w.has_cond) cudaGraphSetConditional(w.cond, done ? 0u : 1u);
 }
 
-// final image = base / spp + splat / (spp * W * H)   (film.h:70-90)
-__global__ void k_resolve(const double *film, double *out, uint32_t npix, int spp) {
-    const double bs = 1.0 / double(spp), as = 1.0 / double(spp) / double(npix);
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 3 * size_t(npix); i += size_t(gridDim.x) * blockDim.x) {
+// final image = base / spp + splat / (spp * W * H) per job (film.h:70-90)
+__global__ void k_resolve(const double *film, double *out, uint32_t total_pix, const DevJob *jobs, int njobs,
+                          DevJob job0) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 3 * size_t(total_pix);
+         i += size_t(gridDim.x) * blockDim.x) {
+        const uint32_t pix = uint32_t(i / 3);
+        const DevJob &J = jobs ? jobs[job_of_pixel(jobs, njobs, pix)] : job0;
+        const double bs = 1.0 / double(J.spp), as = 1.0 / double(J.spp) / double(J.npix);
         double c = 0.0;
         c += film[i] * bs;
-        c += film[3 * size_t(npix) + i] * as;
+        c += film[3 * size_t(total_pix) + i] * as;
         out[i] = c;
     }
 }
@@ -740,11 +782,13 @@ static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &
     w.total_samples = r.total_samples;
     w.capacity = b.capacity;
     w.shadow_capacity = b.shadow_capacity;
-    w.cam = r.cam;
-    w.spp = r.spp;
-    w.nverts = r.nverts;
-    w.seed = r.seed;
-    w.npix = uint32_t(r.cam.width) * uint32_t(r.cam.height);
+    w.jobs = r.jobs;
+    w.job0 = r.job0;
+    w.num_jobs = r.num_jobs;
+    w.total_pix = r.total_pix;
+    w.iter_limit = r.iter_limit;
+    w.cond = r.cond;
+    w.has_cond = r.has_cond;
     w.prof = r.prof;
     return w;
 }
@@ -768,12 +812,15 @@ void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunc
 }
 
 void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st) {
-    // the first wavefront: raygen into buffer 0 (parity 1 makes buffer 0 the "next" one), then bookkeeping
-    for (int k : {KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE}) launch_kernel(k, s, b, r, 1, st);
+    // the first wavefront: raygen into buffer 0 (parity 1 makes buffer 0 the "next" one), then bookkeeping;
+    // the graph condition is not touched here (it is only set inside the loop body)
+    RenderLaunch r0 = r;
+    r0.has_cond = 0;
+    for (int k : {KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE}) launch_kernel(k, s, b, r0, 1, st);
 }
 
-void launch_resolve(const double *film, double *out, uint32_t npix, int spp, cudaStream_t st) {
-    k_resolve<<<592, 256, 0, st>>>(film, out, npix, spp);
+void launch_resolve(const double *film, double *out, const RenderLaunch &r, cudaStream_t st) {
+    k_resolve<<<592, 256, 0, st>>>(film, out, r.total_pix, r.jobs, r.num_jobs, r.job0);
 }
 
 void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,

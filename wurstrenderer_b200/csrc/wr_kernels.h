@@ -22,11 +22,15 @@ struct WaveBuffers {
 };
 
 struct RenderLaunch {
-    wrd::DevCamera cam;
-    int spp, nverts;
-    uint32_t seed;
+    const wrd::DevJob *jobs;    // device job table (nullptr: the single job `job0`)
+    wrd::DevJob job0;
+    int num_jobs;
+    uint32_t total_pix;         // film pixels over all jobs
     unsigned long long total_samples;
+    uint32_t iter_limit;        // the loop stops (and reports CTR_TIMEOUT) after this many iterations
     int grid_trace, grid_shade;
+    cudaGraphConditionalHandle cond;   // while-loop condition when the loop body is captured in a graph
+    int has_cond;
     unsigned long long *prof;   // device profiling totals or nullptr
 };
 
@@ -37,7 +41,7 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
                    cudaStream_t st);
 void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st);
 void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity, cudaStream_t st);
-void launch_resolve(const double *film, double *out, uint32_t npix, int spp, cudaStream_t st);
+void launch_resolve(const double *film, double *out, const RenderLaunch &r, cudaStream_t st);
 void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,
                         int grid, cudaStream_t st);
 void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t ntables, float *cdf, float *pdf,

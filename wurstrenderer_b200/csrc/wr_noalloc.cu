@@ -150,13 +150,23 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
     int sms = 148;
     NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v.device));
     wrk::RenderLaunch r{};
-    r.cam = wr_internal::camera_constants(h.camera);
-    r.spp = spp;
-    r.nverts = nverts;
-    r.seed = desc.seed;
+    r.jobs = nullptr;
+    r.num_jobs = 1;
+    r.job0 = wrd::DevJob{};
+    r.job0.cam = wr_internal::camera_constants(h.camera);
+    r.job0.spp = spp;
+    r.job0.nverts = nverts;
+    r.job0.npix = uint32_t(npix);
+    r.job0.pix_offset = 0;
+    r.job0.sample_begin = 0;
+    r.job0.seed = desc.seed;
+    r.total_pix = uint32_t(npix);
     r.total_samples = (unsigned long long)npix * unsigned(spp);
+    const unsigned long long waves = (r.total_samples + kCapacity - 1) / kCapacity;
+    r.iter_limit = uint32_t((waves + 2) * (unsigned long long)(nverts + 2) + 64);
     r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * (wrk::occupancy_blocks(0) > 0 ? wrk::occupancy_blocks(0) : 1);
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * (wrk::occupancy_blocks(1) > 0 ? wrk::occupancy_blocks(1) : 1);
+    r.has_cond = 0;
     r.prof = nullptr;
 
     cudaStream_t st = v.stream;
@@ -166,8 +176,6 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
     NA_CUDA(cudaEventRecord(v.ev0, st));
     unsigned long long iterations = 0, launches = 0;
     if (nverts > 1) {
-        const unsigned long long waves = (r.total_samples + kCapacity - 1) / kCapacity;
-        const unsigned long long limit = (waves + 2) * (unsigned long long)(nverts + 2) + 64;
         wrk::launch_prime(v.dev, b, r, st);
         NA_CUDA(cudaGetLastError());
         launches += 3;
@@ -181,14 +189,14 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
             NA_CUDA(cudaMemcpyAsync(v.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
             NA_CUDA(cudaStreamSynchronize(st));
             done = v.pinned[wrd::CTR_DONE] != 0;
-            if (!done && iterations > limit) {
-                if (prev != v.device) cudaSetDevice(prev);
-                return fail(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
-            }
+        }
+        if (v.pinned[wrd::CTR_TIMEOUT]) {
+            if (prev != v.device) cudaSetDevice(prev);
+            return fail(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
         }
         if (v.pinned[wrd::CTR_OVERFLOW]) return fail(WR_ERR_CUDA, "shadow queue overflow");
     }
-    wrk::launch_resolve(b.film, out_rgb_device, uint32_t(npix), spp, st);
+    wrk::launch_resolve(b.film, out_rgb_device, r, st);
     NA_CUDA(cudaGetLastError());
     launches += 1;
     NA_CUDA(cudaEventRecord(v.ev1, st));
