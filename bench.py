@@ -34,6 +34,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "heightfield_spheres_1M: 1024x512, 64 spp, num_path_vertices 18 (max depth 16), 1,162,250 triangles"
+WORKLOAD_JOBS = ("jobs128: 128 jobs over the 36-triangle Cornell box, random cameras, resolutions {64,128,256,512}^2, "
+                 "spp log-uniform in [4, 256], num_path_vertices 14, one wavefront / one graph launch per step")
 METRIC = "Mpaths/s"
 
 
@@ -44,13 +46,19 @@ def env_int(k, d):
         return d
 
 
-def scene_path(rank, world, dist):
+def scene_path(rank, world, dist, workload="heightfield"):
     """Writes the seeded workload once per node (rank 0), shared by the other ranks."""
     from wurstrenderer_b200 import scenes
-    d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_v1")
-    p = os.path.join(d, "heightfield_spheres.json")
+    if workload == "jobs128":
+        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_cornell_v1")
+        p = os.path.join(d, "cornell.json")
+        writer = lambda: scenes.write_cornell(d)
+    else:
+        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_v1")
+        p = os.path.join(d, "heightfield_spheres.json")
+        writer = lambda: scenes.write_heightfield_spheres(d)
     if rank == 0 and not os.path.exists(p + ".done"):
-        scenes.write_heightfield_spheres(d)
+        writer()
         open(p + ".done", "w").write("ok")
     if world > 1:
         dist.barrier()
@@ -206,6 +214,10 @@ def main():
     ap.add_argument("--queue-capacity", type=int, default=0)
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs only)")
     ap.add_argument("--quick", action="store_true", help="skip e2e, profile and CPU baseline (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true", help="use the default wavefront settings")
+    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128"],
+                    help="heightfield: the 1M-triangle single render (headline); jobs128: 128 batched jobs "
+                         "over the Cornell box, one graph launch per step")
     args = ap.parse_args()
 
     world = env_int("WORLD_SIZE", 1)
@@ -227,7 +239,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     wr.set_device(local_rank)
-    path = scene_path(rank, world, dist)
+    path = scene_path(rank, world, dist, args.workload)
 
     t0 = time.perf_counter()
     scene = wr.Scene.from_file(path)
@@ -239,10 +251,31 @@ def main():
         spp = args.spp
     film = torch.empty((H, W, 3), dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
-    qc = args.queue_capacity or None
+    tune = {}
+    tune_ms = None
+    if not args.no_autotune:
+        tune, tune_ms = scene.autotune(probe_spp=4)
+        tune = {k: v for k, v in tune.items() if k != "use_graph"}
+    if args.queue_capacity:
+        tune["queue_capacity"] = args.queue_capacity
+    qc = tune.get("queue_capacity")
+    knobs = dict(grid_trace=tune.get("grid_trace"), grid_shade=tune.get("grid_shade"),
+                 trace_block=tune.get("trace_block"))
+
+    batch_jobs = None
+    if args.workload == "jobs128":
+        from wurstrenderer_b200 import scenes
+        batch_jobs = scenes.batch_jobs(seed=1003, n_jobs=128, num_path_vertices=14)
+        paths_batch = sum(j["camera"]["resolution"][0] * j["camera"]["resolution"][1] * j["num_spp"]
+                          for j in batch_jobs)
 
     def step(seed):
-        scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc)
+        if batch_jobs is not None:
+            for k, j in enumerate(batch_jobs):
+                j["seed"] = seed + k
+            scene.render_batch(batch_jobs, queue_capacity=qc, **knobs)
+            return scene.stats
+        scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc, **knobs)
         st = scene.stats
         if world > 1:
             dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
@@ -275,7 +308,7 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
-    paths_per_rank = W * H * spp
+    paths_per_rank = W * H * spp if batch_jobs is None else paths_batch
     value = paths_per_rank * world * args.steps / (max_ms / 1e3) / 1e6
 
     if args.quick:
@@ -293,7 +326,10 @@ def main():
     for i in range(args.steps):
         torch.cuda.synchronize()
         a = time.perf_counter()
-        scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc)
+        if batch_jobs is not None:
+            step(424242 + 1000 * i)
+        else:
+            scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc, **knobs)
         e2e_ms += (time.perf_counter() - a) * 1e3
     e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -301,7 +337,12 @@ def main():
     e2e_value = paths_per_rank * world * args.steps / (float(e2e_t.item()) / 1e3) / 1e6
 
     # one profiled render (per-kernel events + traversal counters) for the roofline, outside the timed region
-    scene.render_device(film.data_ptr(), spp=spp, seed=99, queue_capacity=qc, profile=2)
+    if batch_jobs is not None:
+        for k, j in enumerate(batch_jobs):
+            j["seed"] = 99 + k
+        scene.render_batch(batch_jobs, queue_capacity=qc, profile=2, **knobs)
+    else:
+        scene.render_device(film.data_ptr(), spp=spp, seed=99, queue_capacity=qc, profile=2, **knobs)
     prof = scene.stats
     kn = wr.KERNELS
     k_ms = dict(zip(kn, prof["kernel_ms"]))
@@ -325,22 +366,28 @@ def main():
                 "tri_tests_per_ray": nt / max(1, rays),
                 "kernel_share": {k: k_ms[k] / max(1e-9, sum(k_ms.values())) for k in kn}}
 
+    if batch_jobs is None:
+        h2d, d2h = 104, W * H * 3 * 8     # render request (camera, spp, seed) in, FP64 film out
+    else:
+        h2d = 160 * len(batch_jobs)       # job table (camera + spp + depth + offsets per job)
+        d2h = sum(j["camera"]["resolution"][0] * j["camera"]["resolution"][1] * 24 for j in batch_jobs)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 film + CDF build)", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": WORKLOAD, "parallelism": "replicas x%d, FP64 film reduce" % world,
+            "config": {"workload": WORKLOAD if batch_jobs is None else WORKLOAD_JOBS,
+                       "parallelism": "replicas x%d, FP64 film reduce" % world,
+                       "autotuned": tune, "autotune_probe_ms": tune_ms,
                        "l2": "256 MB buffer written between timed steps; path state > L2",
                        "queue_capacity": prof["queue_capacity"], "grid_trace": prof["grid_trace"],
                        "grid_shade": prof["grid_shade"], "scene_load_s": load_s,
                        "bvh_nodes": info["bvh_nodes"], "bvh_depth": info["bvh_depth"],
                        "iterations_per_step": iters / args.steps, "wall_ms_per_step": wall_ms / args.steps},
-            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 104,
-                    "d2h_bytes_per_step": W * H * 3 * 8},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roofline,
             "clocks": clk,
             "mrays_per_s": (k_items["extend"] + k_items["shadow"]) * world * args.steps / (max_ms / 1e3) / 1e6}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and batch_jobs is None:
         line["cpu_baseline"] = cpu_baseline(path)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -48,7 +48,8 @@ typedef struct wr_render_desc {
                                 bounce iterations); 0: host-driven launches */
     int profile;             /* 0: off; 1: per-kernel CUDA-event timing (plain launches);
                                 2: timing + traversal counters (node visits, triangle tests) */
-    int reserved[7];
+    int trace_block;         /* threads per block of the traversal kernels: 64, 128 or 256; 0 = 128 */
+    int reserved[6];
 } wr_render_desc;
 
 typedef struct wr_render_stats {
@@ -57,7 +58,8 @@ typedef struct wr_render_stats {
     unsigned long long iterations;    /* wavefront iterations executed */
     unsigned int max_shadow_queue;    /* largest shadow-ray queue seen */
     unsigned int queue_capacity;      /* wavefront slots used */
-    int grid_trace, grid_shade;
+    int grid_trace, grid_shade;       /* persistent blocks used */
+    int trace_block;                  /* threads per traversal block used */
     unsigned long long kernel_launches;   /* kernels launched by the render */
     /* per-kernel totals, filled when desc.profile != 0 (index: WR_K_*) */
     double kernel_ms[6];
@@ -148,6 +150,14 @@ int wr_get_render_stats(const wr_scene *scene, wr_render_stats *stats);
  * overlap on the GPU race; the first call on a device resolves the array's
  * address and should precede any stream capture. */
 int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc, double *out_rgb_device);
+
+/* Autotuner (no counterpart in the reference): times short renders of the
+ * scene's camera at probe_spp samples per pixel over traversal block sizes
+ * {64, 128, 256}, wavefront capacities {2^19 .. 2^22} and persistent-CTA counts
+ * {1/2, 1} x the occupancy limit (coordinate descent, starting from `base`), and
+ * writes the fastest settings into *best (other fields copied from base) and
+ * its time per render into *best_ms. */
+int wr_autotune(wr_scene *scene, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms);
 
 /* Closest-hit queries (EmbreeAccel::intersectTriangleInfo,
  * src/accel/embreeaccel.h:425-464). rays: n x 8 floats

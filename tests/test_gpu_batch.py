@@ -57,3 +57,23 @@ def test_batch_job_matches_oracle(wr_lib, oracle_lib):
     osc.set_camera(jobs[1]["camera"])
     ref, _, _ = osc.render(spp=1024, num_path_vertices=14, threads=0)
     assert abs(imgs[1].mean() / ref.mean() - 1.0) < 0.03
+
+
+def test_autotune_returns_valid_settings(wr_lib):
+    path, _ = golden_scene("zoo")
+    with wr_lib.Scene.from_file(path) as sc:
+        best, ms = sc.autotune(probe_spp=2)
+        assert best["trace_block"] in (0, 64, 128, 256)
+        assert ms > 0
+        a = sc.render(spp=32, seed=5, **{k: v for k, v in best.items() if k != "use_graph"})
+        b = sc.render(spp=32, seed=5)
+    assert np.allclose(a, b, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("block", [64, 256])
+def test_traversal_block_sizes_agree(wr_lib, block):
+    path, _ = golden_scene("hf")
+    with wr_lib.Scene.from_file(path) as sc:
+        a = sc.render(spp=16, seed=2, trace_block=block)
+        b = sc.render(spp=16, seed=2)
+    assert np.allclose(a, b, rtol=1e-9, atol=1e-12)

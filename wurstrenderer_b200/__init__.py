@@ -41,7 +41,7 @@ class RenderDesc(ctypes.Structure):
     _fields_ = [("num_spp", ctypes.c_int), ("num_path_vertices", ctypes.c_int), ("seed", ctypes.c_uint),
                 ("render_index", ctypes.c_int), ("queue_capacity", ctypes.c_int), ("grid_trace", ctypes.c_int),
                 ("grid_shade", ctypes.c_int), ("use_graph", ctypes.c_int), ("profile", ctypes.c_int),
-                ("reserved", ctypes.c_int * 7)]
+                ("trace_block", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 class Job(ctypes.Structure):
@@ -52,7 +52,7 @@ class Job(ctypes.Structure):
 class RenderStats(ctypes.Structure):
     _fields_ = [("render_ms", ctypes.c_double), ("paths", ctypes.c_ulonglong), ("iterations", ctypes.c_ulonglong),
                 ("max_shadow_queue", ctypes.c_uint), ("queue_capacity", ctypes.c_uint),
-                ("grid_trace", ctypes.c_int), ("grid_shade", ctypes.c_int),
+                ("grid_trace", ctypes.c_int), ("grid_shade", ctypes.c_int), ("trace_block", ctypes.c_int),
                 ("kernel_launches", ctypes.c_ulonglong), ("kernel_ms", ctypes.c_double * 6),
                 ("kernel_count", ctypes.c_ulonglong * 6), ("kernel_items", ctypes.c_ulonglong * 6),
                 ("extend_node_visits", ctypes.c_ulonglong), ("extend_tri_tests", ctypes.c_ulonglong),
@@ -75,7 +75,7 @@ EXPORTS = ["wr_scene_create", "wr_scene_create_from_json", "wr_scene_destroy", "
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
-           "wr_render_batch_device"]
+           "wr_render_batch_device", "wr_autotune"]
 
 _lib = None
 
@@ -102,6 +102,8 @@ def load_library(path: str = LIB_PATH):
     L.wr_render_device.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_render_device_noalloc.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_render_batch.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), fp]
+    L.wr_autotune.argtypes = [vp, ctypes.POINTER(RenderDesc), ip, ctypes.POINTER(RenderDesc),
+                              ctypes.POINTER(ctypes.c_double)]
     L.wr_render_batch_device.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), fp]
     L.wr_get_render_stats.argtypes = [vp, ctypes.POINTER(RenderStats)]
     L.wr_trace_closest.argtypes = [vp, fp, ip, fp, fp, fp, fp]
@@ -172,7 +174,7 @@ class Scene:
 
     @staticmethod
     def _desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-              profile=0):
+              profile=0, trace_block=None):
         d = RenderDesc()
         d.num_spp = int(spp or 0)
         d.num_path_vertices = int(num_path_vertices or 0)
@@ -183,27 +185,40 @@ class Scene:
         d.grid_shade = int(grid_shade or 0)
         d.use_graph = 1 if use_graph else 0
         d.profile = int(profile)
+        d.trace_block = int(trace_block or 0)
         return d
 
     def render(self, spp=None, num_path_vertices=None, seed=0, render_index=0, queue_capacity=None,
-               grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0) -> np.ndarray:
+               grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0, trace_block=None) -> np.ndarray:
         """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top)."""
         inf = self.info
         if out is None:
             out = np.empty((inf["height"], inf["width"], 3), np.float64)
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-                       profile)
+                       profile, trace_block)
         _check(load_library().wr_render(self._h, ctypes.byref(d), _ptr(out)))
         return out
 
     def render_device(self, out_device_ptr: int, spp=None, num_path_vertices=None, seed=0, render_index=0,
-                      queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0) -> None:
+                      queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
+                      trace_block=None) -> None:
         """Renders into device memory at `out_device_ptr` (W*H*3 doubles)."""
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-                       profile)
+                       profile, trace_block)
         _check(load_library().wr_render_device(self._h, ctypes.byref(d), ctypes.c_void_p(int(out_device_ptr))))
 
-    def render_batch(self, jobs, queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0):
+    def autotune(self, probe_spp=4, **base):
+        """Runs the library's autotuner; returns (settings dict, ms per probe render)."""
+        d0 = self._desc(None, None, 0, 0, base.get("queue_capacity"), base.get("grid_trace"), base.get("grid_shade"),
+                        base.get("use_graph", True), 0, base.get("trace_block"))
+        best = RenderDesc()
+        ms = ctypes.c_double(0.0)
+        _check(load_library().wr_autotune(self._h, ctypes.byref(d0), int(probe_spp), ctypes.byref(best), ctypes.byref(ms)))
+        keys = ("queue_capacity", "grid_trace", "grid_shade", "trace_block", "use_graph")
+        return {k: getattr(best, k) for k in keys}, ms.value
+
+    def render_batch(self, jobs, queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
+                     trace_block=None):
         """jobs: list of dicts {camera (dict or JSON text), num_spp, num_path_vertices, seed}.
         Returns one (H, W, 3) float64 image per job, rendered in one wavefront."""
         import json as _json
@@ -228,7 +243,7 @@ class Scene:
             arr[i].seed = int(j.get("seed", 0)) & 0xFFFFFFFF
         total = sum(h * w for h, w in shapes)
         out = np.empty(total * 3, np.float64)
-        d = self._desc(None, None, 0, 0, queue_capacity, grid_trace, grid_shade, use_graph, profile)
+        d = self._desc(None, None, 0, 0, queue_capacity, grid_trace, grid_shade, use_graph, profile, trace_block)
         _check(load_library().wr_render_batch(self._h, arr, n, ctypes.byref(d), _ptr(out)))
         imgs, off = [], 0
         for h, w in shapes:

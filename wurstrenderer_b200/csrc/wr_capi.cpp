@@ -429,7 +429,8 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     const unsigned long long waves = (total + capacity - 1) / capacity;
     r.iter_limit = uint32_t(std::min<unsigned long long>((waves + 2) * (unsigned long long)(max_nverts + 2) + 64,
                                                          0xffffffffull));
-    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0));
+    r.trace_block = (desc.trace_block == 64 || desc.trace_block == 256) ? desc.trace_block : 128;
+    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block));
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * std::max(1, wrk::occupancy_blocks(1));
 
     const int profile = desc.profile;
@@ -595,6 +596,7 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     s.stats.queue_capacity = capacity;
     s.stats.grid_trace = r.grid_trace;
     s.stats.grid_shade = r.grid_shade;
+    s.stats.trace_block = r.trace_block;
     (void)launches;
 }
 
@@ -834,6 +836,70 @@ int wr_render_batch_device(wr_scene *s, const wr_job *jobs, int n, const wr_rend
     if (!s || !out_rgb_device) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
     try {
         render_batch(*s, jobs, n, desc, out_rgb_device, false);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms) {
+    if (!s || !best) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        wr_render_desc cur{};
+        if (base) cur = *base;
+        cur.num_spp = probe_spp > 0 ? probe_spp : 4;
+        cur.profile = 0;
+        const wr::Camera &c = s->host.camera;
+        if (!s->host.has_camera) throw Error(WR_ERR_INVALID_ARGUMENT, "scene has no camera");
+        DevBuf out;
+        out.alloc(size_t(c.width) * c.height * 3 * 8);
+        int sms = 148;
+        WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+        auto trial = [&](const wr_render_desc &d) {
+            render(*s, &d, out.as<double>(), false);   // warm (allocations, caches)
+            double t = 0.0;
+            for (int k = 0; k < 2; ++k) {
+                render(*s, &d, out.as<double>(), false);
+                t += s->stats.render_ms;
+            }
+            return t / 2.0;
+        };
+        double bt = trial(cur);
+        // 1) traversal block size (its persistent grid follows the occupancy of that size)
+        for (int blk : {64, 128, 256}) {
+            wr_render_desc d = cur;
+            d.trace_block = blk;
+            d.grid_trace = 0;
+            const double t = trial(d);
+            if (t < bt) { bt = t; cur = d; }
+        }
+        // 2) wavefront capacity
+        for (int cap : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
+            wr_render_desc d = cur;
+            d.queue_capacity = cap;
+            const double t = trial(d);
+            if (t < bt) { bt = t; cur = d; }
+        }
+        // 3) persistent-CTA count of the traversal and shading kernels
+        const int blk = (cur.trace_block == 64 || cur.trace_block == 256) ? cur.trace_block : 128;
+        const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk));
+        const int occ_s = sms * std::max(1, wrk::occupancy_blocks(1));
+        for (double f : {0.5, 1.0}) {
+            wr_render_desc d = cur;
+            d.grid_trace = std::max(sms, int(occ_t * f));
+            const double t = trial(d);
+            if (t < bt) { bt = t; cur = d; }
+        }
+        for (double f : {0.5, 1.0}) {
+            wr_render_desc d = cur;
+            d.grid_shade = std::max(sms, int(occ_s * f));
+            const double t = trial(d);
+            if (t < bt) { bt = t; cur = d; }
+        }
+        *best = cur;
+        if (base) { best->num_spp = base->num_spp; best->profile = base->profile; }
+        else { best->num_spp = 0; }
+        if (best_ms) *best_ms = bt;
         return WR_OK;
     } catch (const Error &e) {
         return fail(e);

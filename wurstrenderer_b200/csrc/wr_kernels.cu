@@ -358,8 +358,9 @@ __device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c)
     atomicAdd(f + 2, double(c.z));
 }
 
-__global__ void __launch_bounds__(kTraceBlock) k_extend(DevScene s, WaveArgs w) {
-    __shared__ uint32_t stack[kSmemStack * kTraceBlock];
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
+    __shared__ uint32_t stack[kSmemStack * BLOCK];
     const uint32_t n = w.ctr[CTR_ACTIVE];
     uint32_t nv = 0, nt = 0;
     uint32_t *pv = w.prof ? &nv : nullptr, *pt = w.prof ? &nt : nullptr;
@@ -611,8 +612,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
     }
 }
 
-__global__ void __launch_bounds__(kTraceBlock) k_shadow(DevScene s, WaveArgs w) {
-    __shared__ uint32_t stack[kSmemStack * kTraceBlock];
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w) {
+    __shared__ uint32_t stack[kSmemStack * BLOCK];
     const uint32_t n = min(w.ctr[CTR_SHADOW], w.shadow_capacity);
     uint32_t nv = 0, nt = 0;
     uint32_t *pv = w.prof ? &nv : nullptr, *pt = w.prof ? &nt : nullptr;
@@ -797,10 +799,18 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
                    cudaStream_t st) {
     const WaveArgs w = make_args(b, parity, r);
     switch (which) {
-        case KERNEL_EXTEND: k_extend<<<r.grid_trace, kTraceBlock, 0, st>>>(s, w); break;
+        case KERNEL_EXTEND:
+            if (r.trace_block == 64) k_extend<64><<<r.grid_trace, 64, 0, st>>>(s, w);
+            else if (r.trace_block == 256) k_extend<256><<<r.grid_trace, 256, 0, st>>>(s, w);
+            else k_extend<128><<<r.grid_trace, 128, 0, st>>>(s, w);
+            break;
         case KERNEL_SHADE: k_shade<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
         case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
-        case KERNEL_SHADOW: k_shadow<<<r.grid_trace, kTraceBlock, 0, st>>>(s, w); break;
+        case KERNEL_SHADOW:
+            if (r.trace_block == 64) k_shadow<64><<<r.grid_trace, 64, 0, st>>>(s, w);
+            else if (r.trace_block == 256) k_shadow<256><<<r.grid_trace, 256, 0, st>>>(s, w);
+            else k_shadow<128><<<r.grid_trace, 128, 0, st>>>(s, w);
+            break;
         case KERNEL_ADVANCE: k_advance<<<1, 1, 0, st>>>(w); break;
         default: break;
     }
@@ -841,10 +851,15 @@ void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n,
     k_scale_pdf<<<592, 256, 0, st>>>(weights, total, pdf, n);
 }
 
-int occupancy_blocks(int which) {
+int occupancy_blocks(int which, int trace_block) {
     int nb = 0;
-    if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend, kTraceBlock, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeBlock, 0);
+    if (which == 0) {
+        if (trace_block == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<64>, 64, 0);
+        else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256>, 256, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128>, 128, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeBlock, 0);
+    }
     return nb;
 }
 

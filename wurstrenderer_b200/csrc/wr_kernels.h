@@ -29,6 +29,7 @@ struct RenderLaunch {
     unsigned long long total_samples;
     uint32_t iter_limit;        // the loop stops (and reports CTR_TIMEOUT) after this many iterations
     int grid_trace, grid_shade;
+    int trace_block;            // threads per block of extend / shadow: 64, 128 or 256
     cudaGraphConditionalHandle cond;   // while-loop condition when the loop body is captured in a graph
     int has_cond;
     unsigned long long *prof;   // device profiling totals or nullptr
@@ -48,6 +49,6 @@ void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t n
                       double *sums, cudaStream_t st);
 void launch_env_weights(const float4 *texels, int w, int h, double *out, cudaStream_t st);
 void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n, cudaStream_t st);
-int occupancy_blocks(int which);
+int occupancy_blocks(int which, int trace_block = 128);
 
 }  // namespace wrk

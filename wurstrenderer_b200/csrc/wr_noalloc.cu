@@ -164,7 +164,9 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
     r.total_samples = (unsigned long long)npix * unsigned(spp);
     const unsigned long long waves = (r.total_samples + kCapacity - 1) / kCapacity;
     r.iter_limit = uint32_t((waves + 2) * (unsigned long long)(nverts + 2) + 64);
-    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * (wrk::occupancy_blocks(0) > 0 ? wrk::occupancy_blocks(0) : 1);
+    r.trace_block = (desc.trace_block == 64 || desc.trace_block == 256) ? desc.trace_block : 128;
+    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace
+                                       : sms * (wrk::occupancy_blocks(0, r.trace_block) > 0 ? wrk::occupancy_blocks(0, r.trace_block) : 1);
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * (wrk::occupancy_blocks(1) > 0 ? wrk::occupancy_blocks(1) : 1);
     r.has_cond = 0;
     r.prof = nullptr;
@@ -211,6 +213,7 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
     stats.queue_capacity = kCapacity;
     stats.grid_trace = r.grid_trace;
     stats.grid_shade = r.grid_shade;
+    stats.trace_block = r.trace_block;
     stats.kernel_launches = launches;
     if (prev != v.device) NA_CUDA(cudaSetDevice(prev));
     return WR_OK;
