@@ -49,7 +49,9 @@ typedef struct wr_render_desc {
     int profile;             /* 0: off; 1: per-kernel CUDA-event timing (plain launches);
                                 2: timing + traversal counters (node visits, triangle tests) */
     int trace_block;         /* threads per block of the traversal kernels: 64, 128 or 256; 0 = 128 */
-    int reserved[6];
+    int integrator;          /* 0: the render entry's "integrator" (default nextevent_path_tracer);
+                                1: nextevent_path_tracer; 2: primitive_path_tracer */
+    int reserved[5];
 } wr_render_desc;
 
 typedef struct wr_render_stats {
@@ -110,7 +112,10 @@ int wr_scene_get_info(const wr_scene *scene, wr_scene_info *info);
 int wr_scene_set_camera_json(wr_scene *scene, const char *camera_json);
 
 /* Renders with the NEE+MIS integrator ("nextevent_path_tracer",
- * PathNeeRenderer::render, src/renderer/pathnextevent.h:152-191) and copies
+ * PathNeeRenderer::render, src/renderer/pathnextevent.h:152-191), or with the
+ * BSDF-only "primitive_path_tracer" (PrimitivePathRenderer::render,
+ * src/renderer/primitivepath.h:60-101) when the render entry or desc->integrator
+ * selects it, and copies
  * the W*H*3 image (base/spp + splat/(spp*W*H)) into host memory. desc may be
  * NULL (defaults). */
 int wr_render(wr_scene *scene, const wr_render_desc *desc, double *out_rgb);
@@ -181,7 +186,8 @@ int wr_write_pfm(const char *path, const double *rgb, int width, int height);
 /* Whole simple2 flow of the reference CLI (src/main.cpp:5-15,
  * src/sceneio/simple2parser.h:102-223): load the scene, render every
  * "nextevent_path_tracer" entry of "render" and write its "output" PFM next
- * to the scene JSON. Other integrators return WR_ERR_UNSUPPORTED. */
+ * to the scene JSON; "primitive_path_tracer" entries likewise. Other
+ * integrators return WR_ERR_UNSUPPORTED. */
 int wr_run_simple2(const char *scene_json_path);
 int wr_run_jsimple2(const char *json_text);
 

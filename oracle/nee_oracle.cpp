@@ -363,6 +363,7 @@ struct Scene {
     RayCaster rc;
     Camera cam;
     int spp = 16, nverts = 10;
+    int integrator = 0;   // 0 nextevent_path_tracer, 1 primitive_path_tracer
     std::string output;
 };
 
@@ -645,6 +646,71 @@ static void eval_contribution(const Scene &s, Sampler &smp, int px, int py, Spla
     }
 }
 
+// PrimitivePathRenderer::evalContribution (src/renderer/primitivepath.h:43-58): camera subpath
+// only, BSDF sampling, an emitter (or the environment) hit ends the path and contributes
+// pathContrib * Le1 * Le0 without MIS. Same sample consumption as createCameraSubpath +
+// randomWalk with the volumetric sample per segment (generalsubpathsampler.h:34-53).
+static void eval_primitive(const Scene &s, Sampler &smp, int px, int py, Splat *sp) {
+    const Camera &cam = s.cam;
+    Vertex c0;
+    {
+        double a, b; smp.get2d(&a, &b);
+        double lx = 0.0, ly = 0.0;
+        double abx = a * 2.0 - 1.0, aby = b * 2.0 - 1.0;
+        if (!(abx == 0 && aby == 0)) {
+            double r, phi;
+            if (abx * abx > aby * aby) { r = abx; phi = (Pi / 4.0) * (aby / abx); }
+            else { r = aby; phi = (Pi / 2.0) - (Pi / 4.0) * (abx / aby); }
+            lx = r * std::cos(phi); ly = r * std::sin(phi);
+        }
+        lx = lx * cam.aperture; ly = ly * cam.aperture;
+        c0.type = V_CAMERA;
+        c0.normal = cam.frame.z;
+        c0.pos = cam.frame.toWorld(V3(lx, ly, 0.0)) + cam.origin;
+        c0.contrib = Spectrum(1.0);
+    }
+    Ray ray;
+    {
+        double a, b; smp.get2d(&a, &b);
+        const double nsx = (double(px) + a) * (1.0 / double(cam.W)), nsy = (double(py) + b) * (1.0 / double(cam.H));
+        const V3 camPos = cam.frame.toLocal(c0.pos - cam.origin);
+        const V3 film((nsx - 0.5) * cam.filmW, (nsy - 0.5) * cam.filmH, -cam.dist);
+        sp->rx = nsx * double(cam.W); sp->ry = nsy * double(cam.H);
+        const V3 fpp = cam.focal * film / film.z;
+        const V3 dir = Normalize(fpp - camPos);
+        ray.o = c0.pos;
+        ray.d = cam.frame.toWorld(dir);
+    }
+    Spectrum prevContrib(1.0);
+    Vertex prev = c0;
+    int countVertices = 0;
+    const int numVertices = s.nverts - 1;
+    if (numVertices == 0) return;
+    while (true) {
+        Vertex v;
+        const bool hit = intersect(s, &ray, &v);
+        double du0, du1; smp.get2d(&du0, &du1);
+        if (!hit) break;
+        v.contrib = prevContrib * prev.contrib;
+        if (v.type == V_LIGHT || v.type == V_ENV) {
+            sp->c = v.contrib * Spectrum(light_le1(v, prev)) * light_le0(s, v);
+            break;
+        }
+        if (++countVertices == numVertices) break;
+        const Material &m = s.materials[s.geoms[v.geom].material];
+        const V3 inLocal = v.frame.toLocal(-ray.d);
+        V3 outLocal;
+        double b0, b1; smp.get2d(&b0, &b1);
+        const Spectrum w = bsdf_sample(m, &outLocal, nullptr, inLocal, b0, b1);
+        if (IsZero(w)) break;
+        prevContrib = w;
+        ray = Ray();
+        ray.o = v.pos;
+        ray.d = v.frame.toWorld(outLocal);
+        prev = v;
+    }
+}
+
 // -------------------------------------------------------------- loading ----
 static V3 vec3_of(const Json &j) {
     if (j.type == Json::Arr && j.arr.size() == 3) return V3(j.arr[0].number(), j.arr[1].number(), j.arr[2].number());
@@ -774,6 +840,9 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
         s->nverts = int(rj.get("num_path_vertices", 10.0));
         s->spp = int(rj.get("num_spp", 16.0));
         s->output = rj.get("output", std::string(""));
+        const std::string integ = rj.get("integrator", std::string("nextevent_path_tracer"));
+        if (integ == "primitive_path_tracer") s->integrator = 1;
+        else if (integ != "nextevent_path_tracer") throw std::runtime_error("integrator not restated by the oracle: " + integ);
     }
     return s.release();
 }
@@ -823,7 +892,8 @@ static RenderStats render(const Scene &s, int spp, int nverts, unsigned salt, in
                 for (int x = t.x0; x < t.x1; ++x)
                     for (int i = 0; i < spp; ++i) {
                         Splat sp[2];
-                        if (nverts > 1) eval_contribution(s, smp, x, y, sp);
+                        if (s.integrator == 1) eval_primitive(s, smp, x, y, sp);
+                        else if (nverts > 1) eval_contribution(s, smp, x, y, sp);
                         const int bx = int(sp[0].rx), by = int(sp[0].ry);
                         double *b = &base[3 * (size_t(by) * W + bx)];
                         b[0] += sp[0].c.x; b[1] += sp[0].c.y; b[2] += sp[0].c.z;

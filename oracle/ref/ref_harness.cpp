@@ -4,7 +4,7 @@
 //
 // It reproduces Simple2Parser::Parse / ParseScene (src/sceneio/simple2parser.h:
 // 27-68,102-223) with the reference's own classes -- ThinlensCamera,
-// PathNeeRenderer, EmbreeAccel, TriangleMeshGeometry, DiffuseAreaLight,
+// PathNeeRenderer, PrimitivePathRenderer, EmbreeAccel, TriangleMeshGeometry, DiffuseAreaLight,
 // EnvmapLight/EquiRectRep, the Lambert/Oren-Nayar/Phong/Mixed/TwoSided BSDFs,
 // Film, FimageIo -- and only replaces the two third-party libraries that
 // need cmake to build:
@@ -27,6 +27,7 @@
 #include "common/wurst.h"
 #include "common/util/json.h"
 #include "renderer/pathnextevent.h"
+#include "renderer/primitivepath.h"
 #include "camera/thinlens.h"
 #include "bsdf/lambertdiffuse.h"
 #include "bsdf/orennayar.h"
@@ -191,21 +192,28 @@ int cmd_render(int argc, char **argv) {
     Loaded L = load(scenePath, cam);
     const double loadSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl0).count();
     json rj = L.root["render"][renderIndex];
-    if (rj["integrator"] != "nextevent_path_tracer") throw std::runtime_error("integrator is not nextevent_path_tracer");
+    const bool primitive = rj["integrator"] == "primitive_path_tracer";
+    if (rj["integrator"] != "nextevent_path_tracer" && !primitive)
+        throw std::runtime_error("integrator is neither nextevent_path_tracer nor primitive_path_tracer");
     if (spp > 0) rj["num_spp"] = spp;
     if (nverts > 0) rj["num_path_vertices"] = nverts;
     shared_ptr<Sampler> sampler = make_shared<SaltedSampler>(salt);
     shared_ptr<const Camera> camera = L.camera;
     shared_ptr<const Scene> scene = L.scene;
-    shared_ptr<PathNeeRenderer> r = PathNeeRenderer::FromSimple2Json(camera, scene, sampler, rj, L.dir);
+    shared_ptr<PathNeeRenderer> r;
+    shared_ptr<PrimitivePathRenderer> rp;
+    if (primitive) rp = PrimitivePathRenderer::FromSimple2Json(camera, scene, sampler, rj, L.dir);
+    else r = PathNeeRenderer::FromSimple2Json(camera, scene, sampler, rj, L.dir);
+    const int numSpp = primitive ? rp->mNumSpp : r->mNumSpp;
+    const int numVerts = primitive ? rp->mNumPathVertices : r->mNumPathVertices;
     const Ivec2 res = camera->mFilm->mResolution;
     const int W = res[0], H = res[1];
     long long paths = 0;
     auto t0 = std::chrono::steady_clock::now();
     std::vector<double> img(size_t(W) * H * 3);
     if (!serial && !crop) {
-        r->render();
-        paths = (long long)W * H * r->mNumSpp;
+        if (primitive) rp->render(); else r->render();
+        paths = (long long)W * H * numSpp;
         Fimage<Spectrum> im = camera->mFilm->getImage();
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x)
@@ -213,7 +221,7 @@ int cmd_render(int argc, char **argv) {
     } else {
         if (!crop) { cx0 = 0; cy0 = 0; cx1 = W; cy1 = H; }
         Film &film = *camera->mFilm;
-        film.requestAtomicBuffer();
+        if (!primitive) film.requestAtomicBuffer();
         film.requestBaseBuffer();
         std::vector<TileB> blocks, sel;
         gen_blocks(Ivec2(0, 0), res, blocks);
@@ -223,9 +231,9 @@ int cmd_render(int argc, char **argv) {
                 sel.push_back(b);
                 npix += (long long)(b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]);
             }
-        film.mBaseScalingFactor = 1.0 / double(r->mNumSpp);
-        film.mAtomicScalingFactor = 1.0 / double(r->mNumSpp) / double(npix);
-        if (r->mNumPathVertices > 1) {
+        film.mBaseScalingFactor = 1.0 / double(numSpp);
+        film.mAtomicScalingFactor = 1.0 / double(numSpp) / double(npix);
+        if (primitive || numVerts > 1) {
             std::atomic<size_t> next(0);
             auto worker = [&]() {
                 for (size_t ti = next++; ti < sel.size(); ti = next++) {
@@ -235,12 +243,18 @@ int cmd_render(int argc, char **argv) {
                     shared_ptr<Sampler> ts = sampler->clone(tileSeed);
                     for (const Ivec2 pixel : bound) {
                         ts->setPixel(pixel);
-                        for (int i = 0; i < r->mNumSpp; ++i) {
-                            Splat splats[2];
-                            r->evalContribution(splats, ts.get(), pixel);
-                            film.addSample(splats[0].mRaster, splats[0].mContrib);
-                            film.atomicAddSample(splats[1].mRaster, splats[1].mContrib);
-                            ts->nextSample();
+                        for (int i = 0; i < numSpp; ++i) {
+                            if (primitive) {
+                                Splat sp;
+                                rp->evalContribution(&sp, ts.get(), pixel);
+                                film.addSample(sp.mRaster, sp.mContrib);
+                            } else {
+                                Splat splats[2];
+                                r->evalContribution(splats, ts.get(), pixel);
+                                film.addSample(splats[0].mRaster, splats[0].mContrib);
+                                film.atomicAddSample(splats[1].mRaster, splats[1].mContrib);
+                                ts->nextSample();
+                            }
                         }
                     }
                 }
@@ -250,7 +264,7 @@ int cmd_render(int argc, char **argv) {
             worker();
             for (auto &th : pool) th.join();
         }
-        paths = npix * r->mNumSpp;
+        paths = npix * numSpp;
         for (int y = 0; y < H; ++y)
             for (int x = 0; x < W; ++x) {
                 Spectrum c = film.getPixel(Ivec2(x, y));

@@ -29,10 +29,22 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from wurstrenderer_b200 import scenes  # noqa: E402
 
-FIXTURES = ["cornell", "zoo", "env", "hf"]
+FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt"]
+
+
+def with_integrator(path, integrator):
+    with open(path) as f:
+        scene = json.load(f)
+    for r in scene["render"]:
+        r["integrator"] = integrator
+    with open(path, "w") as f:
+        json.dump(scene, f, indent=1)
+    return path
 
 
 def write_fixture_scene(name, out_dir):
+    if name.endswith("_pt"):   # the same scene rendered by primitive_path_tracer
+        return with_integrator(write_fixture_scene(name[:-3], out_dir), "primitive_path_tracer")
     if name == "cornell":
         return scenes.write_cornell(out_dir, name="cornell", resolution=(48, 48), spp=4, num_path_vertices=10)
     if name == "zoo":
@@ -102,7 +114,8 @@ def main():
             os.remove(os.path.join(sdir, f))
         with open(os.path.join(HERE, name + "_meta.json"), "w") as f:
             json.dump({"scene": os.path.relpath(path, HERE), "hi_spp": args.hi_spp, "salts": [11, 22],
-                       "width": sc.width, "height": sc.height}, f)
+                       "width": sc.width, "height": sc.height,
+                       "integrator": json.load(open(path))["render"][0]["integrator"]}, f)
 
 
 if __name__ == "__main__":

@@ -47,7 +47,7 @@ def test_inspect_matches_oracle_scene(wr_lib, oracle_lib, name):
     assert info["num_path_vertices"] == sc.num_path_vertices
     assert 0 < info["bvh_depth"] <= 64
     assert info["bvh_nodes"] >= 1
-    assert info["has_envmap"] == (1 if name == "env" else 0)
+    assert info["has_envmap"] == (1 if name.startswith("env") else 0)
 
 
 def test_pfm_roundtrip_layout(wr_lib, tmp_path):

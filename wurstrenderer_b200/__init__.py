@@ -41,7 +41,7 @@ class RenderDesc(ctypes.Structure):
     _fields_ = [("num_spp", ctypes.c_int), ("num_path_vertices", ctypes.c_int), ("seed", ctypes.c_uint),
                 ("render_index", ctypes.c_int), ("queue_capacity", ctypes.c_int), ("grid_trace", ctypes.c_int),
                 ("grid_shade", ctypes.c_int), ("use_graph", ctypes.c_int), ("profile", ctypes.c_int),
-                ("trace_block", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("trace_block", ctypes.c_int), ("integrator", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
 
 
 class Job(ctypes.Structure):
@@ -174,7 +174,7 @@ class Scene:
 
     @staticmethod
     def _desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-              profile=0, trace_block=None):
+              profile=0, trace_block=None, integrator=None):
         d = RenderDesc()
         d.num_spp = int(spp or 0)
         d.num_path_vertices = int(num_path_vertices or 0)
@@ -186,16 +186,19 @@ class Scene:
         d.use_graph = 1 if use_graph else 0
         d.profile = int(profile)
         d.trace_block = int(trace_block or 0)
+        d.integrator = {None: 0, "nextevent_path_tracer": 1, "primitive_path_tracer": 2}[integrator]
         return d
 
     def render(self, spp=None, num_path_vertices=None, seed=0, render_index=0, queue_capacity=None,
-               grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0, trace_block=None) -> np.ndarray:
-        """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top)."""
+               grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0, trace_block=None,
+               integrator=None) -> np.ndarray:
+        """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top).
+        integrator: None (the render entry's), "nextevent_path_tracer" or "primitive_path_tracer"."""
         inf = self.info
         if out is None:
             out = np.empty((inf["height"], inf["width"], 3), np.float64)
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-                       profile, trace_block)
+                       profile, trace_block, integrator)
         _check(load_library().wr_render(self._h, ctypes.byref(d), _ptr(out)))
         return out
 

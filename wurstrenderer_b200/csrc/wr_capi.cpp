@@ -363,7 +363,14 @@ struct HostJob {
     wr::Camera cam;
     int spp = 16, nverts = 10;
     uint32_t seed = 0;
+    int integrator = wrd::INTEGRATOR_NEE;
 };
+
+int integrator_of(const std::string &name) {
+    if (name.empty() || name == "nextevent_path_tracer") return wrd::INTEGRATOR_NEE;
+    if (name == "primitive_path_tracer") return wrd::INTEGRATOR_PRIMITIVE;
+    throw Error(WR_ERR_UNSUPPORTED, "integrator '" + name + "' is not provided by this build");
+}
 
 // Renders a batch of jobs (one camera, spp and depth each) over the scene in one wavefront.
 // The images land in `out` (host or device) concatenated in job order.
@@ -387,9 +394,11 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
         d.pix_offset = uint32_t(total_pix);
         d.sample_begin = total;
         d.seed = hj.seed;
+        d.integrator = hj.integrator;
         total += (unsigned long long)d.npix * unsigned(hj.spp);
         total_pix += d.npix;
         max_nverts = std::max(max_nverts, hj.nverts);
+        if (hj.integrator == wrd::INTEGRATOR_PRIMITIVE && hj.nverts <= 1) table[j].nverts = 1;
         if (total_pix >= (1ull << 31)) throw Error(WR_ERR_UNSUPPORTED, "batch film larger than 2^31 pixels");
         if (jobs.size() >= (1u << 24)) throw Error(WR_ERR_UNSUPPORTED, "more than 2^24 jobs");
     }
@@ -610,6 +619,9 @@ HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
     j.spp = desc.num_spp > 0 ? desc.num_spp : re.num_spp;
     j.nverts = desc.num_path_vertices > 0 ? desc.num_path_vertices : re.num_path_vertices;
     j.seed = desc.seed;
+    j.integrator = desc.integrator == 1 ? wrd::INTEGRATOR_NEE
+                 : desc.integrator == 2 ? wrd::INTEGRATOR_PRIMITIVE
+                                        : integrator_of(re.integrator);
     return j;
 }
 
@@ -676,8 +688,7 @@ void run_scene(wr_scene &s) {
     const wr::Scene &h = s.host;
     for (size_t i = 0; i < h.renders.size(); ++i) {
         const wr::RenderEntry &re = h.renders[i];
-        if (re.integrator != "nextevent_path_tracer")
-            throw Error(WR_ERR_UNSUPPORTED, "integrator '" + re.integrator + "' is not provided by this build");
+        integrator_of(re.integrator);   // nextevent_path_tracer or primitive_path_tracer
         wr_render_desc d{};
         d.render_index = int(i);
         d.use_graph = 1;

@@ -81,8 +81,10 @@ struct DevJob {
     uint32_t npix;
     unsigned long long sample_begin;  // first global sample id of this job
     uint32_t seed;
-    uint32_t pad;
+    int integrator;                   // INTEGRATOR_NEE or INTEGRATOR_PRIMITIVE
 };
+constexpr int INTEGRATOR_NEE = 0;        // nextevent_path_tracer (src/renderer/pathnextevent.h)
+constexpr int INTEGRATOR_PRIMITIVE = 1;  // primitive_path_tracer (src/renderer/primitivepath.h)
 
 struct DevScene {
     const float4 *nodes;

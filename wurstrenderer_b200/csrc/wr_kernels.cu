@@ -405,12 +405,14 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
             sample = __float_as_uint(t4.w);
             const uint32_t tri = __float_as_uint(h.w);
             const float t = h.x;
+            const bool primitive = J.integrator == INTEGRATOR_PRIMITIVE;
             if (tri == MISS) {
                 if (s.has_env) {
-                    // strategy B on the environment (pathnextevent.h:128-146)
+                    // strategy B on the environment (pathnextevent.h:128-146); the primitive tracer
+                    // takes the emission with weight one (primitivepath.h:49-53)
                     const float cPdfA = prevPdfW;   // ConvertToArea to an environment vertex: 1/|d|^2
-                    const float lPdfA = s.env_select_pdf * env_pdf(s, d);
-                    const float mis = cPdfA / (lPdfA + cPdfA);
+                    const float lPdfA = primitive ? 0.f : s.env_select_pdf * env_pdf(s, d);
+                    const float mis = primitive ? 1.f : cPdfA / (lPdfA + cPdfA);
                     const f3 c = thr * env_eval(s, d) * mis;
                     if (!is_zero(c) && isfinite(c.x + c.y + c.z)) film_add(w, pixel, c);
                 }
@@ -427,7 +429,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
                     if (cosl <= 0.f) {   // front face: evalLe1 (diffusearealight.h:48-53)
                         const float cPdfA = prevPdfW * fabsf(cosl) / (t * t);
                         const float lPdfA = __ldg(&s.lights[li].select_pdf) * __ldg(&s.lights[li].inv_area);
-                        const float mis = cPdfA / (lPdfA + cPdfA);
+                        const float mis = primitive ? 1.f : cPdfA / (lPdfA + cPdfA);
                         const f3 c = thr * mk(__ldg(&s.lights[li].intensity[0]), __ldg(&s.lights[li].intensity[1]),
                                               __ldg(&s.lights[li].intensity[2])) * mis;
                         if (!is_zero(c) && isfinite(c.x + c.y + c.z)) film_add(w, pixel, c);
@@ -440,7 +442,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
                     const uint32_t lpix = pixel - J.pix_offset, seed = job_seed(J, job);
                     // strategy A: next-event estimation toward this sample's light vertex
                     const Rand4 r0 = rand4(lpix, sample, 0, seed);
-                    const LightVtx l = sample_light(s, r0.a, r0.b);
+                    LightVtx l{};
+                    if (primitive) l.pdfA = 0.f;   // no connection to the light (primitivepath.h)
+                    else l = sample_light(s, r0.a, r0.b);
                     f3 wo;
                     float G, convA, dist = 0.f;
                     if (l.env) {
@@ -532,7 +536,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
             const uint32_t seed = job_seed(J, job);
             const uint32_t px = lpix % uint32_t(cam.width), py = lpix / uint32_t(cam.width);
             const Rand4 r0 = rand4(lpix, sample, 0, seed);
-            const LightVtx l = sample_light(s, r0.a, r0.b);
+            LightVtx l{};
+            if (J.integrator == INTEGRATOR_PRIMITIVE) l.pdfA = 0.f;   // camera subpath only
+            else l = sample_light(s, r0.a, r0.b);
             // camera vertex: lens point (pinhole when the aperture is zero)
             f3 c0 = corg;
             if (cam.aperture > 0.f) {
