@@ -269,7 +269,10 @@ def main():
         paths_batch = sum(j["camera"]["resolution"][0] * j["camera"]["resolution"][1] * j["num_spp"]
                           for j in batch_jobs)
 
+    from wurstrenderer_b200.distributed import combine_films, max_over_ranks, rank_seed
+
     def step(seed):
+        seed = rank_seed(seed, rank)
         if batch_jobs is not None:
             for k, j in enumerate(batch_jobs):
                 j["seed"] = seed + k
@@ -277,8 +280,7 @@ def main():
             return scene.stats
         scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc, **knobs)
         st = scene.stats
-        if world > 1:
-            dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
+        combine_films(film, world, dist)
         return st
 
     for i in range(args.warmup):
@@ -304,10 +306,7 @@ def main():
         dist.barrier()
     clk = clocks.stop()
 
-    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(dev_ms, world, dist, device="cuda")
     paths_per_rank = W * H * spp if batch_jobs is None else paths_batch
     value = paths_per_rank * world * args.steps / (max_ms / 1e3) / 1e6
 
@@ -331,10 +330,7 @@ def main():
         else:
             scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc, **knobs)
         e2e_ms += (time.perf_counter() - a) * 1e3
-    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = paths_per_rank * world * args.steps / (float(e2e_t.item()) / 1e3) / 1e6
+    e2e_value = paths_per_rank * world * args.steps / (max_over_ranks(e2e_ms, world, dist, device="cuda") / 1e3) / 1e6
 
     # one profiled render (per-kernel events + traversal counters) for the roofline, outside the timed region
     if batch_jobs is not None:
