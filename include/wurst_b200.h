@@ -87,12 +87,26 @@ typedef struct wr_scene_info {
     double bvh_sah_cost;
     double build_ms;                  /* scene parse + BVH + upload + CDF build */
     int num_renders;
+    int bvh_builder;                  /* WR_BVH_* used */
+    double bvh_ms;                    /* BVH build time (device time for WR_BVH_DEVICE_LBVH) */
 } wr_scene_info;
+
+#define WR_BVH_HOST_SAH 0       /* binned SAH on the host, <= max_leaf triangles per leaf (default) */
+#define WR_BVH_DEVICE_LBVH 1    /* linear BVH built on the device (Morton codes, radix sort, Karras 2012) */
+
+typedef struct wr_scene_options {
+    int bvh_builder;         /* WR_BVH_HOST_SAH or WR_BVH_DEVICE_LBVH */
+    int max_leaf;            /* host SAH: triangles per leaf, 1..16 (0 = 4) */
+    int reserved[6];
+} wr_scene_options;
 
 /* Parses a simple2 scene JSON (Simple2Parser::Parse, src/sceneio/simple2parser.h:84-100),
  * loads its OBJ/MTL meshes and envmap, builds the BVH and the FP64 light /
  * environment CDFs, and uploads everything to the current CUDA device. */
 int wr_scene_create(const char *scene_json_path, wr_scene **out);
+
+/* Same with build options (opts may be NULL: defaults). */
+int wr_scene_create_ex(const char *scene_json_path, const wr_scene_options *opts, wr_scene **out);
 
 /* Same from JSON text (the --jsimple2parse path, src/main.cpp:12-15);
  * relative mesh paths resolve against base_dir (NULL: current directory). */

@@ -67,11 +67,20 @@ class SceneInfo(ctypes.Structure):
                 ("num_path_vertices", ctypes.c_int), ("num_triangles", ctypes.c_ulonglong),
                 ("num_meshes", ctypes.c_int), ("num_lights", ctypes.c_int), ("has_envmap", ctypes.c_int),
                 ("bvh_nodes", ctypes.c_int), ("bvh_depth", ctypes.c_int), ("bvh_sah_cost", ctypes.c_double),
-                ("build_ms", ctypes.c_double), ("num_renders", ctypes.c_int)]
+                ("build_ms", ctypes.c_double), ("num_renders", ctypes.c_int), ("bvh_builder", ctypes.c_int),
+                ("bvh_ms", ctypes.c_double)]
+
+
+class SceneOptions(ctypes.Structure):
+    _fields_ = [("bvh_builder", ctypes.c_int), ("max_leaf", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
+BVH_HOST_SAH = 0
+BVH_DEVICE_LBVH = 1
 
 
 # every function the C ABI exports (include/wurst_b200.h)
-EXPORTS = ["wr_scene_create", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
+EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
@@ -93,6 +102,7 @@ def load_library(path: str = LIB_PATH):
     L.wr_abi_version.restype = ctypes.c_int
     L.wr_scene_create.argtypes = [cp, ctypes.POINTER(vp)]
     L.wr_scene_create_from_json.argtypes = [cp, cp, ctypes.POINTER(vp)]
+    L.wr_scene_create_ex.argtypes = [cp, ctypes.POINTER(SceneOptions), ctypes.POINTER(vp)]
     L.wr_scene_destroy.argtypes = [vp]
     L.wr_scene_destroy.restype = None
     L.wr_scene_get_info.argtypes = [vp, ctypes.POINTER(SceneInfo)]
@@ -133,10 +143,13 @@ class Scene:
         self._h = handle
 
     @classmethod
-    def from_file(cls, json_path: str) -> "Scene":
+    def from_file(cls, json_path: str, bvh_builder: int = BVH_HOST_SAH, max_leaf: int = 0) -> "Scene":
         L = load_library()
         h = ctypes.c_void_p()
-        _check(L.wr_scene_create(os.fspath(json_path).encode(), ctypes.byref(h)))
+        opts = SceneOptions()
+        opts.bvh_builder = int(bvh_builder)
+        opts.max_leaf = int(max_leaf)
+        _check(L.wr_scene_create_ex(os.fspath(json_path).encode(), ctypes.byref(opts), ctypes.byref(h)))
         return cls(h)
 
     @classmethod

@@ -27,6 +27,10 @@
 
 using wr::Error;
 
+namespace wr {
+BvhBuildResult build_bvh_lbvh(const std::vector<float> &tri_vertices, cudaStream_t st, double *device_ms);
+}
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -75,8 +79,9 @@ struct wr_scene {
     DevBuf nodes, tris, tri_mat, materials, lights, light_tris, light_tri_cdf, light_tri_pdf, light_cdf, light_pdf;
     DevBuf env_texels, env_pixel_pdf, env_row_cdf, env_row_pdf, env_col_cdf, env_col_pdf;
     wrd::DevScene dev{};
+    wr_scene_options opts{};
     int bvh_nodes = 0, bvh_depth = 0;
-    double sah_cost = 0.0, build_ms = 0.0;
+    double sah_cost = 0.0, build_ms = 0.0, bvh_ms = 0.0;
     // wavefront buffers
     DevBuf w_o[2], w_d[2], w_thr[2], w_meta[2], w_hit, w_sho, w_shd, w_shc, w_film, w_ctr, w_sample, w_out, w_prof,
         w_jobs;
@@ -136,7 +141,14 @@ void build_device_scene(wr_scene &s) {
             }
         }
     }
-    wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, 4, 0);
+    wr::BvhBuildResult bvh;
+    const auto tb = std::chrono::steady_clock::now();
+    if (s.opts.bvh_builder == WR_BVH_DEVICE_LBVH) {
+        bvh = wr::build_bvh_lbvh(verts, st, &s.bvh_ms);
+    } else {
+        bvh = wr::build_bvh_sah(verts, s.opts.max_leaf > 0 ? s.opts.max_leaf : 4, 0);
+        s.bvh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+    }
     s.bvh_nodes = int(bvh.nodes.size() / 16);
     s.bvh_depth = bvh.depth;
     s.sah_cost = bvh.sah_cost;
@@ -677,8 +689,11 @@ void trace_batch(wr_scene &s, const float *rays, int n, int any_hit, std::vector
     if (nt) *nt = vis[1];
 }
 
-std::unique_ptr<wr_scene> create(wr::Scene &&host) {
+std::unique_ptr<wr_scene> create(wr::Scene &&host, const wr_scene_options *opts = nullptr) {
     std::unique_ptr<wr_scene> s(new wr_scene());
+    if (opts) s->opts = *opts;
+    if (s->opts.bvh_builder != WR_BVH_HOST_SAH && s->opts.bvh_builder != WR_BVH_DEVICE_LBVH)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "unknown bvh_builder");
     s->host = std::move(host);
     build_device_scene(*s);
     return s;
@@ -722,6 +737,20 @@ int wr_scene_create(const char *path, wr_scene **out) {
     *out = nullptr;
     try {
         *out = create(wr::load_simple2_file(path)).release();
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return WR_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int wr_scene_create_ex(const char *path, const wr_scene_options *opts, wr_scene **out) {
+    if (!path || !out) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    try {
+        *out = create(wr::load_simple2_file(path), opts).release();
         return WR_OK;
     } catch (const Error &e) {
         return fail(e);
@@ -799,6 +828,8 @@ int wr_scene_get_info(const wr_scene *s, wr_scene_info *info) {
     info->bvh_sah_cost = s->sah_cost;
     info->build_ms = s->build_ms;
     info->num_renders = int(h.renders.size());
+    info->bvh_builder = s->opts.bvh_builder;
+    info->bvh_ms = s->bvh_ms;
     return WR_OK;
 }
 
