@@ -51,7 +51,19 @@ typedef struct wr_render_desc {
     int trace_block;         /* threads per block of the traversal kernels: 64, 128 or 256; 0 = 128 */
     int integrator;          /* 0: the render entry's "integrator" (default nextevent_path_tracer);
                                 1: nextevent_path_tracer; 2: primitive_path_tracer */
-    int reserved[5];
+    int guiding;             /* learned proposal (no counterpart in the reference; NEE+MIS only):
+                                0: off (plain NEE+MIS);
+                                1: train a fresh network online on the first guide_train_spp samples per
+                                   pixel (in passes, Adam after each pass), use it for the remaining samples;
+                                2: use the scene's current network as it is (no training) */
+    int guide_train_spp;     /* samples per pixel of the training phase; 0 = 32 */
+    int guide_pass_spp;      /* samples per pixel per training pass; 0 = about 2^22 paths per pass, at
+                                least four passes */
+    int guide_batch;         /* training records per Adam step; 0 = 16384 */
+    int guide_steps;         /* Adam steps of the training phase, spread evenly over its passes; 0 = 2048 */
+    float guide_clamp;       /* loss weights are clamped at guide_clamp x their mean over the pass;
+                                0 = 1000, < 0 = no clamp */
+    int reserved[4];
 } wr_render_desc;
 
 typedef struct wr_render_stats {
@@ -64,11 +76,18 @@ typedef struct wr_render_stats {
     int trace_block;                  /* threads per traversal block used */
     unsigned long long kernel_launches;   /* kernels launched by the render */
     /* per-kernel totals, filled when desc.profile != 0 (index: WR_K_*) */
-    double kernel_ms[6];
-    unsigned long long kernel_count[6];   /* launches */
-    unsigned long long kernel_items[6];   /* rays / paths processed */
+    double kernel_ms[8];
+    unsigned long long kernel_count[8];   /* launches */
+    unsigned long long kernel_items[8];   /* rays / paths processed */
     unsigned long long extend_node_visits, extend_tri_tests;   /* profile == 2 */
     unsigned long long shadow_node_visits, shadow_tri_tests;
+    /* guided renders */
+    unsigned long long guide_records;     /* training records collected */
+    unsigned long long guide_steps;       /* Adam steps taken */
+    double guide_train_ms;                /* device time of the training kernels */
+    double guide_loss;                    /* mean loss of the last training pass */
+    int guide_passes;                     /* render passes (training passes + the final one) */
+    int reserved_stats;
 } wr_render_stats;
 
 #define WR_K_EXTEND 0
@@ -77,6 +96,8 @@ typedef struct wr_render_stats {
 #define WR_K_SHADOW 3
 #define WR_K_ADVANCE 4
 #define WR_K_RESOLVE 5
+#define WR_K_GUIDE 6      /* guiding-network inference over the wavefront */
+#define WR_K_TRAIN 7      /* guiding-network training (gradient + Adam) */
 
 typedef struct wr_scene_info {
     int width, height;                /* camera resolution */
@@ -177,6 +198,37 @@ int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc, double
  * writes the fastest settings into *best (other fields copied from base) and
  * its time per render into *best_ms. */
 int wr_autotune(wr_scene *scene, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms);
+
+/* ---- Learned guiding proposal (no counterpart in the reference) ----
+ * A 64-64-64-64-64-64 ReLU MLP (BF16 weights and activations, FP32 accumulation on
+ * the tensor cores, FP32 master weights) maps 64 encoded inputs -- the hit position
+ * normalised to the scene box, sin/cos(2^f pi p) for f = 0..5, the geometric normal
+ * turned toward the outgoing direction, the outgoing direction, sin/cos(pi n),
+ * sin/cos(pi wo), zeros and a constant 1 -- to 8 von Mises-Fisher lobes: axis
+ * (outputs 5k..5k+2, normalised), sharpness softplus(5k+3) + 0.5, weight softmax(5k+4).
+ * Unit 63 of every hidden layer is the constant 1, so column 63 is a bias.
+ * Weights: WR_GUIDE_PARAMS floats, [layer][out][in]. One network per scene handle. */
+#define WR_GUIDE_PARAMS 20480
+
+/* Initialises the network with seeded uniform (Glorot) weights and clears Adam's state. */
+int wr_guide_reset(wr_scene *scene, unsigned int seed);
+int wr_guide_get_params(wr_scene *scene, float *params);
+int wr_guide_set_params(wr_scene *scene, const float *params);
+/* The position normalisation: feature = (p - lo) * inv_extent. */
+int wr_guide_box(const wr_scene *scene, float lo[3], float inv_extent[3]);
+/* Lobes for n rows of 9 floats (position, normal, outgoing direction), host memory:
+ * 40 floats per row, 8 x (axis xyz, sharpness) then the 8 weights. */
+int wr_guide_eval(wr_scene *scene, const float *rows, int n, float *lobes);
+/* Gradient of sum_i -min(c_i, c_max) log q_i(direction_i) over n training records of
+ * 20 floats (position, c, normal, -, outgoing, -, direction, -, throughput, -),
+ * host memory, into grad (WR_GUIDE_PARAMS floats); *loss receives the summed loss
+ * (may be NULL). The network is not changed. */
+int wr_guide_gradient(wr_scene *scene, const float *records, int n, float c_max, float *grad, double *loss);
+/* `steps` Adam steps (learning rate lr) on minibatches of `batch` records drawn in a
+ * fixed shuffled order from the n records; loss_per_step (may be NULL) receives
+ * each step's mean loss before its update. */
+int wr_guide_train(wr_scene *scene, const float *records, int n, int steps, int batch, float lr,
+                   double *loss_per_step);
 
 /* Closest-hit queries (EmbreeAccel::intersectTriangleInfo,
  * src/accel/embreeaccel.h:425-464). rays: n x 8 floats

@@ -41,7 +41,9 @@ class RenderDesc(ctypes.Structure):
     _fields_ = [("num_spp", ctypes.c_int), ("num_path_vertices", ctypes.c_int), ("seed", ctypes.c_uint),
                 ("render_index", ctypes.c_int), ("queue_capacity", ctypes.c_int), ("grid_trace", ctypes.c_int),
                 ("grid_shade", ctypes.c_int), ("use_graph", ctypes.c_int), ("profile", ctypes.c_int),
-                ("trace_block", ctypes.c_int), ("integrator", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+                ("trace_block", ctypes.c_int), ("integrator", ctypes.c_int), ("guiding", ctypes.c_int),
+                ("guide_train_spp", ctypes.c_int), ("guide_pass_spp", ctypes.c_int), ("guide_batch", ctypes.c_int),
+                ("guide_steps", ctypes.c_int), ("guide_clamp", ctypes.c_float), ("reserved", ctypes.c_int * 4)]
 
 
 class Job(ctypes.Structure):
@@ -53,13 +55,17 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("render_ms", ctypes.c_double), ("paths", ctypes.c_ulonglong), ("iterations", ctypes.c_ulonglong),
                 ("max_shadow_queue", ctypes.c_uint), ("queue_capacity", ctypes.c_uint),
                 ("grid_trace", ctypes.c_int), ("grid_shade", ctypes.c_int), ("trace_block", ctypes.c_int),
-                ("kernel_launches", ctypes.c_ulonglong), ("kernel_ms", ctypes.c_double * 6),
-                ("kernel_count", ctypes.c_ulonglong * 6), ("kernel_items", ctypes.c_ulonglong * 6),
+                ("kernel_launches", ctypes.c_ulonglong), ("kernel_ms", ctypes.c_double * 8),
+                ("kernel_count", ctypes.c_ulonglong * 8), ("kernel_items", ctypes.c_ulonglong * 8),
                 ("extend_node_visits", ctypes.c_ulonglong), ("extend_tri_tests", ctypes.c_ulonglong),
-                ("shadow_node_visits", ctypes.c_ulonglong), ("shadow_tri_tests", ctypes.c_ulonglong)]
+                ("shadow_node_visits", ctypes.c_ulonglong), ("shadow_tri_tests", ctypes.c_ulonglong),
+                ("guide_records", ctypes.c_ulonglong), ("guide_steps", ctypes.c_ulonglong),
+                ("guide_train_ms", ctypes.c_double), ("guide_loss", ctypes.c_double),
+                ("guide_passes", ctypes.c_int), ("reserved_stats", ctypes.c_int)]
 
 
-KERNELS = ["extend", "shade", "raygen", "shadow", "advance", "resolve"]
+KERNELS = ["extend", "shade", "raygen", "shadow", "advance", "resolve", "guide", "train"]
+GUIDE_PARAMS = 20480   # 5 layers x 64 x 64 FP32 weights, [layer][out][in]
 
 
 class SceneInfo(ctypes.Structure):
@@ -84,7 +90,8 @@ EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
-           "wr_render_batch_device", "wr_autotune"]
+           "wr_render_batch_device", "wr_autotune", "wr_guide_reset", "wr_guide_get_params", "wr_guide_set_params",
+           "wr_guide_box", "wr_guide_eval", "wr_guide_gradient", "wr_guide_train"]
 
 _lib = None
 
@@ -123,6 +130,13 @@ def load_library(path: str = LIB_PATH):
     L.wr_run_simple2.argtypes = [cp]
     L.wr_run_jsimple2.argtypes = [cp]
     L.wr_set_device.argtypes = [ip]
+    L.wr_guide_reset.argtypes = [vp, ctypes.c_uint]
+    L.wr_guide_get_params.argtypes = [vp, fp]
+    L.wr_guide_set_params.argtypes = [vp, fp]
+    L.wr_guide_box.argtypes = [vp, fp, fp]
+    L.wr_guide_eval.argtypes = [vp, fp, ip, fp]
+    L.wr_guide_gradient.argtypes = [vp, fp, ip, ctypes.c_float, fp, ctypes.POINTER(ctypes.c_double)]
+    L.wr_guide_train.argtypes = [vp, fp, ip, ip, ip, ctypes.c_float, fp]
     _lib = L
     return L
 
@@ -187,7 +201,8 @@ class Scene:
 
     @staticmethod
     def _desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-              profile=0, trace_block=None, integrator=None):
+              profile=0, trace_block=None, integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
+              guide_batch=None, guide_steps=None, guide_clamp=None):
         d = RenderDesc()
         d.num_spp = int(spp or 0)
         d.num_path_vertices = int(num_path_vertices or 0)
@@ -200,18 +215,28 @@ class Scene:
         d.profile = int(profile)
         d.trace_block = int(trace_block or 0)
         d.integrator = {None: 0, "nextevent_path_tracer": 1, "primitive_path_tracer": 2}[integrator]
+        d.guiding = {False: 0, True: 1, 0: 0, 1: 1, 2: 2, "off": 0, "train": 1, "frozen": 2}[guiding]
+        d.guide_train_spp = int(guide_train_spp or 0)
+        d.guide_pass_spp = int(guide_pass_spp or 0)
+        d.guide_batch = int(guide_batch or 0)
+        d.guide_steps = int(guide_steps or 0)
+        d.guide_clamp = float(guide_clamp or 0.0)
         return d
 
     def render(self, spp=None, num_path_vertices=None, seed=0, render_index=0, queue_capacity=None,
                grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0, trace_block=None,
-               integrator=None) -> np.ndarray:
+               integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
+               guide_batch=None, guide_steps=None, guide_clamp=None) -> np.ndarray:
         """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top).
-        integrator: None (the render entry's), "nextevent_path_tracer" or "primitive_path_tracer"."""
+        integrator: None (the render entry's), "nextevent_path_tracer" or "primitive_path_tracer".
+        guiding: 0 / "off" (plain NEE+MIS), 1 / "train" (learned proposal trained online on the first
+        guide_train_spp samples, default 32), 2 / "frozen" (the scene's current network, no training)."""
         inf = self.info
         if out is None:
             out = np.empty((inf["height"], inf["width"], 3), np.float64)
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-                       profile, trace_block, integrator)
+                       profile, trace_block, integrator, guiding, guide_train_spp, guide_pass_spp, guide_batch,
+                       guide_steps, guide_clamp)
         _check(load_library().wr_render(self._h, ctypes.byref(d), _ptr(out)))
         return out
 
@@ -276,6 +301,54 @@ class Scene:
             v = getattr(st, k)
             out[k] = list(v) if isinstance(v, ctypes.Array) else v
         return out
+
+    # ---- learned guiding proposal ----
+    def guide_reset(self, seed=0) -> None:
+        _check(load_library().wr_guide_reset(self._h, int(seed) & 0xFFFFFFFF))
+
+    def guide_params(self) -> np.ndarray:
+        """FP32 master weights, shape (5, 64, 64) [layer][out][in]."""
+        w = np.empty(GUIDE_PARAMS, np.float32)
+        _check(load_library().wr_guide_get_params(self._h, _ptr(w)))
+        return w.reshape(5, 64, 64)
+
+    def guide_set_params(self, w) -> None:
+        w = np.ascontiguousarray(w, np.float32).reshape(-1)
+        if w.size != GUIDE_PARAMS:
+            raise ValueError("expected %d weights" % GUIDE_PARAMS)
+        _check(load_library().wr_guide_set_params(self._h, _ptr(w)))
+
+    def guide_box(self):
+        lo = np.empty(3, np.float32)
+        inv = np.empty(3, np.float32)
+        _check(load_library().wr_guide_box(self._h, _ptr(lo), _ptr(inv)))
+        return lo, inv
+
+    def guide_eval(self, rows):
+        """rows (n, 9) [position, normal, outgoing] -> (axis (n, 8, 3), sharpness (n, 8), weight (n, 8))."""
+        rows = np.ascontiguousarray(rows, np.float32)
+        n = rows.shape[0]
+        out = np.empty((n, 40), np.float32)
+        _check(load_library().wr_guide_eval(self._h, _ptr(rows), n, _ptr(out)))
+        lob = out[:, :32].reshape(n, 8, 4)
+        return lob[..., :3], lob[..., 3], out[:, 32:]
+
+    def guide_gradient(self, records, c_max=100.0):
+        """records (n, 20) -> (gradient (5, 64, 64), summed loss)."""
+        records = np.ascontiguousarray(records, np.float32)
+        g = np.empty(GUIDE_PARAMS, np.float32)
+        loss = ctypes.c_double(0.0)
+        _check(load_library().wr_guide_gradient(self._h, _ptr(records), records.shape[0], float(c_max), _ptr(g),
+                                                ctypes.byref(loss)))
+        return g.reshape(5, 64, 64), loss.value
+
+    def guide_train(self, records, steps, batch=65536, lr=1e-3):
+        """Adam steps on the records; returns each step's mean loss."""
+        records = np.ascontiguousarray(records, np.float32)
+        losses = np.zeros(int(steps), np.float64)
+        _check(load_library().wr_guide_train(self._h, _ptr(records), records.shape[0], int(steps), int(batch),
+                                             float(lr), _ptr(losses)))
+        return losses
 
     def trace_closest(self, rays: np.ndarray):
         """rays (n, 8) float32 [ox, oy, oz, tnear, dx, dy, dz, tfar] -> (geom_id, prim_id, t, uv)."""

@@ -27,7 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall,-Wno-
           "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 CU_FLAGS = ARCH + COMMON + ["--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES = ["wr_scene_io.cpp", "wr_bvh.cpp", "wr_capi.cpp", "wr_kernels.cu", "wr_noalloc.cu", "wr_lbvh.cu"]
+SOURCES = ["wr_scene_io.cpp", "wr_bvh.cpp", "wr_capi.cpp", "wr_kernels.cu", "wr_noalloc.cu", "wr_lbvh.cu", "wr_guide.cu"]
 
 
 def _newest_header():

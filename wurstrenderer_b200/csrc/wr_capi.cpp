@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/wurst_b200.h"
+#include "wr_guide.h"
 #include "wr_host.h"
 #include "wr_kernels.h"
 
@@ -86,12 +87,20 @@ struct wr_scene {
     DevBuf w_o[2], w_d[2], w_thr[2], w_meta[2], w_hit, w_sho, w_shd, w_shc, w_film, w_ctr, w_sample, w_out, w_prof,
         w_jobs;
     std::vector<cudaEvent_t> kev;
+    // learned guiding: network, per-slot lobes / record links, training records
+    wrg::GuideNet guide{};
+    bool guide_ready = false;
+    int guide_step = 0;
+    float box_lo[3] = {0.f, 0.f, 0.f}, box_inv[3] = {1.f, 1.f, 1.f};
+    DevBuf w_rec[2], w_lobes, w_records, w_rec_count, g_scratch, g_scratch2, g_loss;
+    uint32_t w_guide_capacity = 0, w_record_capacity = 0;
     uint32_t w_capacity = 0;
     size_t w_npix = 0;
     uint32_t *pinned = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     wr_render_stats stats{};
     ~wr_scene() {
+        if (guide_ready) wrg::guide_free(guide);
         if (pinned) cudaFreeHost(pinned);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -139,6 +148,20 @@ void build_device_scene(wr_scene &s) {
                 tri_prim[g] = t;
                 tri_code[g] = code;
             }
+        }
+    }
+    {   // scene box of the guiding network's position feature (1% margin per side)
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (size_t i = 0; i + 2 < verts.size(); i += 3)
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = std::min(lo[k], verts[i + k]);
+                hi[k] = std::max(hi[k], verts[i + k]);
+            }
+        for (int k = 0; k < 3; ++k) {
+            if (!(lo[k] <= hi[k])) { lo[k] = 0.f; hi[k] = 1.f; }
+            const float ext = std::max(hi[k] - lo[k], 1e-6f);
+            s.box_lo[k] = lo[k] - 0.01f * ext;
+            s.box_inv[k] = 1.f / (1.02f * ext);
         }
     }
     wr::BvhBuildResult bvh;
@@ -376,7 +399,31 @@ struct HostJob {
     int spp = 16, nverts = 10;
     uint32_t seed = 0;
     int integrator = wrd::INTEGRATOR_NEE;
+    uint32_t sample_offset = 0;   // per-pixel index of the first sample (renders split in passes)
+    int spp_norm = 0;             // film normalisation (0: spp)
 };
+
+// options of one render pass (guided renders are a sequence of passes over one film)
+struct PassOpts {
+    const wrg::GuideNet *guide = nullptr;   // lobes for shading (nullptr: plain NEE+MIS)
+    bool record = false;                    // collect training records
+    bool keep_film = false;                 // add to the film of the previous pass
+    uint32_t record_capacity = 0;
+};
+
+void ensure_guide_wave(wr_scene &s, uint32_t capacity, uint32_t record_capacity) {
+    if (s.w_guide_capacity != capacity) {
+        s.w_rec[0].alloc(size_t(capacity) * 4);
+        s.w_rec[1].alloc(size_t(capacity) * 4);
+        s.w_lobes.alloc(size_t(capacity) * wrg::kPackedChunks * 16);
+        s.w_guide_capacity = capacity;
+    }
+    if (record_capacity > s.w_record_capacity) {
+        s.w_records.alloc(size_t(record_capacity) * wrg::kRecordFloat4 * 16);
+        s.w_record_capacity = record_capacity;
+    }
+    s.w_rec_count.alloc(16);
+}
 
 int integrator_of(const std::string &name) {
     if (name.empty() || name == "nextevent_path_tracer") return wrd::INTEGRATOR_NEE;
@@ -387,7 +434,7 @@ int integrator_of(const std::string &name) {
 // Renders a batch of jobs (one camera, spp and depth each) over the scene in one wavefront.
 // The images land in `out` (host or device) concatenated in job order.
 void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_desc &desc, double *out,
-                 bool out_on_host) {
+                 bool out_on_host, const PassOpts &po = PassOpts{}) {
     if (jobs.empty()) throw Error(WR_ERR_INVALID_ARGUMENT, "no jobs");
     std::vector<wrd::DevJob> table(jobs.size());
     unsigned long long total = 0;
@@ -407,6 +454,8 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
         d.sample_begin = total;
         d.seed = hj.seed;
         d.integrator = hj.integrator;
+        d.sample_offset = hj.sample_offset;
+        d.spp_norm = hj.spp_norm;
         total += (unsigned long long)d.npix * unsigned(hj.spp);
         total_pix += d.npix;
         max_nverts = std::max(max_nverts, hj.nverts);
@@ -437,8 +486,21 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     b.sample_next = s.w_sample.as<unsigned long long>();
     b.capacity = capacity;
     b.shadow_capacity = 2 * capacity;
+    const bool guided = po.guide || po.record;
+    if (guided) {
+        ensure_guide_wave(s, capacity, po.record_capacity);
+        b.rec[0] = s.w_rec[0].as<uint32_t>();
+        b.rec[1] = s.w_rec[1].as<uint32_t>();
+        b.lobes = s.w_lobes.as<uint4>();
+        b.records = s.w_records.as<float4>();
+        b.rec_count = s.w_rec_count.as<uint32_t>();
+        b.rec_capacity = s.w_record_capacity;
+    }
 
     wrk::RenderLaunch r{};
+    r.guide = po.guide;
+    r.record = po.record ? 1 : 0;
+    r.guide_sms = sms;
     r.num_jobs = int(table.size());
     r.job0 = table[0];
     if (table.size() > 1) {
@@ -458,11 +520,12 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     s.w_prof.alloc(16 * 8);
     r.prof = profile >= 2 ? s.w_prof.as<unsigned long long>() : nullptr;
     s.stats = wr_render_stats{};
-    double *dst = out_on_host ? s.w_out.as<double>() : out;
+    double *dst = (out_on_host || !out) ? s.w_out.as<double>() : out;
     unsigned long long launches = 0;
 
     auto clear = [&]() {
-        WR_CUDA(cudaMemsetAsync(b.film, 0, total_pix * 6 * 8, st));
+        if (!po.keep_film) WR_CUDA(cudaMemsetAsync(b.film, 0, total_pix * 6 * 8, st));
+        if (po.record) WR_CUDA(cudaMemsetAsync(b.rec_count, 0, 4, st));
         WR_CUDA(cudaMemsetAsync(b.ctr, 0, wrd::CTR_COUNT * 4, st));
         WR_CUDA(cudaMemsetAsync(b.sample_next, 0, 8, st));
     };
@@ -495,9 +558,9 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
             timed(wrk::KERNEL_ADVANCE, 1);
             int parity = 0;
             while (true) {
-                for (int k : {wrk::KERNEL_EXTEND, wrk::KERNEL_SHADE, wrk::KERNEL_RAYGEN, wrk::KERNEL_SHADOW,
-                              wrk::KERNEL_ADVANCE})
-                    timed(k, parity);
+                for (int k : {wrk::KERNEL_EXTEND, wrk::KERNEL_GUIDE, wrk::KERNEL_SHADE, wrk::KERNEL_RAYGEN,
+                              wrk::KERNEL_SHADOW, wrk::KERNEL_ADVANCE})
+                    if (k != wrk::KERNEL_GUIDE || po.guide) timed(k, parity);
                 parity ^= 1;
                 WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
                 WR_CUDA(cudaStreamSynchronize(st));
@@ -593,7 +656,8 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     }
     if (!desc.use_graph || profile) WR_CUDA(cudaEventRecord(s.ev1, st));
     WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
-    if (out_on_host) WR_CUDA(cudaMemcpyAsync(out, dst, total_pix * 3 * 8, cudaMemcpyDeviceToHost, st));
+    if (out_on_host && out) WR_CUDA(cudaMemcpyAsync(out, dst, total_pix * 3 * 8, cudaMemcpyDeviceToHost, st));
+    if (po.record) WR_CUDA(cudaMemcpyAsync(s.pinned + 12, b.rec_count, 4, cudaMemcpyDeviceToHost, st));
     WR_CUDA(cudaStreamSynchronize(st));
     if (trace && s.pinned[wrd::CTR_TIMEOUT]) throw Error(WR_ERR_TIMEOUT, "wavefront did not drain within the iteration bound");
     if (trace && s.pinned[wrd::CTR_OVERFLOW]) throw Error(WR_ERR_CUDA, "shadow queue overflow");
@@ -611,8 +675,9 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     s.stats.render_ms = ms;
     s.stats.paths = total;
     s.stats.iterations = trace ? s.pinned[wrd::CTR_ITER] : 0;
-    // kernels per render: prime 3 + 5 per iteration + resolve (a graph launch runs the same kernels)
-    s.stats.kernel_launches = trace ? 3ull + 5ull * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
+    // kernels per render: prime 3 + 5 (6 with guiding) per iteration + resolve (a graph launch runs the
+    // same kernels)
+    s.stats.kernel_launches = trace ? 3ull + (po.guide ? 6ull : 5ull) * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
     s.stats.max_shadow_queue = s.pinned[wrd::CTR_SHADOW_MAX];
     s.stats.queue_capacity = capacity;
     s.stats.grid_trace = r.grid_trace;
@@ -637,9 +702,217 @@ HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
     return j;
 }
 
+// ------------------------------------------------------------ guiding ----
+constexpr float kGuideLr = 1e-3f;   // Adam learning rate
+
+int sm_count(const wr_scene &s) {
+    int sms = 148;
+    WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
+    return sms;
+}
+
+void ensure_guide(wr_scene &s) {
+    if (s.guide_ready) return;
+    wrg::GuideNet g{};
+    for (int k = 0; k < 3; ++k) {
+        g.box_lo[k] = s.box_lo[k];
+        g.box_inv[k] = s.box_inv[k];
+    }
+    try {
+        wrg::guide_alloc(g);
+        wrg::guide_init(g, 0x9E3779B9u, s.stream);
+        WR_CUDA(cudaStreamSynchronize(s.stream));
+    } catch (...) {
+        wrg::guide_free(g);
+        throw;
+    }
+    s.guide = g;
+    s.guide_ready = true;
+    s.guide_step = 0;
+}
+
+void check_guide_status(wr_scene &s) {
+    uint32_t err = 0;
+    WR_CUDA(cudaMemcpyAsync(&err, s.guide.err, 4, cudaMemcpyDeviceToHost, s.stream));
+    WR_CUDA(cudaStreamSynchronize(s.stream));
+    if (err) {
+        WR_CUDA(cudaMemsetAsync(s.guide.err, 0, 4, s.stream));
+        throw Error(WR_ERR_TIMEOUT, "guiding network: a tensor-core completion wait timed out");
+    }
+}
+
+// a stride coprime with n (a fixed shuffle of the records: i -> i * stride mod n)
+uint32_t shuffle_stride(uint32_t n) {
+    if (n <= 2) return 1u;
+    uint64_t c = uint64_t(double(n) * 0.6180339887) | 1u;
+    auto gcd = [](uint64_t a, uint64_t b) { while (b) { const uint64_t t = a % b; a = b; b = t; } return a; };
+    while (gcd(c, n) != 1) c += 2;
+    return uint32_t(c % n);
+}
+
+// Adam steps over minibatches of records [0, n) in device memory; returns the summed loss
+double train_records(wr_scene &s, const float4 *records, uint32_t n, uint32_t batch, int max_steps, float lr,
+                     float c_max, std::vector<double> *per_step, unsigned long long *steps_out) {
+    cudaStream_t st = s.stream;
+    const int sms = sm_count(s);
+    s.g_loss.alloc(8 * 2);
+    const uint32_t stride = shuffle_stride(n);
+    const int steps = max_steps > 0 ? max_steps : int((n + batch - 1) / batch);
+    double total = 0.0;
+    WR_CUDA(cudaMemsetAsync(s.g_loss.p, 0, 8, st));
+    for (int k = 0; k < steps && n > 0; ++k) {
+        const uint32_t first = uint32_t((uint64_t(k) * batch) % n);
+        const uint32_t cnt = std::min(batch, n - first);
+        if (per_step) WR_CUDA(cudaMemsetAsync(s.g_loss.p, 0, 8, st));
+        wrg::guide_gradient(s.guide, records, nullptr, first + cnt, first, n, stride, c_max, s.g_loss.as<double>(),
+                            sms, st);
+        wrg::guide_adam(s.guide, lr, 1.f / float(cnt), ++s.guide_step, st);
+        if (per_step) {
+            double l = 0.0;
+            WR_CUDA(cudaMemcpyAsync(&l, s.g_loss.p, 8, cudaMemcpyDeviceToHost, st));
+            WR_CUDA(cudaStreamSynchronize(st));
+            per_step->push_back(l / double(cnt));
+            total += l;
+        }
+        if (steps_out) ++*steps_out;
+    }
+    if (!per_step) {
+        WR_CUDA(cudaMemcpyAsync(&total, s.g_loss.p, 8, cudaMemcpyDeviceToHost, st));
+        WR_CUDA(cudaStreamSynchronize(st));
+    }
+    check_guide_status(s);
+    return total;
+}
+
+void add_stats(wr_render_stats &a, const wr_render_stats &b) {
+    a.render_ms += b.render_ms;
+    a.paths += b.paths;
+    a.iterations += b.iterations;
+    a.max_shadow_queue = std::max(a.max_shadow_queue, b.max_shadow_queue);
+    a.queue_capacity = b.queue_capacity;
+    a.grid_trace = b.grid_trace;
+    a.grid_shade = b.grid_shade;
+    a.trace_block = b.trace_block;
+    a.kernel_launches += b.kernel_launches;
+    for (int k = 0; k < 8; ++k) {
+        a.kernel_ms[k] += b.kernel_ms[k];
+        a.kernel_count[k] += b.kernel_count[k];
+        a.kernel_items[k] += b.kernel_items[k];
+    }
+    a.extend_node_visits += b.extend_node_visits;
+    a.extend_tri_tests += b.extend_tri_tests;
+    a.shadow_node_visits += b.shadow_node_visits;
+    a.shadow_tri_tests += b.shadow_tri_tests;
+}
+
+// Guided render: training passes (records collected, Adam after each pass; the first pass
+// samples the BSDF only), then one pass with the trained network for the remaining samples.
+// All passes add to one film, normalised by the total spp, so the image is the same
+// unbiased estimator as the plain render with a different sampling density.
+void render_guided(wr_scene &s, const wr_render_desc &desc, double *out, bool out_on_host) {
+    HostJob base = scene_job(s.host, desc);
+    if (base.integrator != wrd::INTEGRATOR_NEE)
+        throw Error(WR_ERR_UNSUPPORTED, "guiding applies to nextevent_path_tracer only");
+    if (desc.guiding != 1 && desc.guiding != 2) throw Error(WR_ERR_INVALID_ARGUMENT, "guiding must be 0, 1 or 2");
+    if (base.spp <= 0) throw Error(WR_ERR_INVALID_ARGUMENT, "num_spp must be positive");
+    ensure_guide(s);
+    cudaStream_t st = s.stream;
+    const int total = base.spp;
+    const size_t npix = size_t(std::max(base.cam.width, 0)) * size_t(std::max(base.cam.height, 0));
+    if (npix == 0) throw Error(WR_ERR_INVALID_ARGUMENT, "resolution must be positive");
+    const int train = desc.guiding == 1 ? std::min(desc.guide_train_spp > 0 ? desc.guide_train_spp : 32, total) : 0;
+    // training passes of about 2^22 paths, at least four of them
+    const int pass = desc.guide_pass_spp > 0
+                         ? desc.guide_pass_spp
+                         : int(std::max<size_t>(1, std::min<size_t>(size_t(std::max(train / 4, 1)),
+                                                                    (size_t(1) << 22) / npix)));
+    const uint32_t batch = desc.guide_batch > 0 ? uint32_t(desc.guide_batch) : 16384u;
+    const int n_train_passes = train > 0 ? (train + pass - 1) / pass : 0;
+    const int total_steps = desc.guide_steps > 0 ? desc.guide_steps : 2048;
+    const uint64_t per_pass = uint64_t(npix) * uint64_t(pass) * uint64_t(std::max(1, base.nverts - 2));
+    const uint32_t rec_cap = uint32_t(std::min<uint64_t>(per_pass, uint64_t(1) << 24));
+    if (desc.guiding == 1) {
+        wrg::guide_init(s.guide, desc.seed * 0x85EBCA6Bu + 0x6A09E667u, st);
+        s.guide_step = 0;
+    }
+    wr_render_stats agg{};
+    bool trained = desc.guiding == 2;
+    double train_ms = 0.0, last_loss = 0.0;
+    unsigned long long records = 0, steps = 0;
+    int done = 0, passes = 0;
+    const int sms = sm_count(s);
+    while (done < train) {
+        const int k = std::min(pass, train - done);
+        HostJob j = base;
+        j.spp = k;
+        j.sample_offset = uint32_t(done);
+        j.spp_norm = total;
+        PassOpts po;
+        po.guide = trained ? &s.guide : nullptr;
+        po.record = true;
+        po.keep_film = done > 0;
+        po.record_capacity = rec_cap;
+        const bool last = done + k == total;
+        render_jobs(s, {j}, desc, last ? out : nullptr, out_on_host, po);
+        add_stats(agg, s.stats);
+        ++passes;
+        const uint32_t n = std::min(s.pinned[12], s.w_record_capacity);
+        records += n;
+        // loss weight clamp: 20 x the mean c of the pass's records
+        s.g_scratch2.alloc(16);
+        wrg::guide_cstats(s.w_records.as<float4>(), n, s.g_scratch2.as<double>(), sms, st);
+        double cs[2] = {0.0, 0.0};
+        WR_CUDA(cudaMemcpyAsync(cs, s.g_scratch2.p, 16, cudaMemcpyDeviceToHost, st));
+        WR_CUDA(cudaStreamSynchronize(st));
+        const double clamp = desc.guide_clamp > 0.f ? double(desc.guide_clamp) : 1000.0;
+        const float c_max = desc.guide_clamp < 0.f ? INFINITY
+                          : cs[1] > 0.0 ? float(clamp * cs[0] / cs[1]) : wrg::kCMax;
+        // the step budget spread evenly over the training passes
+        const int pass_steps = total_steps * (passes) / n_train_passes - total_steps * (passes - 1) / n_train_passes;
+        WR_CUDA(cudaEventRecord(s.ev0, st));
+        const double loss = train_records(s, s.w_records.as<float4>(), n, batch, std::max(pass_steps, 1), kGuideLr,
+                                          c_max, nullptr, &steps);
+        WR_CUDA(cudaEventRecord(s.ev1, st));
+        WR_CUDA(cudaEventSynchronize(s.ev1));
+        float ms = 0.f;
+        WR_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
+        train_ms += ms;
+        last_loss = n ? loss / (double(std::max(pass_steps, 1)) * double(std::min(batch, n))) : 0.0;
+        trained = trained || n > 0;
+        done += k;
+    }
+    if (done < total) {
+        HostJob j = base;
+        j.spp = total - done;
+        j.sample_offset = uint32_t(done);
+        j.spp_norm = total;
+        PassOpts po;
+        po.guide = trained ? &s.guide : nullptr;
+        po.keep_film = done > 0;
+        render_jobs(s, {j}, desc, out, out_on_host, po);
+        add_stats(agg, s.stats);
+        ++passes;
+    }
+    check_guide_status(s);
+    agg.render_ms += train_ms;
+    agg.kernel_ms[WR_K_TRAIN] += train_ms;
+    agg.kernel_count[WR_K_TRAIN] += steps;
+    agg.kernel_items[WR_K_TRAIN] += records;
+    agg.guide_records = records;
+    agg.guide_steps = steps;
+    agg.guide_train_ms = train_ms;
+    agg.guide_loss = last_loss;
+    agg.guide_passes = passes;
+    s.stats = agg;
+}
+
 void render(wr_scene &s, const wr_render_desc *desc_in, double *out, bool out_on_host) {
     wr_render_desc desc{};
     if (desc_in) desc = *desc_in;
+    if (desc.guiding) {
+        render_guided(s, desc, out, out_on_host);
+        return;
+    }
     render_jobs(s, {scene_job(s.host, desc)}, desc, out, out_on_host);
 }
 
@@ -952,6 +1225,131 @@ int wr_get_render_stats(const wr_scene *s, wr_render_stats *st) {
     if (!s || !st) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
     *st = s->stats;
     return WR_OK;
+}
+
+// ---- learned guiding proposal ----
+int wr_guide_reset(wr_scene *s, unsigned int seed) {
+    if (!s) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        ensure_guide(*s);
+        wrg::guide_init(s->guide, seed, s->stream);
+        s->guide_step = 0;
+        WR_CUDA(cudaStreamSynchronize(s->stream));
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_guide_get_params(wr_scene *s, float *params) {
+    if (!s || !params) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        ensure_guide(*s);
+        wrg::guide_get_master(s->guide, params, s->stream);
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_guide_set_params(wr_scene *s, const float *params) {
+    if (!s || !params) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        ensure_guide(*s);
+        wrg::guide_set_master(s->guide, params, s->stream);
+        WR_CUDA(cudaStreamSynchronize(s->stream));
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_guide_box(const wr_scene *s, float lo[3], float inv_extent[3]) {
+    if (!s || !lo || !inv_extent) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = s->box_lo[k];
+        inv_extent[k] = s->box_inv[k];
+    }
+    return WR_OK;
+}
+
+int wr_guide_eval(wr_scene *s, const float *rows, int n, float *lobes) {
+    if (!s || n < 0 || (n > 0 && (!rows || !lobes))) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    if (n == 0) return WR_OK;
+    try {
+        ensure_guide(*s);
+        cudaStream_t st = s->stream;
+        s->g_scratch.alloc(size_t(n) * 9 * 4);
+        s->g_scratch2.alloc(size_t(n) * wrg::kLobeFloat4 * 16);
+        WR_CUDA(cudaMemcpyAsync(s->g_scratch.p, rows, size_t(n) * 9 * 4, cudaMemcpyHostToDevice, st));
+        wrg::guide_infer_rows(s->guide, s->g_scratch.as<float>(), uint32_t(n), s->g_scratch2.as<float4>(), sm_count(*s),
+                              st);
+        std::vector<float4> out(size_t(n) * wrg::kLobeFloat4);
+        WR_CUDA(cudaMemcpyAsync(out.data(), s->g_scratch2.p, out.size() * 16, cudaMemcpyDeviceToHost, st));
+        WR_CUDA(cudaStreamSynchronize(st));
+        check_guide_status(*s);
+        for (int i = 0; i < n; ++i) {
+            const float4 *L = &out[size_t(i) * wrg::kLobeFloat4];
+            float *o = lobes + 40 * size_t(i);
+            for (int k = 0; k < 8; ++k) {
+                o[4 * k + 0] = L[k].x;
+                o[4 * k + 1] = L[k].y;
+                o[4 * k + 2] = L[k].z;
+                o[4 * k + 3] = L[k].w;
+            }
+            const float w[8] = {L[8].x, L[8].y, L[8].z, L[8].w, L[9].x, L[9].y, L[9].z, L[9].w};
+            for (int k = 0; k < 8; ++k) o[32 + k] = w[k];
+        }
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_guide_gradient(wr_scene *s, const float *records, int n, float c_max, float *grad, double *loss) {
+    if (!s || !grad || n < 0 || (n > 0 && !records)) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        ensure_guide(*s);
+        cudaStream_t st = s->stream;
+        s->g_scratch.alloc(std::max<size_t>(size_t(n), 1) * wrg::kRecordFloat4 * 16);
+        s->g_loss.alloc(16);
+        if (n) WR_CUDA(cudaMemcpyAsync(s->g_scratch.p, records, size_t(n) * 80, cudaMemcpyHostToDevice, st));
+        WR_CUDA(cudaMemsetAsync(s->g_loss.p, 0, 8, st));
+        wrg::guide_gradient(s->guide, s->g_scratch.as<float4>(), nullptr, uint32_t(n), 0, uint32_t(n), 1u, c_max,
+                            s->g_loss.as<double>(), sm_count(*s), st);
+        wrg::guide_sum_gradient(s->guide, st);
+        WR_CUDA(cudaMemcpyAsync(grad, s->guide.grad, size_t(wrg::kGuideParams) * 4, cudaMemcpyDeviceToHost, st));
+        double l = 0.0;
+        WR_CUDA(cudaMemcpyAsync(&l, s->g_loss.p, 8, cudaMemcpyDeviceToHost, st));
+        WR_CUDA(cudaStreamSynchronize(st));
+        check_guide_status(*s);
+        if (loss) *loss = l;
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_guide_train(wr_scene *s, const float *records, int n, int steps, int batch, float lr, double *loss_per_step) {
+    if (!s || n < 0 || (n > 0 && !records) || steps < 0 || batch <= 0) {
+        g_last_error = "invalid argument";
+        return WR_ERR_INVALID_ARGUMENT;
+    }
+    if (n == 0 || steps == 0) return WR_OK;
+    try {
+        ensure_guide(*s);
+        cudaStream_t st = s->stream;
+        s->g_scratch.alloc(size_t(n) * wrg::kRecordFloat4 * 16);
+        WR_CUDA(cudaMemcpyAsync(s->g_scratch.p, records, size_t(n) * 80, cudaMemcpyHostToDevice, st));
+        std::vector<double> per;
+        train_records(*s, s->g_scratch.as<float4>(), uint32_t(n), uint32_t(batch), steps, lr, wrg::kCMax, &per,
+                      nullptr);
+        if (loss_per_step)
+            for (int k = 0; k < steps && k < int(per.size()); ++k) loss_per_step[k] = per[size_t(k)];
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
 }
 
 int wr_trace_closest(wr_scene *s, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *uv) {

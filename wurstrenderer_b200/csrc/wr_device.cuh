@@ -82,6 +82,8 @@ struct DevJob {
     unsigned long long sample_begin;  // first global sample id of this job
     uint32_t seed;
     int integrator;                   // INTEGRATOR_NEE or INTEGRATOR_PRIMITIVE
+    uint32_t sample_offset;           // per-pixel sample index of the first sample (renders split in passes)
+    int spp_norm;                     // film normalisation spp (0: spp)
 };
 constexpr int INTEGRATOR_NEE = 0;        // nextevent_path_tracer (src/renderer/pathnextevent.h)
 constexpr int INTEGRATOR_PRIMITIVE = 1;  // primitive_path_tracer (src/renderer/primitivepath.h)

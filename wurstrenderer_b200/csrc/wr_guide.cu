@@ -1,0 +1,526 @@
+// Learned guiding proposal: a small MLP trained online on incident-radiance
+// samples produced by the path tracer, predicting 8 von Mises-Fisher lobes that
+// serve as a directional sampling density (combined with BSDF sampling by
+// one-sample MIS in k_shade, so the estimator stays unbiased). It has no
+// counterpart in the reference; the plain NEE+MIS path is unchanged when it is off.
+//
+// Network: 64 encoded inputs (57 features + zeros + a constant 1), 4 hidden
+// layers of 64 ReLU units, 64 outputs of which 40 are used (8 x axis, sharpness,
+// weight). Unit 63 of every hidden layer is held at 1 (its weight row is e_63),
+// so column 63 of the following layer is that layer's bias.
+// Arithmetic: BF16 weights and activations, FP32 accumulation on the 5th-gen
+// tensor cores (tcgen05.mma, accumulators in TMEM), FP32 master weights and Adam.
+//
+//   k_guide_infer   128-row tiles: encode -> 5 x (tcgen05.mma M128 N64 K64 -> TMEM ->
+//                   ReLU -> smem) -> lobe parameters per path
+//   k_guide_train   forward (activations kept in smem), mixture-NLL gradient, backward:
+//                   dX = dH W (M128 N64 K64), dW += dH^T X (M64 N64 K128, MN-major operands,
+//                   accumulated in TMEM across all tiles of the CTA), one atomic flush per CTA
+//   k_guide_adam    Adam on the FP32 master weights, BF16 copies (W and W^T) for the kernels
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "wr_device.cuh"
+#include "wr_guide.h"
+#include "wr_host.h"
+#include "wr_guide_net.cuh"
+#include "wr_guide_tc.cuh"
+
+namespace wrg {
+
+// training kernel shared memory: W 40 KB, W^T 40 KB, X_0..X_4 80 KB, dH 16 KB + 8 KB pad, barrier
+constexpr int kTrainBarrier = 163840 + 16384 + 8192;
+
+// --------------------------------------------------------------- inference ----
+// Inputs come either from the wavefront (hit point of every live path) or from an
+// explicit array of (p, n, wo) rows (validation).
+struct InferSource {
+    // wavefront
+    const float4 *o, *d, *hit;
+    const uint32_t *count;      // device counter of live paths
+    const float4 *tris;
+    const uint32_t *tri_mat;
+    // explicit rows: 9 floats (p, n, wo)
+    const float *rows;
+    uint32_t nrows;
+};
+
+__device__ __forceinline__ bool fetch_point(const InferSource &s, uint32_t i, f3 &p, f3 &n, f3 &wo) {
+    if (s.rows) {
+        const float *r = s.rows + 9 * size_t(i);
+        p = mk(r[0], r[1], r[2]); n = mk(r[3], r[4], r[5]); wo = mk(r[6], r[7], r[8]);
+        return true;
+    }
+    const float4 h = s.hit[i];
+    const uint32_t tri = __float_as_uint(h.w);
+    if (tri == wrd::MISS || (__ldg(s.tri_mat + tri) & wrd::LIGHT_BIT)) return false;
+    const float4 o = s.o[i], d = s.d[i];
+    const f3 a = wrd::xyz(__ldg(s.tris + 3 * tri)), b = wrd::xyz(__ldg(s.tris + 3 * tri + 1)),
+             c = wrd::xyz(__ldg(s.tris + 3 * tri + 2));
+    const f3 dd = mk(d.x, d.y, d.z);
+    p = mk(o.x, o.y, o.z) + dd * h.x;
+    wo = -dd;
+    n = guide_normal(wrd::normalize(wrd::cross(b - a, c - a)), wo);
+    return true;
+}
+
+// Inference: kGroups warpgroups per CTA, each running its own chain of 128-row tiles
+// (its own activation tile, TMEM columns, mbarrier and named barrier) over weights
+// loaded once per CTA, so one group's tensor-core work overlaps another's epilogue.
+// Output: lobes as FP32 (kLobeFloat4 float4 per row, the validation API) or packed
+// halves (chunk-major with `packed_stride`, the render).
+constexpr int kGroups = 2;
+constexpr size_t kInferSmem = size_t(kWeightBytesInfer) + size_t(kGroups) * kActBytes + 64;
+
+__global__ void __launch_bounds__(kTile *kGroups, 3) k_guide_infer(GuideNet g, InferSource src, float4 *lobes_f,
+                                                                  uint4 *lobes_packed, size_t packed_stride) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *wt = smem;                                   // weight tiles (last layer: 48 rows)
+    const int tid = threadIdx.x, grp = tid >> 7, r = tid & 127, warp = tid >> 5;
+    unsigned char *at = smem + kWeightBytesInfer + grp * kActBytes;   // this group's activation tile
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kWeightBytesInfer + kGroups * kActBytes) + grp;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kWeightBytesInfer + kGroups * kActBytes + 8 * kGroups);
+    if (warp == 0) tmem_alloc(smem_addr(slot), 64 * kGroups);
+    if (r == 0) mbar_init(smem_addr(mbar), 1);
+    load_weights(wt, g.w, kLastRows);
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *slot + uint32_t(64 * grp);
+    const int bar = 1 + grp;
+    const uint32_t n_rows = src.rows ? src.nrows : *src.count;
+    const uint32_t ntiles = (n_rows + kTile - 1) / kTile;
+    uint32_t phase = 0;
+    for (uint32_t tile = blockIdx.x * kGroups + grp; tile < ntiles; tile += gridDim.x * kGroups) {
+        const uint32_t row = tile * kTile + r;
+        float x[kW];
+        f3 p, n, wo;
+        const bool valid = row < n_rows && fetch_point(src, row, p, n, wo);
+        if (valid) encode(p, n, wo, g, x);
+        else {
+#pragma unroll
+            for (int k = 0; k < kW; ++k) x[k] = 0.f;
+        }
+        store_row(at, r, x);
+        fence_async_smem();
+        fence_before_sync();
+        group_sync(bar);
+        fence_after_sync();
+        if (!mlp_forward_tile(at, wt, mbar, tmem, phase, x, bar, kLastRows)) {
+            if (r == 0) atomicExch(g.err, 1u);
+            break;
+        }
+        if (row < n_rows) {
+            Lobes L;
+            raw_to_lobes(x, L);
+            if (lobes_packed) {
+                store_packed_lobes(lobes_packed, packed_stride, row, L, valid);
+            } else {
+                float4 *out = lobes_f + kLobeFloat4 * size_t(row);
+                if (valid) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) out[k] = make_float4(L.mu[k][0], L.mu[k][1], L.mu[k][2], L.lam[k]);
+                    out[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
+                    out[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
+                } else {
+                    out[8] = make_float4(0.f, 0.f, 0.f, 0.f);   // zero weights: no lobe
+                    out[9] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(*slot, 64 * kGroups);
+}
+
+// ----------------------------------------------------------------- training ----
+// Gradient of -c log p(w) with respect to the 40 used outputs (oracle: loss_grad_output).
+__device__ __forceinline__ float loss_grad(const float *o, f3 d, float c, float c_max, float *go) {
+    float amax = -1e30f;
+    for (int k = 0; k < 8; ++k) amax = fmaxf(amax, o[5 * k + 4]);
+    float w[8], f[8], lam[8], cosk[8], mu[8][3], nr[8], s[8], wsum = 0.f;
+    for (int k = 0; k < 8; ++k) {
+        const float rx = o[5 * k], ry = o[5 * k + 1], rz = o[5 * k + 2];
+        nr[k] = fmaxf(sqrtf(rx * rx + ry * ry + rz * rz), 1e-12f);
+        mu[k][0] = rx / nr[k]; mu[k][1] = ry / nr[k]; mu[k][2] = rz / nr[k];
+        s[k] = o[5 * k + 3];
+        lam[k] = fminf(softplus(s[k]) + kLambdaMin, kLambdaMax);
+        w[k] = __expf(o[5 * k + 4] - amax);
+        wsum += w[k];
+    }
+    float p = 0.f;
+    for (int k = 0; k < 8; ++k) {
+        w[k] /= wsum;
+        cosk[k] = mu[k][0] * d.x + mu[k][1] * d.y + mu[k][2] * d.z;
+        f[k] = lam[k] / (2.f * wrd::kPi * -expm1f(-2.f * lam[k])) * __expf(lam[k] * (cosk[k] - 1.f));
+        p += w[k] * f[k];
+    }
+    p = fmaxf(p, 1e-30f);
+    const float cc = fminf(c, c_max);
+    for (int k = 0; k < 8; ++k) {
+        const float resp = w[k] * f[k] / p;
+        const float e2 = __expf(-2.f * lam[k]);
+        const float dldl = 1.f / lam[k] - 2.f * e2 / -expm1f(-2.f * lam[k]) + (cosk[k] - 1.f);
+        const float sig = 1.f / (1.f + __expf(-s[k]));
+        go[5 * k + 4] = -cc * (resp - w[k]);
+        go[5 * k + 3] = -cc * resp * dldl * sig;
+        const float a = -cc * resp * lam[k] / nr[k];
+        go[5 * k + 0] = a * (d.x - mu[k][0] * cosk[k]);
+        go[5 * k + 1] = a * (d.y - mu[k][1] * cosk[k]);
+        go[5 * k + 2] = a * (d.z - mu[k][2] * cosk[k]);
+    }
+    for (int k = 40; k < kW; ++k) go[k] = 0.f;
+    return -cc * logf(p);
+}
+
+// training records: kRecordFloat4 float4 each (layout in wr_guide.h)
+// rows [first, count) of the minibatch map to records (row * stride) % total (a fixed shuffle
+// when stride and total are coprime)
+__global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 *records, const uint32_t *count_dev,
+                                                      uint32_t count_host, uint32_t first, uint32_t total,
+                                                      uint32_t stride, float c_max, double *loss_out) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *wt = smem;                       // W tiles   5 x 8 KB
+    unsigned char *wtt = smem + 40960;              // W^T tiles 5 x 8 KB
+    unsigned char *xt = smem + 81920;               // X_0..X_4  5 x 16 KB
+    // dH: 16 KB + 8 KB of zeroed padding, so that the operand reach of the weight-gradient
+    // MMA stays inside this allocation for either reading of the descriptor's two strides
+    unsigned char *dh = smem + 163840;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kTrainBarrier);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kTrainBarrier + 8);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) tmem_alloc(smem_addr(slot), 512);
+    if (tid == 0) mbar_init(smem_addr(mbar), 1);
+    load_weights(wt, g.w);
+    load_weights(wtt, g.wt);
+    for (int i = tid; i < 8192 / 4; i += blockDim.x) reinterpret_cast<uint32_t *>(dh + 16384)[i] = 0u;
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *slot;
+    const uint32_t tD = tmem, tdW = tmem + 64;       // columns [0,64) scratch, [64, 384) dW of layers 0..4
+    const uint32_t lane_base = uint32_t(warp * 32) << 16;
+    uint32_t n = count_dev ? *count_dev : count_host;
+    n = n > first ? n - first : 0u;
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    const uint32_t id_fwd = idesc_bf16(128, 64, 0, 0);
+    const uint32_t id_dw = idesc_bf16(64, 64, 1, 1);
+    uint32_t phase = 0;
+    bool failed = false, any_tile = false;
+    double loss = 0.0;
+    for (uint32_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+        const uint32_t row = tile * kTile + tid;
+        const bool valid = row < n;
+        float x[kW];
+        f3 dir = mk(0.f, 1.f, 0.f);
+        float c = 0.f;
+        if (valid) {
+            const uint32_t ri = uint32_t((uint64_t(first + row) * stride) % (total ? total : 1u));
+            const float4 *rec = records + kRecordFloat4 * size_t(ri);
+            const float4 s0 = rec[0], s1 = rec[1], s2 = rec[2], s3 = rec[3];
+            encode(mk(s0.x, s0.y, s0.z), mk(s1.x, s1.y, s1.z), mk(s2.x, s2.y, s2.z), g, x);
+            dir = mk(s3.x, s3.y, s3.z);
+            c = s0.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < kW; ++k) x[k] = 0.f;
+        }
+        store_row(xt, tid, x);
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        // forward; X_l kept for the backward pass
+        float out[kW];
+        for (int l = 0; l < kLayers; ++l) {
+            if (tid == 0) {
+                const uint32_t a0 = smem_addr(xt + l * 16384), b0 = smem_addr(wt + l * 8192);
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks)
+                    mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 256, 128, 1024), id_fwd,
+                             ks > 0 ? 1u : 0u);
+                mma_commit(smem_addr(mbar));
+            }
+            const bool ok = mbar_wait(smem_addr(mbar), phase, kWaitIters);
+            phase ^= 1u;
+            if (__syncthreads_or(!ok)) { failed = true; break; }
+            fence_after_sync();
+            tmem_ld64(tD + lane_base, out);
+            if (l < kLayers - 1) store_row_relu(xt + (l + 1) * 16384, tid, out);
+            fence_async_smem();
+            fence_before_sync();
+            __syncthreads();
+            fence_after_sync();
+        }
+        if (failed) break;
+        // loss gradient at the outputs -> dH (bf16)
+        float go[kW];
+        if (valid && c > 0.f) {
+            loss += double(loss_grad(out, dir, c, c_max, go));
+        } else {
+#pragma unroll
+            for (int k = 0; k < kW; ++k) go[k] = 0.f;
+        }
+        store_row(dh, tid, go);
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        // backward
+        for (int l = kLayers - 1; l >= 0; --l) {
+            if (tid == 0) {
+                // dW_l += dH^T X_l : M = 64 (out), N = 64 (in), K = 128 (rows), MN-major operands
+                const uint32_t a0 = smem_addr(dh), b0 = smem_addr(xt + l * 16384);
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks)
+                    mma_bf16(tdW + 64 * l, smem_desc(a0 + ks * 2048, 1024, 128), smem_desc(b0 + ks * 2048, 1024, 128),
+                             id_dw, (any_tile || ks > 0) ? 1u : 0u);
+                if (l > 0) {
+                    // dX = dH W_l : M = 128, N = 64 (in), K = 64 (out); B = W^T tile
+                    const uint32_t c0 = smem_addr(wtt + l * 8192);
+#pragma unroll
+                    for (int ks = 0; ks < 4; ++ks)
+                        mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(c0 + ks * 256, 128, 1024), id_fwd,
+                                 ks > 0 ? 1u : 0u);
+                }
+                mma_commit(smem_addr(mbar));
+            }
+            const bool ok = mbar_wait(smem_addr(mbar), phase, kWaitIters);
+            phase ^= 1u;
+            if (__syncthreads_or(!ok)) { failed = true; break; }
+            fence_after_sync();
+            if (l > 0) {
+                float v[kW];
+                tmem_ld64(tD + lane_base, v);
+                relu_mask_row(xt + l * 16384, tid, v);   // input of layer l = ReLU output of layer l-1
+                store_row(dh, tid, v);
+            }
+            fence_async_smem();
+            fence_before_sync();
+            __syncthreads();
+            fence_after_sync();
+        }
+        any_tile = true;
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(g.err, 1u);
+    } else {
+        // this CTA's dW into its own partial slot (summed in a fixed order by the optimiser, so
+        // the gradient is deterministic). M = 64 accumulator row n lives in TMEM lane
+        // (n % 16) + 32 (n / 16); a CTA without tiles writes zeros.
+        const int lane = tid & 31;
+        float *slot_base = g.partial + size_t(blockIdx.x) * kParams;
+        for (int l = 0; l < kLayers; ++l) {
+            float v[kW];
+            if (any_tile) {
+                tmem_ld64(tdW + 64 * l + lane_base, v);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kW; ++k) v[k] = 0.f;
+            }
+            if (lane < 16) {
+                float4 *gr = reinterpret_cast<float4 *>(slot_base + l * kW * kW + (16 * warp + lane) * kW);
+#pragma unroll
+                for (int k = 0; k < kW / 4; ++k) gr[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+            }
+        }
+    }
+    if (loss_out) {
+        // block reduction of the loss
+        __shared__ double red[kTile];
+        red[tid] = loss;
+        __syncthreads();
+        for (int s = kTile / 2; s > 0; s >>= 1) {
+            if (tid < s) red[tid] += red[tid + s];
+            __syncthreads();
+        }
+        if (tid == 0) atomicAdd(loss_out, red[0]);
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+// ------------------------------------------------------------- optimiser ----
+__device__ __forceinline__ float sum_partials(const GuideNet &g, int i) {
+    float s = 0.f;
+    for (int k = 0; k < g.slots; ++k) s += g.partial[size_t(k) * kParams + i];
+    return s;
+}
+
+// the summed gradient into g.grad (for callers that read it)
+__global__ void k_guide_sum(GuideNet g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x)
+        g.grad[i] = sum_partials(g, i);
+}
+
+__global__ void k_guide_adam(GuideNet g, float lr, float scale, int step, int apply) {
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        const int l = i / (kW * kW), nrow = (i / kW) % kW, k = i % kW;
+        float w = g.master[i];
+        if (apply) {
+            const float gr = sum_partials(g, i) * scale;
+            const float m = b1 * g.m[i] + (1.f - b1) * gr;
+            const float v = b2 * g.v[i] + (1.f - b2) * gr * gr;
+            g.m[i] = m;
+            g.v[i] = v;
+            w -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+        }
+        if (l < kLayers - 1 && nrow == kW - 1) w = (k == kW - 1) ? 1.f : 0.f;   // the constant unit
+        g.master[i] = w;
+        const __nv_bfloat16 h = __float2bfloat16_rn(w);
+        g.w[i] = h;
+        g.wt[l * kW * kW + k * kW + nrow] = h;
+    }
+}
+
+// sum of c and number of records with c > 0 over records [0, n)
+__global__ void k_guide_cstats(const float4 *records, uint32_t n, double *out) {
+    __shared__ double red[2][256];
+    double sum = 0.0, cnt = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float c = records[kRecordFloat4 * size_t(i)].w;
+        if (c > 0.f && isfinite(c)) { sum += double(c); cnt += 1.0; }
+    }
+    red[0][threadIdx.x] = sum;
+    red[1][threadIdx.x] = cnt;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (int(threadIdx.x) < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(out, red[0][0]);
+        atomicAdd(out + 1, red[1][0]);
+    }
+}
+
+__global__ void k_guide_init(GuideNet g, uint32_t seed) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
+        const int l = i / (kW * kW);
+        const uint4 h = wrd::pcg4d(make_uint4(uint32_t(i), seed, 0x6a09e667u, 77u));
+        const float u = wrd::u01(h.x) * 2.f - 1.f;
+        const float limit = sqrtf(6.f / float(kW + kW)) * (l == kLayers - 1 ? 0.1f : 1.f);
+        g.master[i] = u * limit;
+        g.m[i] = 0.f;
+        g.v[i] = 0.f;
+        g.grad[i] = 0.f;
+    }
+}
+
+}  // namespace wrg
+
+// ------------------------------------------------------------------ host ----
+namespace wrg {
+
+static void check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess)
+        throw wr::Error(e == cudaErrorMemoryAllocation ? WR_ERR_OUT_OF_MEMORY : WR_ERR_CUDA,
+                        std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+constexpr size_t kTrainSmem = kTrainBarrier + 64;
+
+void guide_alloc(GuideNet &g) {
+    check(cudaMalloc(&g.w, kParams * 2), "guide alloc");
+    check(cudaMalloc(&g.wt, kParams * 2), "guide alloc");
+    check(cudaMalloc(&g.master, kParams * 4), "guide alloc");
+    check(cudaMalloc(&g.grad, kParams * 4), "guide alloc");
+    int dev = 0, sms = 148;
+    check(cudaGetDevice(&dev), "guide alloc");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "guide alloc");
+    g.slots = sms;
+    check(cudaMalloc(&g.partial, size_t(g.slots) * kParams * 4), "guide alloc");
+    check(cudaMalloc(&g.m, kParams * 4), "guide alloc");
+    check(cudaMalloc(&g.v, kParams * 4), "guide alloc");
+    check(cudaMalloc(&g.err, 4), "guide alloc");
+    check(cudaMemset(g.err, 0, 4), "guide memset");
+    check(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kInferSmem)),
+          "guide smem attribute");
+    check(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)),
+          "guide smem attribute");
+}
+
+void guide_free(GuideNet &g) {
+    for (void *p : {(void *)g.w, (void *)g.wt, (void *)g.master, (void *)g.grad, (void *)g.partial, (void *)g.m,
+                    (void *)g.v,
+                    (void *)g.err})
+        if (p) cudaFree(p);
+    g = GuideNet{};
+}
+
+void guide_init(GuideNet &g, uint32_t seed, cudaStream_t st) {
+    k_guide_init<<<40, 512, 0, st>>>(g, seed);
+    k_guide_adam<<<40, 512, 0, st>>>(g, 0.f, 0.f, 1, 0);   // constant unit, bf16 copies
+    check(cudaGetLastError(), "guide init");
+}
+
+void guide_set_master(GuideNet &g, const float *host_w, cudaStream_t st) {
+    check(cudaMemcpyAsync(g.master, host_w, kParams * 4, cudaMemcpyHostToDevice, st), "guide set");
+    k_guide_adam<<<40, 512, 0, st>>>(g, 0.f, 0.f, 1, 0);
+    check(cudaGetLastError(), "guide set");
+}
+
+void guide_get_master(const GuideNet &g, float *host_w, cudaStream_t st) {
+    check(cudaMemcpyAsync(host_w, g.master, kParams * 4, cudaMemcpyDeviceToHost, st), "guide get");
+    check(cudaStreamSynchronize(st), "guide get");
+}
+
+int infer_grid(int sms) { return sms * 3; }   // three CTAs per SM (shared memory and registers)
+
+void guide_infer_rows(const GuideNet &g, const float *rows_dev, uint32_t n, float4 *lobes_dev, int sms, cudaStream_t st) {
+    InferSource s{};
+    s.rows = rows_dev;
+    s.nrows = n;
+    k_guide_infer<<<infer_grid(sms), kTile * kGroups, kInferSmem, st>>>(g, s, lobes_dev, nullptr, 0);
+    check(cudaGetLastError(), "guide infer");
+}
+
+void guide_infer_wavefront(const GuideNet &g, const float4 *o, const float4 *d, const float4 *hit, const uint32_t *count,
+                           const float4 *tris, const uint32_t *tri_mat, uint4 *lobes_packed, size_t stride, int sms,
+                           cudaStream_t st) {
+    InferSource s{};
+    s.o = o; s.d = d; s.hit = hit; s.count = count; s.tris = tris; s.tri_mat = tri_mat;
+    k_guide_infer<<<infer_grid(sms), kTile * kGroups, kInferSmem, st>>>(g, s, nullptr, lobes_packed, stride);
+}
+
+void guide_gradient(GuideNet &g, const float4 *records_dev, const uint32_t *count_dev, uint32_t count_host,
+                    uint32_t first, uint32_t total, uint32_t stride, float c_max, double *loss_dev, int sms,
+                    cudaStream_t st) {
+    // one CTA per partial-gradient slot (the shared memory allows one CTA per SM)
+    k_guide_train<<<g.slots, kTile, kTrainSmem, st>>>(g, records_dev, count_dev, count_host, first, total, stride,
+                                                      c_max, loss_dev);
+    check(cudaGetLastError(), "guide train");
+}
+
+void guide_cstats(const float4 *records_dev, uint32_t n, double *out_dev, int sms, cudaStream_t st) {
+    check(cudaMemsetAsync(out_dev, 0, 16, st), "guide cstats");
+    if (n) k_guide_cstats<<<sms * 2, 256, 0, st>>>(records_dev, n, out_dev);
+    check(cudaGetLastError(), "guide cstats");
+}
+
+void guide_sum_gradient(GuideNet &g, cudaStream_t st) {
+    k_guide_sum<<<40, 512, 0, st>>>(g);
+    check(cudaGetLastError(), "guide sum");
+}
+
+void guide_adam(GuideNet &g, float lr, float scale, int step, cudaStream_t st) {
+    k_guide_adam<<<40, 512, 0, st>>>(g, lr, scale, step, 1);
+    check(cudaGetLastError(), "guide adam");
+}
+
+}  // namespace wrg

@@ -1,0 +1,245 @@
+// The guiding network's per-tile building blocks, shared by the stand-alone
+// inference / training kernels (wr_guide.cu) and the fused guided shade kernel
+// (wr_kernels.cu): feature encoding, the bf16 canonical operand tiles, the
+// five-layer tcgen05 forward pass over one 128-row tile, and the output
+// transform to von Mises-Fisher lobes.
+#pragma once
+
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "wr_device.cuh"
+#include "wr_guide.h"
+#include "wr_guide_tc.cuh"
+
+namespace wrg {
+
+using wrd::f3;
+using wrd::mk;
+
+constexpr int kLayers = kGuideLayers;
+constexpr int kW = kGuideWidth;              // layer width (inputs and outputs)
+constexpr int kParams = kGuideParams;
+constexpr int kTile = 128;                   // rows per tile = threads per CTA
+constexpr uint32_t kWaitIters = 1u << 24;    // bounded mbarrier waits
+constexpr int kWeightBytes = kLayers * 8192; // 5 bf16 64x64 tiles
+constexpr int kLastRows = 48;                // output rows of the last layer that inference computes (40 used)
+constexpr int kWeightBytesInfer = (kLayers - 1) * 8192 + kLastRows * kW * 2;
+constexpr int kActBytes = kTile * kW * 2;    // one 128 x 64 bf16 activation tile
+
+// ------------------------------------------------------------------ encoding ----
+// 64 features: p in [0,1]^3, sin/cos(2^f pi p) for f = 0..5, n, wo, sin/cos(pi n),
+// sin/cos(pi wo), six zeros, the constant 1. sincospif gives sin/cos(pi p); the
+// higher frequencies follow by the double-angle identities (sin 2a = 2 sin a cos a,
+// cos 2a = 1 - 2 sin^2 a), whose error (a few 1e-6 after five doublings) is far
+// below the bf16 rounding of the features.
+__device__ __forceinline__ void encode(f3 p, f3 n, f3 wo, const GuideNet &g, float *x) {
+    const float q[3] = {(p.x - g.box_lo[0]) * g.box_inv[0], (p.y - g.box_lo[1]) * g.box_inv[1],
+                        (p.z - g.box_lo[2]) * g.box_inv[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        x[a] = q[a];
+        float sn, cs;
+        sincospif(q[a], &sn, &cs);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            x[3 + 6 * f + a] = sn;
+            x[6 + 6 * f + a] = cs;
+            const float s2 = 2.f * sn * cs, c2 = 1.f - 2.f * sn * sn;
+            sn = s2;
+            cs = c2;
+        }
+    }
+    const float nv[3] = {n.x, n.y, n.z}, wv[3] = {wo.x, wo.y, wo.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        x[39 + a] = nv[a];
+        x[42 + a] = wv[a];
+        sincospif(nv[a], &x[45 + a], &x[48 + a]);
+        sincospif(wv[a], &x[51 + a], &x[54 + a]);
+    }
+#pragma unroll
+    for (int k = 57; k < 63; ++k) x[k] = 0.f;
+    x[63] = 1.f;
+}
+
+// one 64-wide row of a canonical tile: 8 stores of 16 bytes (8 bf16 each)
+__device__ __forceinline__ void store_row(unsigned char *tile, int row, const float *v) {
+#pragma unroll
+    for (int c = 0; c < kW; c += 8) {
+        uint4 q;
+        __nv_bfloat162 h0 = __floats2bfloat162_rn(v[c], v[c + 1]), h1 = __floats2bfloat162_rn(v[c + 2], v[c + 3]),
+                       h2 = __floats2bfloat162_rn(v[c + 4], v[c + 5]), h3 = __floats2bfloat162_rn(v[c + 6], v[c + 7]);
+        q.x = *reinterpret_cast<uint32_t *>(&h0);
+        q.y = *reinterpret_cast<uint32_t *>(&h1);
+        q.z = *reinterpret_cast<uint32_t *>(&h2);
+        q.w = *reinterpret_cast<uint32_t *>(&h3);
+        *reinterpret_cast<uint4 *>(tile + tile_offset(row, c)) = q;
+    }
+}
+
+// multiplies v by the mask (x > 0) of a stored row
+__device__ __forceinline__ void relu_mask_row(const unsigned char *tile, int row, float *v) {
+#pragma unroll
+    for (int c = 0; c < kW; c += 8) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(tile + tile_offset(row, c));
+        const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            // a bf16 is positive when its sign bit is clear and it is not +0
+            const uint32_t lo = wds[j] & 0xffffu, hi = wds[j] >> 16;
+            if (!(lo != 0u && lo < 0x8000u)) v[c + 2 * j] = 0.f;
+            if (!(hi != 0u && hi < 0x8000u)) v[c + 2 * j + 1] = 0.f;
+        }
+    }
+}
+
+// bf16 weights [l][n][k] -> canonical tiles (rows n, columns k), 16 bytes at a time;
+// rows >= last_rows of the last layer are not loaded
+__device__ __forceinline__ void load_weights(unsigned char *dst, const __nv_bfloat16 *src, int last_rows = kW) {
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+    for (int i = threadIdx.x; i < kParams / 8; i += blockDim.x) {
+        const int l = i / (kW * kW / 8), n = (i / (kW / 8)) % kW, k = (i % (kW / 8)) * 8;
+        if (l == kLayers - 1 && n >= last_rows) continue;
+        *reinterpret_cast<uint4 *>(dst + l * 8192 + tile_offset(n, k)) = __ldg(s4 + i);
+    }
+}
+
+// columns [c0, c0 + 8 * chunks) of a row of a canonical tile from FP32 values v[0..] with
+// ReLU applied (cvt.rn.relu)
+__device__ __forceinline__ void store_row_relu(unsigned char *tile, int row, const float *v, int c0 = 0,
+                                               int chunks = kW / 8) {
+#pragma unroll
+    for (int j = 0; j < chunks; ++j) {
+        uint4 q;
+        q.x = relu_bf16x2(v[8 * j], v[8 * j + 1]);
+        q.y = relu_bf16x2(v[8 * j + 2], v[8 * j + 3]);
+        q.z = relu_bf16x2(v[8 * j + 4], v[8 * j + 5]);
+        q.w = relu_bf16x2(v[8 * j + 6], v[8 * j + 7]);
+        *reinterpret_cast<uint4 *>(tile + tile_offset(row, c0 + 8 * j)) = q;
+    }
+}
+
+// ------------------------------------------------------------------ forward ----
+// The five layers over the 128-row tile whose features are stored in `at` by the 128
+// threads of one warpgroup (stores fenced for the async proxy, the group synchronised
+// on named barrier `bar` by the caller). Thread r of the group (r = threadIdx.x % 128)
+// receives row r's raw outputs in `out`. The group's first thread issues each layer's
+// four K=16 MMAs (M=128, N=64; N=last_n for the last layer) into the 64 TMEM columns at
+// `tmem`; every thread waits on the group's mbarrier (bounded) and reads its TMEM lane
+// back. Returns false on every thread of the group when a wait timed out (the caller
+// then does not use the outputs). On return the tensor core no longer reads `at`;
+// out[0..47] hold the last layer's outputs (out[48..63] are undefined).
+__device__ __forceinline__ bool mlp_forward_tile(unsigned char *at, const unsigned char *wt, uint64_t *mbar,
+                                                 uint32_t tmem, uint32_t &phase, float *out, int bar,
+                                                 int last_n = kW) {
+    const int r = threadIdx.x & 127;
+    const uint32_t lane_base = uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16;
+    for (int l = 0; l < kLayers; ++l) {
+        if (r == 0) {
+            const uint32_t idesc = idesc_bf16(128, l == kLayers - 1 ? last_n : kW, 0, 0);
+            const uint32_t a0 = smem_addr(at), b0 = smem_addr(wt + l * 8192);
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks)
+                mma_bf16(tmem, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 256, 128, 1024), idesc,
+                         ks > 0 ? 1u : 0u);
+            mma_commit(smem_addr(mbar));
+        }
+        const bool ok = mbar_wait(smem_addr(mbar), phase, kWaitIters);
+        phase ^= 1u;
+        if (group_any(bar, !ok)) return false;
+        fence_after_sync();
+        if (l < kLayers - 1) {   // hidden layer: two halves of 32 columns (fewer live registers)
+            tmem_ld32(tmem + lane_base, out);
+            store_row_relu(at, r, out, 0, 4);
+            tmem_ld32(tmem + lane_base + 32, out);
+            store_row_relu(at, r, out, 32, 4);
+            fence_async_smem();
+        } else {                 // outputs 0..47
+            tmem_ld32(tmem + lane_base, out);
+            tmem_ld16(tmem + lane_base + 32, out + 32);
+        }
+        fence_before_sync();
+        group_sync(bar);
+        fence_after_sync();
+    }
+    return true;
+}
+
+// -------------------------------------------------------------- output lobes ----
+// lobe parameters from raw outputs (the transform of oracle/guide_oracle.py: axis
+// normalised, sharpness softplus + kLambdaMin, weights softmax)
+struct Lobes {
+    float mu[8][3], lam[8], w[8];
+};
+
+__device__ __forceinline__ float softplus(float s) { return s > 20.f ? s : log1pf(__expf(s)); }
+
+__device__ __forceinline__ void raw_to_lobes(const float *o, Lobes &L) {
+    float amax = -1e30f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) amax = fmaxf(amax, o[5 * k + 4]);
+    float wsum = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float rx = o[5 * k], ry = o[5 * k + 1], rz = o[5 * k + 2];
+        const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
+        if (nr > 1e-12f) { L.mu[k][0] = rx / nr; L.mu[k][1] = ry / nr; L.mu[k][2] = rz / nr; }
+        else { L.mu[k][0] = 0.f; L.mu[k][1] = 1.f; L.mu[k][2] = 0.f; }
+        L.lam[k] = fminf(softplus(o[5 * k + 3]) + kLambdaMin, kLambdaMax);
+        L.w[k] = __expf(o[5 * k + 4] - amax);
+        wsum += L.w[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) L.w[k] /= wsum;
+}
+
+// ------------------------------------------------------------ packed lobes ----
+// The render keeps each path's lobes as halves in five 16-byte chunks, stored
+// chunk-major in HBM (chunk c of wavefront slot i at c * capacity + i, coalesced):
+//   chunk 0/1/2 = axis x/y/z of lobes 0..7, chunk 3 = sharpness, chunk 4 = weight.
+// The shade kernel loads the five chunks of its path once into registers. Sampling and
+// density evaluation both use these rounded values (the axis is renormalised after
+// loading, the weights divided by their sum), so the density used for MIS is exactly the
+// density that is sampled.
+struct PackedLobes {
+    uint4 c[kPackedChunks];
+
+    __device__ __forceinline__ void load(int chunk, float *v) const {
+        const uint4 q = c[chunk];
+        const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&wds[j]));
+            v[2 * j] = f.x;
+            v[2 * j + 1] = f.y;
+        }
+    }
+};
+
+__device__ __forceinline__ void store_packed_lobes(uint4 *base, size_t stride, size_t slot, const Lobes &L,
+                                                   bool valid) {
+    float v[kPackedChunks][8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        v[0][k] = L.mu[k][0];
+        v[1][k] = L.mu[k][1];
+        v[2][k] = L.mu[k][2];
+        v[3][k] = L.lam[k];
+        v[4][k] = valid ? L.w[k] : 0.f;   // zero weights: no guide for this slot
+    }
+#pragma unroll
+    for (int c = 0; c < kPackedChunks; ++c) {
+        uint4 q;
+        __half2 h0 = __floats2half2_rn(v[c][0], v[c][1]), h1 = __floats2half2_rn(v[c][2], v[c][3]),
+                h2 = __floats2half2_rn(v[c][4], v[c][5]), h3 = __floats2half2_rn(v[c][6], v[c][7]);
+        q.x = *reinterpret_cast<uint32_t *>(&h0);
+        q.y = *reinterpret_cast<uint32_t *>(&h1);
+        q.z = *reinterpret_cast<uint32_t *>(&h2);
+        q.w = *reinterpret_cast<uint32_t *>(&h3);
+        base[c * stride + slot] = q;
+    }
+}
+
+}  // namespace wrg

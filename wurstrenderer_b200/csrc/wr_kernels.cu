@@ -23,6 +23,9 @@
 #include <cuda_runtime.h>
 
 #include "wr_device.cuh"
+#include "wr_guide.h"
+#include "wr_guide_dev.cuh"
+#include "wr_guide_net.cuh"
 #include "wr_kernels.h"
 #include "wr_trace.cuh"
 
@@ -277,6 +280,7 @@ __device__ __forceinline__ LightVtx sample_light(const DevScene &s, float u0, fl
 struct PathState {
     float4 *o, *d, *thr;
     uint32_t *meta;     // depth (bits 0-7) | job (bits 8-31)
+    uint32_t *rec;      // newest training record of the path (only while records are collected)
 };
 
 struct ShadowQueue {
@@ -301,6 +305,11 @@ struct WaveArgs {
     cudaGraphConditionalHandle cond;   // while-loop condition of the captured graph (0: none)
     int has_cond;
     unsigned long long *prof;   // profiling totals (nullptr when off): items[6], extend nv/nt, shadow nv/nt
+    // learned guiding (nullptr when off)
+    const uint4 *lobes;    // packed lobes of the current wavefront (chunk c of slot i at c * capacity + i)
+    float4 *records;       // training records (kRecordFloat4 float4 each), nullptr: not collected
+    uint32_t *rec_count;
+    uint32_t rec_capacity;
 };
 
 __device__ __forceinline__ const DevJob &job_at(const WaveArgs &w, uint32_t j) { return w.jobs ? w.jobs[j] : w.job0; }
@@ -341,13 +350,14 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred, ui
     return base + __popc(mask & ((1u << lane_id()) - 1u));
 }
 
-__device__ __forceinline__ void push_shadow(const WaveArgs &w, bool pred, f3 o, f3 d, float tmax, uint32_t slot, f3 c) {
+__device__ __forceinline__ void push_shadow(const WaveArgs &w, bool pred, f3 o, f3 d, float tmax, uint32_t slot, f3 c,
+                                            uint32_t rec = wrg::kNoRecord) {
     uint32_t n;
     const uint32_t idx = warp_append(w.ctr + CTR_SHADOW, pred, n);
     if (pred && idx < w.shadow_capacity) {
         w.sq.o[idx] = make_float4(o.x, o.y, o.z, tmax);
         w.sq.d[idx] = make_float4(d.x, d.y, d.z, __uint_as_float(slot));
-        w.sq.c[idx] = make_float4(c.x, c.y, c.z, 0.f);
+        w.sq.c[idx] = make_float4(c.x, c.y, c.z, __uint_as_float(rec));
     }
 }
 
@@ -379,129 +389,210 @@ __global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
     }
 }
 
-__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, WaveArgs w) {
+// One path of the current wavefront: emitter hit (strategy B) or NEE at a surface
+// (strategy A, one shadow ray), then BSDF sampling -- or, with lobes `gl` of the learned
+// proposal, one-sample MIS between the guide and the BSDF -- and compaction of the
+// continued path into the next wavefront. Called by all 32 lanes of a warp together
+// (warp-aggregated appends); `valid` is false for lanes past the end of the wavefront.
+__device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w, uint32_t i, bool valid,
+                                           const wrg::PackedLobes *gl) {
+    bool alive = false, shadow = false;
+    f3 so = mk(0, 0, 0), sd = mk(0, 0, 1), sc = mk(0, 0, 0);
+    float stmax = 0.f;
+    f3 no = mk(0, 0, 0), nd = mk(0, 0, 1), nthr = mk(0, 0, 0);
+    float npdf = 0.f;
+    uint32_t pixel = 0, sample = 0, meta = 0;
+    uint32_t rec = wrg::kNoRecord;      // newest training record of this path
+    uint32_t nrec = wrg::kNoRecord;     // record of the continued path
+    bool want_rec = false;              // a record is created for this vertex
+    f3 rec_pos = mk(0, 0, 0), rec_n = mk(0, 1, 0), rec_wo = mk(0, 1, 0), rec_thr = mk(0, 0, 0);
+    if (valid) {
+        const float4 o4 = w.cur.o[i], d4 = w.cur.d[i], t4 = w.cur.thr[i];
+        meta = w.cur.meta[i];
+        if (w.records) rec = w.cur.rec[i];
+        const uint32_t depth = meta & 0xffu, job = meta >> 8;
+        const DevJob &J = job_at(w, job);
+        const float4 h = w.hit[i];
+        const f3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
+        const float prevPdfW = o4.w;
+        pixel = __float_as_uint(d4.w);   // global film pixel
+        sample = __float_as_uint(t4.w);
+        const uint32_t tri = __float_as_uint(h.w);
+        const float t = h.x;
+        const bool primitive = J.integrator == INTEGRATOR_PRIMITIVE;
+        if (tri == MISS) {
+            if (s.has_env) {
+                // strategy B on the environment (pathnextevent.h:128-146); the primitive tracer
+                // takes the emission with weight one (primitivepath.h:49-53)
+                const float cPdfA = prevPdfW;   // ConvertToArea to an environment vertex: 1/|d|^2
+                const float lPdfA = primitive ? 0.f : s.env_select_pdf * env_pdf(s, d);
+                const float mis = primitive ? 1.f : cPdfA / (lPdfA + cPdfA);
+                const f3 c = thr * env_eval(s, d) * mis;
+                if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                    film_add(w, pixel, c);
+                    if (w.records) record_contribution(w.records, rec, c);
+                }
+            }
+        } else {
+            const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
+            const f3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(cc);
+            const f3 ng = normalize(cross(p1 - p0, p2 - p0));
+            const f3 pos = o + d * t;
+            const uint32_t mat = __ldg(s.tri_mat + tri);
+            if (mat & LIGHT_BIT) {
+                // strategy B: BSDF-sampled hit on an emitter
+                const uint32_t li = mat & ~LIGHT_BIT;
+                const float cosl = dot(ng, d);
+                if (cosl <= 0.f) {   // front face: evalLe1 (diffusearealight.h:48-53)
+                    const float cPdfA = prevPdfW * fabsf(cosl) / (t * t);
+                    const float lPdfA = __ldg(&s.lights[li].select_pdf) * __ldg(&s.lights[li].inv_area);
+                    const float mis = primitive ? 1.f : cPdfA / (lPdfA + cPdfA);
+                    const f3 c = thr * mk(__ldg(&s.lights[li].intensity[0]), __ldg(&s.lights[li].intensity[1]),
+                                          __ldg(&s.lights[li].intensity[2])) * mis;
+                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                        film_add(w, pixel, c);
+                        if (w.records) record_contribution(w.records, rec, c);
+                    }
+                }
+            } else if (int(depth) + 2 < J.nverts) {
+                const DevMaterial mm = s.materials[mat];
+                const Frame fr(ng);
+                const f3 wi = -d;
+                const f3 inL = fr.to_local(wi);
+                const uint32_t lpix = pixel - J.pix_offset, seed = job_seed(J, job);
+                // learned proposal at this vertex (one-sample MIS with BSDF sampling)
+                const bool guided = gl && !primitive && guide_weight_sum(*gl) > 0.f;
+                // strategy A: next-event estimation toward this sample's light vertex
+                const Rand4 r0 = rand4(lpix, sample, 0, seed);
+                LightVtx l{};
+                if (primitive) l.pdfA = 0.f;   // no connection to the light (primitivepath.h)
+                else l = sample_light(s, r0.a, r0.b);
+                f3 wo;
+                float G, convA, dist = 0.f;
+                if (l.env) {
+                    wo = l.pos;
+                    G = fabsf(dot(ng, wo));
+                    convA = 1.f;
+                } else {
+                    const f3 uv = l.pos - pos;
+                    const float d2 = len2(uv);
+                    dist = sqrtf(d2);
+                    wo = uv / dist;
+                    const float cl = fabsf(dot(l.n, wo));
+                    convA = cl / d2;
+                    G = fabsf(dot(ng, wo)) * convA;
+                }
+                const bool front = l.env || dot(l.n, wo) <= 0.f;   // light emits toward -wo
+                if (G > 0.f && front && l.pdfA > 0.f) {
+                    const f3 outL = fr.to_local(wo);
+                    const f3 f = bsdf_eval(mm, inL, outL);
+                    if (!is_zero(f)) {
+                        float pdfW = bsdf_pdf(mm, inL, outL);
+                        if (guided) pdfW = kGuideAlpha * guide_pdf(*gl, wo) + (1.f - kGuideAlpha) * pdfW;
+                        const float bsdfPdfA = pdfW * convA;
+                        const float mis = l.pdfA / (l.pdfA + bsdfPdfA);
+                        const float le1 = l.env ? 1.f : kInvPi;
+                        const f3 c = thr * f * (le1 * G * mis) * l.contrib;
+                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                            shadow = true;
+                            so = pos; sd = wo; sc = c;
+                            stmax = l.env ? __int_as_float(0x7f800000) : dist - kRayEps;
+                        }
+                    }
+                }
+                // BSDF sampling (or, when guided, the guide/BSDF mixture) continues the path
+                const Rand4 rb = rand4(lpix, sample, 2 + depth, seed);
+                f3 outL;
+                float pdfW;
+                f3 wgt;
+                if (!guided) {
+                    wgt = bsdf_sample(mm, inL, rb.a, rb.b, outL, pdfW);
+                } else if (rb.c < kGuideAlpha) {
+                    const f3 dg = guide_sample(*gl, rb.c * (1.f / kGuideAlpha), rb.a, rb.b);
+                    outL = fr.to_local(dg);
+                    const float pb = bsdf_pdf(mm, inL, outL);
+                    pdfW = kGuideAlpha * guide_pdf(*gl, dg) + (1.f - kGuideAlpha) * pb;
+                    wgt = pdfW > 0.f ? bsdf_eval(mm, inL, outL) * (fabsf(outL.y) / pdfW) : mk(0.f, 0.f, 0.f);
+                } else {
+                    float pb;
+                    const f3 wb = bsdf_sample(mm, inL, rb.a, rb.b, outL, pb);   // f cos / pb
+                    pdfW = pb;
+                    wgt = mk(0.f, 0.f, 0.f);
+                    if (pb > 0.f && !is_zero(wb)) {
+                        pdfW = kGuideAlpha * guide_pdf(*gl, normalize(fr.to_world(outL))) +
+                               (1.f - kGuideAlpha) * pb;
+                        wgt = wb * (pb / pdfW);
+                    }
+                }
+                if (!is_zero(wgt) && isfinite(wgt.x + wgt.y + wgt.z)) {
+                    alive = true;
+                    no = pos;
+                    nd = normalize(fr.to_world(outL));
+                    nthr = thr * wgt;
+                    npdf = pdfW;
+                    if (w.records) {
+                        want_rec = true;
+                        rec_pos = pos;
+                        rec_wo = wi;
+                        rec_n = wrg::guide_normal(ng, wi);
+                        rec_thr = thr;
+                    }
+                }
+            }
+        }
+    }
+    push_shadow(w, shadow, so, sd, stmax, pixel, sc, rec);
+    if (w.records) {   // training record of this vertex (parent: the path's previous record)
+        uint32_t nr;
+        const uint32_t r = warp_append(w.rec_count, want_rec, nr);
+        nrec = rec;
+        if (want_rec && r < w.rec_capacity) {
+            float4 *R = w.records + wrg::kRecordFloat4 * size_t(r);
+            R[0] = make_float4(rec_pos.x, rec_pos.y, rec_pos.z, 0.f);
+            R[1] = make_float4(rec_n.x, rec_n.y, rec_n.z, __uint_as_float(rec));
+            R[2] = make_float4(rec_wo.x, rec_wo.y, rec_wo.z, 0.f);
+            R[3] = make_float4(nd.x, nd.y, nd.z, 0.f);
+            R[4] = make_float4(rec_thr.x, rec_thr.y, rec_thr.z, 0.f);
+            nrec = r;
+        }
+    }
+    uint32_t cnt;
+    const uint32_t j = warp_append(w.ctr + CTR_NEXT, alive, cnt);
+    if (alive) {
+        w.nxt.o[j] = make_float4(no.x, no.y, no.z, npdf);
+        w.nxt.d[j] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel));
+        w.nxt.thr[j] = make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample));
+        w.nxt.meta[j] = meta + 1u;
+        if (w.records) w.nxt.rec[j] = nrec;
+    }
+}
+
+// GUIDED: the learned proposal is on (w.lobes); a separate instantiation keeps the plain
+// shade kernel's register count (and occupancy) unchanged
+template <bool GUIDED>
+__global__ void __launch_bounds__(kShadeBlock, GUIDED ? 2 : 1) k_shade(DevScene s, WaveArgs w) {
     const uint32_t n = w.ctr[CTR_ACTIVE];
     if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 1, (unsigned long long)n);
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t base = warp_global * 32u; base < n; base += nwarps * 32u) {
         const uint32_t i = base + lane_id();
-        const bool valid = i < n;
-        bool alive = false, shadow = false;
-        f3 so = mk(0, 0, 0), sd = mk(0, 0, 1), sc = mk(0, 0, 0);
-        float stmax = 0.f;
-        f3 no = mk(0, 0, 0), nd = mk(0, 0, 1), nthr = mk(0, 0, 0);
-        float npdf = 0.f;
-        uint32_t pixel = 0, sample = 0, meta = 0;
-        if (valid) {
-            const float4 o4 = w.cur.o[i], d4 = w.cur.d[i], t4 = w.cur.thr[i];
-            meta = w.cur.meta[i];
-            const uint32_t depth = meta & 0xffu, job = meta >> 8;
-            const DevJob &J = job_at(w, job);
-            const float4 h = w.hit[i];
-            const f3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
-            const float prevPdfW = o4.w;
-            pixel = __float_as_uint(d4.w);   // global film pixel
-            sample = __float_as_uint(t4.w);
-            const uint32_t tri = __float_as_uint(h.w);
-            const float t = h.x;
-            const bool primitive = J.integrator == INTEGRATOR_PRIMITIVE;
-            if (tri == MISS) {
-                if (s.has_env) {
-                    // strategy B on the environment (pathnextevent.h:128-146); the primitive tracer
-                    // takes the emission with weight one (primitivepath.h:49-53)
-                    const float cPdfA = prevPdfW;   // ConvertToArea to an environment vertex: 1/|d|^2
-                    const float lPdfA = primitive ? 0.f : s.env_select_pdf * env_pdf(s, d);
-                    const float mis = primitive ? 1.f : cPdfA / (lPdfA + cPdfA);
-                    const f3 c = thr * env_eval(s, d) * mis;
-                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) film_add(w, pixel, c);
-                }
+        if (GUIDED) {   // learned proposal: this path's packed lobes, loaded once
+            wrg::PackedLobes pl;
+            if (i < n) {
+#pragma unroll
+                for (int c = 0; c < wrg::kPackedChunks; ++c) pl.c[c] = w.lobes[c * size_t(w.capacity) + i];
             } else {
-                const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
-                const f3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(cc);
-                const f3 ng = normalize(cross(p1 - p0, p2 - p0));
-                const f3 pos = o + d * t;
-                const uint32_t mat = __ldg(s.tri_mat + tri);
-                if (mat & LIGHT_BIT) {
-                    // strategy B: BSDF-sampled hit on an emitter
-                    const uint32_t li = mat & ~LIGHT_BIT;
-                    const float cosl = dot(ng, d);
-                    if (cosl <= 0.f) {   // front face: evalLe1 (diffusearealight.h:48-53)
-                        const float cPdfA = prevPdfW * fabsf(cosl) / (t * t);
-                        const float lPdfA = __ldg(&s.lights[li].select_pdf) * __ldg(&s.lights[li].inv_area);
-                        const float mis = primitive ? 1.f : cPdfA / (lPdfA + cPdfA);
-                        const f3 c = thr * mk(__ldg(&s.lights[li].intensity[0]), __ldg(&s.lights[li].intensity[1]),
-                                              __ldg(&s.lights[li].intensity[2])) * mis;
-                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) film_add(w, pixel, c);
-                    }
-                } else if (int(depth) + 2 < J.nverts) {
-                    const DevMaterial mm = s.materials[mat];
-                    const Frame fr(ng);
-                    const f3 wi = -d;
-                    const f3 inL = fr.to_local(wi);
-                    const uint32_t lpix = pixel - J.pix_offset, seed = job_seed(J, job);
-                    // strategy A: next-event estimation toward this sample's light vertex
-                    const Rand4 r0 = rand4(lpix, sample, 0, seed);
-                    LightVtx l{};
-                    if (primitive) l.pdfA = 0.f;   // no connection to the light (primitivepath.h)
-                    else l = sample_light(s, r0.a, r0.b);
-                    f3 wo;
-                    float G, convA, dist = 0.f;
-                    if (l.env) {
-                        wo = l.pos;
-                        G = fabsf(dot(ng, wo));
-                        convA = 1.f;
-                    } else {
-                        const f3 uv = l.pos - pos;
-                        const float d2 = len2(uv);
-                        dist = sqrtf(d2);
-                        wo = uv / dist;
-                        const float cl = fabsf(dot(l.n, wo));
-                        convA = cl / d2;
-                        G = fabsf(dot(ng, wo)) * convA;
-                    }
-                    const bool front = l.env || dot(l.n, wo) <= 0.f;   // light emits toward -wo
-                    if (G > 0.f && front && l.pdfA > 0.f) {
-                        const f3 outL = fr.to_local(wo);
-                        const f3 f = bsdf_eval(mm, inL, outL);
-                        if (!is_zero(f)) {
-                            const float bsdfPdfA = bsdf_pdf(mm, inL, outL) * convA;
-                            const float mis = l.pdfA / (l.pdfA + bsdfPdfA);
-                            const float le1 = l.env ? 1.f : kInvPi;
-                            const f3 c = thr * f * (le1 * G * mis) * l.contrib;
-                            if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
-                                shadow = true;
-                                so = pos; sd = wo; sc = c;
-                                stmax = l.env ? __int_as_float(0x7f800000) : dist - kRayEps;
-                            }
-                        }
-                    }
-                    // BSDF sampling continues the path
-                    const Rand4 rb = rand4(lpix, sample, 2 + depth, seed);
-                    f3 outL;
-                    float pdfW;
-                    const f3 wgt = bsdf_sample(mm, inL, rb.a, rb.b, outL, pdfW);
-                    if (!is_zero(wgt) && isfinite(wgt.x + wgt.y + wgt.z)) {
-                        alive = true;
-                        no = pos;
-                        nd = normalize(fr.to_world(outL));
-                        nthr = thr * wgt;
-                        npdf = pdfW;
-                    }
-                }
+#pragma unroll
+                for (int c = 0; c < wrg::kPackedChunks; ++c) pl.c[c] = make_uint4(0u, 0u, 0u, 0u);
             }
-        }
-        push_shadow(w, shadow, so, sd, stmax, pixel, sc);
-        uint32_t cnt;
-        const uint32_t j = warp_append(w.ctr + CTR_NEXT, alive, cnt);
-        if (alive) {
-            w.nxt.o[j] = make_float4(no.x, no.y, no.z, npdf);
-            w.nxt.d[j] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel));
-            w.nxt.thr[j] = make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample));
-            w.nxt.meta[j] = meta + 1u;
+            shade_path(s, w, i, i < n, &pl);
+        } else {
+            shade_path(s, w, i, i < n, nullptr);
         }
     }
 }
+
 
 __device__ __forceinline__ uint32_t new_samples(const WaveArgs &w, uint32_t filled, unsigned long long issued) {
     const unsigned long long remaining = w.total_samples > issued ? w.total_samples - issued : 0ull;
@@ -532,7 +623,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
             const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), cfz = ld3(cam.fz), corg = ld3(cam.origin);
             const unsigned long long lid = id - J.sample_begin;
             const uint32_t lpix = uint32_t(lid % J.npix);
-            const uint32_t sample = uint32_t(lid / J.npix);
+            const uint32_t sample = J.sample_offset + uint32_t(lid / J.npix);
             const uint32_t seed = job_seed(J, job);
             const uint32_t px = lpix % uint32_t(cam.width), py = lpix / uint32_t(cam.width);
             const Rand4 r0 = rand4(lpix, sample, 0, seed);
@@ -613,6 +704,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
             w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(J.pix_offset + lpix));
             w.nxt.thr[j] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sample));
             w.nxt.meta[j] = job << 8;
+            if (w.records) w.nxt.rec[j] = wrg::kNoRecord;
         }
         push_shadow(w, shadow, so, sd, stmax, slot, sc);
     }
@@ -633,6 +725,7 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w) {
         if (!occ) {
             const float4 c = w.sq.c[i];
             film_add(w, __float_as_uint(d.w), mk(c.x, c.y, c.z));
+            if (w.records) record_contribution(w.records, __float_as_uint(c.w), mk(c.x, c.y, c.z));
         }
     }
     if (w.prof) {
@@ -670,7 +763,8 @@ __global__ void k_resolve(const double *film, double *out, uint32_t total_pix, c
          i += size_t(gridDim.x) * blockDim.x) {
         const uint32_t pix = uint32_t(i / 3);
         const DevJob &J = jobs ? jobs[job_of_pixel(jobs, njobs, pix)] : job0;
-        const double bs = 1.0 / double(J.spp), as = 1.0 / double(J.spp) / double(J.npix);
+        const double spp = double(J.spp_norm > 0 ? J.spp_norm : J.spp);
+        const double bs = 1.0 / spp, as = 1.0 / spp / double(J.npix);
         double c = 0.0;
         c += film[i] * bs;
         c += film[3 * size_t(total_pix) + i] * as;
@@ -780,8 +874,8 @@ using namespace wrd;
 static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &r) {
     WaveArgs w;
     const int c = parity & 1, n = c ^ 1;
-    w.cur = {b.o[c], b.d[c], b.thr[c], b.meta[c]};
-    w.nxt = {b.o[n], b.d[n], b.thr[n], b.meta[n]};
+    w.cur = {b.o[c], b.d[c], b.thr[c], b.meta[c], b.rec[c]};
+    w.nxt = {b.o[n], b.d[n], b.thr[n], b.meta[n], b.rec[n]};
     w.hit = b.hit;
     w.sq = {b.sh_o, b.sh_d, b.sh_c};
     w.film = b.film;
@@ -798,6 +892,10 @@ static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &
     w.cond = r.cond;
     w.has_cond = r.has_cond;
     w.prof = r.prof;
+    w.lobes = r.guide ? b.lobes : nullptr;
+    w.records = r.record ? b.records : nullptr;
+    w.rec_count = b.rec_count;
+    w.rec_capacity = b.rec_capacity;
     return w;
 }
 
@@ -810,7 +908,15 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
             else if (r.trace_block == 256) k_extend<256><<<r.grid_trace, 256, 0, st>>>(s, w);
             else k_extend<128><<<r.grid_trace, 128, 0, st>>>(s, w);
             break;
-        case KERNEL_SHADE: k_shade<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
+        case KERNEL_SHADE:
+            if (w.lobes) k_shade<true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else k_shade<false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            break;
+        case KERNEL_GUIDE:
+            if (r.guide)
+                wrg::guide_infer_wavefront(*r.guide, w.cur.o, w.cur.d, w.hit, w.ctr + CTR_ACTIVE, s.tris, s.tri_mat,
+                                           b.lobes, b.capacity, r.guide_sms, st);
+            break;
         case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
         case KERNEL_SHADOW:
             if (r.trace_block == 64) k_shadow<64><<<r.grid_trace, 64, 0, st>>>(s, w);
@@ -823,8 +929,8 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
 }
 
 void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity, cudaStream_t st) {
-    for (int k : {KERNEL_EXTEND, KERNEL_SHADE, KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE})
-        launch_kernel(k, s, b, r, parity, st);
+    for (int k : {KERNEL_EXTEND, KERNEL_GUIDE, KERNEL_SHADE, KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE})
+        if (k != KERNEL_GUIDE || r.guide) launch_kernel(k, s, b, r, parity, st);
 }
 
 void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st) {
@@ -864,7 +970,7 @@ int occupancy_blocks(int which, int trace_block) {
         else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256>, 256, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128>, 128, 0);
     } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false>, kShadeBlock, 0);
     }
     return nb;
 }

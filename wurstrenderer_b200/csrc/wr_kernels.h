@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "wr_device.cuh"
+#include "wr_guide.h"
 
 namespace wrk {
 
@@ -13,12 +14,17 @@ using namespace wrd;
 struct WaveBuffers {
     float4 *o[2], *d[2], *thr[2];
     uint32_t *meta[2];
+    uint32_t *rec[2];                  // per-slot training record (guided renders that collect records)
     float4 *hit;
     float4 *sh_o, *sh_d, *sh_c;
     double *film;                      // base (npix*3) then splat (npix*3)
     uint32_t *ctr;                     // CTR_COUNT counters
     unsigned long long *sample_next;
     uint32_t capacity, shadow_capacity;
+    uint4 *lobes;                      // packed lobes, wrg::kPackedChunks x capacity (guided renders)
+    float4 *records;                   // training records
+    uint32_t *rec_count;
+    uint32_t rec_capacity;
 };
 
 struct RenderLaunch {
@@ -33,10 +39,13 @@ struct RenderLaunch {
     cudaGraphConditionalHandle cond;   // while-loop condition when the loop body is captured in a graph
     int has_cond;
     unsigned long long *prof;   // device profiling totals or nullptr
+    const wrg::GuideNet *guide; // learned proposal used by shade (nullptr: plain NEE+MIS)
+    int record;                 // 1: collect training records
+    int guide_sms;              // SM count (grid of the inference kernel)
 };
 
 enum KernelId { KERNEL_EXTEND = 0, KERNEL_SHADE = 1, KERNEL_RAYGEN = 2, KERNEL_SHADOW = 3, KERNEL_ADVANCE = 4,
-                KERNEL_RESOLVE = 5 };
+                KERNEL_RESOLVE = 5, KERNEL_GUIDE = 6 };
 
 void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
                    cudaStream_t st);
