@@ -53,6 +53,11 @@ def scene_path(rank, world, dist, workload="heightfield"):
         d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_cornell_v1")
         p = os.path.join(d, "cornell.json")
         writer = lambda: scenes.write_cornell(d)
+    elif workload == "door":
+        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_door_v1")
+        p = os.path.join(d, "door.json")
+        writer = lambda: scenes.write_spec(d, "door", scenes.door_room_spec(seed=1004), scenes.DOOR_ROOM_CAMERA,
+                                           (1024, 1024), 256, 10)
     else:
         d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_v1")
         p = os.path.join(d, "heightfield_spheres.json")
@@ -204,6 +209,73 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def relmse(x, ref, eps=1e-2):
+    import numpy as np
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + eps)))
+
+
+DOOR_WORKLOAD = ("door_room_200k: closed 6x3x6 m room, 1x1 emitter behind a partition with a 0.2 m door gap, "
+                 "300 seeded Phong / Oren-Nayar boxes (197,782 triangles), 1024x1024, num_path_vertices 10")
+
+
+def guided_vs_plain(wr, plain_spp=256, seeds=2):
+    """Equal-time relMSE of the learned proposal against plain NEE+MIS on the door-gap room, both
+    measured against the reference's own FP64 render of a 128x128 crop at 16384 spp
+    (tests/golden/door_crop_ref_{a,b}.npy, two independent 8192-spp halves). The guided render
+    (training on its first 32 spp included) gets the device time of the plain render."""
+    import numpy as np
+    from wurstrenderer_b200 import scenes
+    gdir = os.path.join(ROOT, "tests", "golden")
+    meta_p = os.path.join(gdir, "door_crop_meta.json")
+    if not os.path.exists(meta_p):
+        return {"unavailable": "door-room reference crop not generated (tests/golden/make_door_golden.py)"}
+    meta = json.load(open(meta_p))
+    ref_a = np.load(os.path.join(gdir, "door_crop_ref_a.npy")).astype(np.float64)
+    ref_b = np.load(os.path.join(gdir, "door_crop_ref_b.npy")).astype(np.float64)
+    ref = 0.5 * (ref_a + ref_b)
+    x0, y0, x1, y1 = meta["crop"]
+    d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_door_v1")
+    p = os.path.join(d, "door.json")
+    if not os.path.exists(p + ".done"):
+        res = tuple(meta["resolution"])
+        scenes.write_spec(d, "door", scenes.door_room_spec(seed=1004), dict(scenes.DOOR_ROOM_CAMERA, resolution=list(res)),
+                          res, 64, meta["num_path_vertices"])
+        open(p + ".done", "w").write("ok")
+    out = {"workload": DOOR_WORKLOAD, "oracle": "reference PathNeeRenderer (FP64 CPU), 16384 spp, crop %s" % meta["crop"],
+           "relmse_def": "mean over crop pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)",
+           "oracle_noise_relmse": relmse(ref_a, ref_b) / 4.0}
+    with wr.Scene.from_file(p) as sc:
+        sc.render(spp=4, seed=1)                       # warm-up (allocations, graph paths)
+        sc.render(spp=8, seed=2, guiding=1, guide_train_spp=8, guide_steps=16)
+        plain_err, plain_ms = [], []
+        for i in range(seeds):
+            img = sc.render(spp=plain_spp, seed=100 + i)
+            plain_ms.append(sc.stats["render_ms"])
+            plain_err.append(relmse(img[y0:y1, x0:x1], ref))
+        t_budget = float(np.mean(plain_ms))
+        img = sc.render(spp=plain_spp, seed=200, guiding=1)     # calibration: guided time per spp
+        st = sc.stats
+        per_spp = (st["render_ms"] - st["guide_train_ms"]) / plain_spp
+        g_spp = max(33, int((t_budget - st["guide_train_ms"]) / per_spp))
+        g_err, g_ms, g_train = [], [], []
+        for i in range(seeds):
+            img = sc.render(spp=g_spp, seed=300 + i, guiding=1)
+            st = sc.stats
+            g_ms.append(st["render_ms"])
+            g_train.append(st["guide_train_ms"])
+            g_err.append(relmse(img[y0:y1, x0:x1], ref))
+            steps, records = st["guide_steps"], st["guide_records"]
+    pe, ge = float(np.mean(plain_err)), float(np.mean(g_err))
+    pm, gm = float(np.mean(plain_ms)), float(np.mean(g_ms))
+    out.update({"plain": {"spp": plain_spp, "relmse": pe, "ms": pm, "runs": seeds},
+                "guided": {"spp": g_spp, "relmse": ge, "ms": gm, "train_ms": float(np.mean(g_train)),
+                           "adam_steps": steps, "records": records, "runs": seeds},
+                "relmse_ratio_equal_time": (ge * gm) / (pe * pm),
+                "note": "ratio = (relMSE_guided x time_guided) / (relMSE_plain x time_plain); relMSE of an "
+                        "unbiased estimator scales as 1/time, so this is the equal-time ratio"})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,9 +287,11 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs only)")
     ap.add_argument("--quick", action="store_true", help="skip e2e, profile and CPU baseline (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="use the default wavefront settings")
-    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128"],
+    ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time study")
+    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128", "door"],
                     help="heightfield: the 1M-triangle single render (headline); jobs128: 128 batched jobs "
-                         "over the Cornell box, one graph launch per step")
+                         "over the Cornell box, one graph launch per step; door: one guided render (learned "
+                         "proposal trained on its first 32 spp) of the 200k-triangle door-gap room")
     args = ap.parse_args()
 
     world = env_int("WORLD_SIZE", 1)
@@ -278,7 +352,8 @@ def main():
                 j["seed"] = seed + k
             scene.render_batch(batch_jobs, queue_capacity=qc, **knobs)
             return scene.stats
-        scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc, **knobs)
+        scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc,
+                            guiding=1 if args.workload == "door" else 0, **knobs)
         st = scene.stats
         combine_films(film, world, dist)
         return st
@@ -385,6 +460,8 @@ def main():
             "mrays_per_s": (k_items["extend"] + k_items["shadow"]) * world * args.steps / (max_ms / 1e3) / 1e6}
     if rank == 0 and not args.no_cpu_baseline and batch_jobs is None:
         line["cpu_baseline"] = cpu_baseline(path)
+    if world == 1 and not args.no_guiding and batch_jobs is None:
+        line["equal_time_relmse"] = guided_vs_plain(wr)
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()

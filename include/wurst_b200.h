@@ -60,7 +60,9 @@ typedef struct wr_render_desc {
     int guide_pass_spp;      /* samples per pixel per training pass; 0 = about 2^22 paths per pass, at
                                 least four passes */
     int guide_batch;         /* training records per Adam step; 0 = 16384 */
-    int guide_steps;         /* Adam steps of the training phase, spread evenly over its passes; 0 = 2048 */
+    int guide_steps;         /* Adam steps of the training phase, spread evenly over its passes; 0 = a
+                                budget of about 8 % of the render's device time (estimated from the first
+                                pass), 256 to 8192 steps */
     float guide_clamp;       /* loss weights are clamped at guide_clamp x their mean over the pass;
                                 0 = 1000, < 0 = no clamp */
     int reserved[4];

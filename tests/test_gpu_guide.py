@@ -248,6 +248,42 @@ def test_door_room_guiding_reduces_error(wr_lib, tmp_path):
     with wr_lib.Scene.from_file(path) as sc:
         ref = np.mean([sc.render(spp=4096, seed=50 + i) for i in range(4)], axis=0)
         plain = [relmse(sc.render(spp=256, seed=90 + i), ref) for i in range(3)]
-        guided = [relmse(sc.render(spp=256, seed=90 + i, guiding=1), ref) for i in range(3)]
+        guided = [relmse(sc.render(spp=256, seed=90 + i, guiding=1, guide_steps=2048), ref) for i in range(3)]
     print("door room relMSE plain %s guided %s" % (plain, guided))
     assert np.mean(guided) < 0.8 * np.mean(plain), (plain, guided)
+
+
+def _door_reference():
+    import json
+    meta_p = os.path.join(GOLDEN, "door_crop_meta.json")
+    if not os.path.exists(meta_p):
+        pytest.skip("door-room reference crop not generated")
+    meta = json.load(open(meta_p))
+    a = np.load(os.path.join(GOLDEN, "door_crop_ref_a.npy")).astype(np.float64)
+    b = np.load(os.path.join(GOLDEN, "door_crop_ref_b.npy")).astype(np.float64)
+    return meta, a, b
+
+
+@pytest.mark.parametrize("guiding", [0, 1])
+def test_door_room_crop_matches_reference(wr_lib, tmp_path, guiding):
+    """The 200k-triangle door-gap room at full resolution (1024^2, 10 vertices) against the
+    reference's FP64 render of a 128x128 crop at 16384 spp: plain and guided renders (4 x 1024
+    spp) within the reference's noise floor, every 8x8 block |z| < 4, crop mean within 1%."""
+    from test_gpu_render import block_z
+    from wurstrenderer_b200 import scenes
+    meta, ref_a, ref_b = _door_reference()
+    res = tuple(meta["resolution"])
+    path = scenes.write_spec(str(tmp_path), "door", scenes.door_room_spec(seed=1004),
+                             dict(scenes.DOOR_ROOM_CAMERA, resolution=list(res)), res, 64, meta["num_path_vertices"])
+    x0, y0, x1, y1 = meta["crop"]
+    K = 4
+    with wr_lib.Scene.from_file(path) as sc:
+        runs = np.stack([sc.render(spp=1024, seed=700 + i, guiding=guiding)[y0:y1, x0:x1] for i in range(K)])
+    ref = 0.5 * (ref_a + ref_b)
+    img = runs.mean(axis=0)
+    floor = relmse(ref_a, ref_b)
+    err = relmse(img, ref)
+    assert err <= 2.0 * floor, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
+    z = block_z(runs, ref)
+    assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
+    assert abs(img.mean() / ref.mean() - 1.0) < 0.01

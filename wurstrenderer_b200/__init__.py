@@ -242,10 +242,10 @@ class Scene:
 
     def render_device(self, out_device_ptr: int, spp=None, num_path_vertices=None, seed=0, render_index=0,
                       queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
-                      trace_block=None) -> None:
+                      trace_block=None, guiding=0, guide_steps=None) -> None:
         """Renders into device memory at `out_device_ptr` (W*H*3 doubles)."""
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-                       profile, trace_block)
+                       profile, trace_block, None, guiding, None, None, None, guide_steps)
         _check(load_library().wr_render_device(self._h, ctypes.byref(d), ctypes.c_void_p(int(out_device_ptr))))
 
     def autotune(self, probe_spp=4, **base):

@@ -703,7 +703,9 @@ HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
 }
 
 // ------------------------------------------------------------ guiding ----
-constexpr float kGuideLr = 1e-3f;   // Adam learning rate
+constexpr float kGuideLr = 1e-3f;          // Adam learning rate
+constexpr double kGuideTimeShare = 0.08;   // default training budget: share of the render's device time
+constexpr double kGuideStepMsGuess = 0.035; // Adam step time assumed before the first one is measured
 
 int sm_count(const wr_scene &s) {
     int sms = 148;
@@ -828,7 +830,10 @@ void render_guided(wr_scene &s, const wr_render_desc &desc, double *out, bool ou
                                                                     (size_t(1) << 22) / npix)));
     const uint32_t batch = desc.guide_batch > 0 ? uint32_t(desc.guide_batch) : 16384u;
     const int n_train_passes = train > 0 ? (train + pass - 1) / pass : 0;
-    const int total_steps = desc.guide_steps > 0 ? desc.guide_steps : 2048;
+    // Adam step budget: fixed (desc.guide_steps) or kGuideTimeShare of the render's estimated
+    // device time, estimated from the first (unguided) pass and the measured time per step
+    int planned_steps = desc.guide_steps > 0 ? desc.guide_steps : 0;
+    double budget_ms = 0.0;
     const uint64_t per_pass = uint64_t(npix) * uint64_t(pass) * uint64_t(std::max(1, base.nverts - 2));
     const uint32_t rec_cap = uint32_t(std::min<uint64_t>(per_pass, uint64_t(1) << 24));
     if (desc.guiding == 1) {
@@ -867,18 +872,35 @@ void render_guided(wr_scene &s, const wr_render_desc &desc, double *out, bool ou
         const double clamp = desc.guide_clamp > 0.f ? double(desc.guide_clamp) : 1000.0;
         const float c_max = desc.guide_clamp < 0.f ? INFINITY
                           : cs[1] > 0.0 ? float(clamp * cs[0] / cs[1]) : wrg::kCMax;
-        // the step budget spread evenly over the training passes
-        const int pass_steps = total_steps * (passes) / n_train_passes - total_steps * (passes - 1) / n_train_passes;
+        if (desc.guide_steps <= 0 && passes == 1) {
+            const double est_ms = s.stats.render_ms / double(k) * double(total) * 1.1;   // guided passes ~10 % slower
+            budget_ms = kGuideTimeShare * est_ms;
+            planned_steps = int(std::min(8192.0, std::max(256.0, budget_ms / kGuideStepMsGuess)));
+        }
+        // the remaining step budget spread evenly over the remaining training passes
+        int pass_steps = 0;
+        {
+            const int passes_left = n_train_passes - (passes - 1);
+            int steps_left = planned_steps - int(steps);
+            if (desc.guide_steps <= 0 && steps > 0) {   // re-plan with the measured time per step
+                const double per_step = train_ms / double(steps);
+                steps_left = int(std::max(0.0, (budget_ms - train_ms) / per_step));
+                steps_left = std::min(steps_left, 8192 - int(steps));
+                steps_left = std::max(steps_left, 256 - int(steps));
+            }
+            pass_steps = passes_left > 0 ? std::max(steps_left, 0) / passes_left : 0;
+        }
         WR_CUDA(cudaEventRecord(s.ev0, st));
-        const double loss = train_records(s, s.w_records.as<float4>(), n, batch, std::max(pass_steps, 1), kGuideLr,
-                                          c_max, nullptr, &steps);
+        const double loss = pass_steps > 0 ? train_records(s, s.w_records.as<float4>(), n, batch, pass_steps, kGuideLr,
+                                                          c_max, nullptr, &steps)
+                                           : 0.0;
         WR_CUDA(cudaEventRecord(s.ev1, st));
         WR_CUDA(cudaEventSynchronize(s.ev1));
         float ms = 0.f;
         WR_CUDA(cudaEventElapsedTime(&ms, s.ev0, s.ev1));
         train_ms += ms;
-        last_loss = n ? loss / (double(std::max(pass_steps, 1)) * double(std::min(batch, n))) : 0.0;
-        trained = trained || n > 0;
+        if (pass_steps > 0 && n > 0) last_loss = loss / (double(pass_steps) * double(std::min(batch, n)));
+        trained = trained || (n > 0 && steps > 0);
         done += k;
     }
     if (done < total) {

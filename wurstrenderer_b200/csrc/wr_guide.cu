@@ -56,12 +56,14 @@ __device__ __forceinline__ bool fetch_point(const InferSource &s, uint32_t i, f3
         p = mk(r[0], r[1], r[2]); n = mk(r[3], r[4], r[5]); wo = mk(r[6], r[7], r[8]);
         return true;
     }
-    const float4 h = s.hit[i];
+    // the path's records first (independent loads), then the triangle they name
+    const float4 h = s.hit[i], o = s.o[i], d = s.d[i];
     const uint32_t tri = __float_as_uint(h.w);
-    if (tri == wrd::MISS || (__ldg(s.tri_mat + tri) & wrd::LIGHT_BIT)) return false;
-    const float4 o = s.o[i], d = s.d[i];
+    if (tri == wrd::MISS) return false;
+    const uint32_t mat = __ldg(s.tri_mat + tri);
     const f3 a = wrd::xyz(__ldg(s.tris + 3 * tri)), b = wrd::xyz(__ldg(s.tris + 3 * tri + 1)),
              c = wrd::xyz(__ldg(s.tris + 3 * tri + 2));
+    if (mat & wrd::LIGHT_BIT) return false;
     const f3 dd = mk(d.x, d.y, d.z);
     p = mk(o.x, o.y, o.z) + dd * h.x;
     wo = -dd;

@@ -507,22 +507,22 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                 f3 wgt;
                 if (!guided) {
                     wgt = bsdf_sample(mm, inL, rb.a, rb.b, outL, pdfW);
-                } else if (rb.c < kGuideAlpha) {
-                    const f3 dg = guide_sample(*gl, rb.c * (1.f / kGuideAlpha), rb.a, rb.b);
-                    outL = fr.to_local(dg);
-                    const float pb = bsdf_pdf(mm, inL, outL);
-                    pdfW = kGuideAlpha * guide_pdf(*gl, dg) + (1.f - kGuideAlpha) * pb;
-                    wgt = pdfW > 0.f ? bsdf_eval(mm, inL, outL) * (fabsf(outL.y) / pdfW) : mk(0.f, 0.f, 0.f);
                 } else {
-                    float pb;
-                    const f3 wb = bsdf_sample(mm, inL, rb.a, rb.b, outL, pb);   // f cos / pb
-                    pdfW = pb;
-                    wgt = mk(0.f, 0.f, 0.f);
-                    if (pb > 0.f && !is_zero(wb)) {
-                        pdfW = kGuideAlpha * guide_pdf(*gl, normalize(fr.to_world(outL))) +
-                               (1.f - kGuideAlpha) * pb;
-                        wgt = wb * (pb / pdfW);
+                    // one-sample MIS: the direction from the guide (probability kGuideAlpha) or from the
+                    // BSDF, weighted by f cos / (alpha q + (1 - alpha) p_bsdf); both techniques share
+                    // the density evaluation (no divergent second evaluation)
+                    f3 dw;
+                    if (rb.c < kGuideAlpha) {
+                        dw = guide_sample(*gl, rb.c * (1.f / kGuideAlpha), rb.a, rb.b);
+                        outL = fr.to_local(dw);
+                    } else {
+                        float pb_unused;
+                        bsdf_sample(mm, inL, rb.a, rb.b, outL, pb_unused);
+                        dw = normalize(fr.to_world(outL));
                     }
+                    pdfW = kGuideAlpha * guide_pdf(*gl, dw) + (1.f - kGuideAlpha) * bsdf_pdf(mm, inL, outL);
+                    const f3 f = bsdf_eval(mm, inL, outL);
+                    wgt = (pdfW > 0.f && !is_zero(f)) ? f * (fabsf(outL.y) / pdfW) : mk(0.f, 0.f, 0.f);
                 }
                 if (!is_zero(wgt) && isfinite(wgt.x + wgt.y + wgt.z)) {
                     alive = true;
