@@ -288,6 +288,9 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip e2e, profile and CPU baseline (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="use the default wavefront settings")
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time study")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="host-driven launches instead of one graph per render (profiling runs: ncu does not "
+                         "profile kernels inside conditional graph nodes)")
     ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128", "door"],
                     help="heightfield: the 1M-triangle single render (headline); jobs128: 128 batched jobs "
                          "over the Cornell box, one graph launch per step; door: one guided render (learned "
@@ -334,7 +337,7 @@ def main():
         tune["queue_capacity"] = args.queue_capacity
     qc = tune.get("queue_capacity")
     knobs = dict(grid_trace=tune.get("grid_trace"), grid_shade=tune.get("grid_shade"),
-                 trace_block=tune.get("trace_block"))
+                 trace_block=tune.get("trace_block"), use_graph=not args.no_graph)
 
     batch_jobs = None
     if args.workload == "jobs128":
@@ -403,7 +406,8 @@ def main():
         if batch_jobs is not None:
             step(424242 + 1000 * i)
         else:
-            scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc, **knobs)
+            scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc,
+                         guiding=1 if args.workload == "door" else 0, **knobs)
         e2e_ms += (time.perf_counter() - a) * 1e3
     e2e_value = paths_per_rank * world * args.steps / (max_over_ranks(e2e_ms, world, dist, device="cuda") / 1e3) / 1e6
 
@@ -413,7 +417,8 @@ def main():
             j["seed"] = 99 + k
         scene.render_batch(batch_jobs, queue_capacity=qc, profile=2, **knobs)
     else:
-        scene.render_device(film.data_ptr(), spp=spp, seed=99, queue_capacity=qc, profile=2, **knobs)
+        scene.render_device(film.data_ptr(), spp=spp, seed=99, queue_capacity=qc, profile=2,
+                            guiding=1 if args.workload == "door" else 0, **knobs)
     prof = scene.stats
     kn = wr.KERNELS
     k_ms = dict(zip(kn, prof["kernel_ms"]))
@@ -445,7 +450,9 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 film + CDF build)", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": WORKLOAD if batch_jobs is None else WORKLOAD_JOBS,
+            "config": {"workload": {"heightfield": WORKLOAD, "jobs128": WORKLOAD_JOBS,
+                                    "door": DOOR_WORKLOAD + ", guided (learned proposal trained on its first 32 spp)"}[
+                                        args.workload],
                        "parallelism": "replicas x%d, FP64 film reduce" % world,
                        "autotuned": tune, "autotune_probe_ms": tune_ms,
                        "l2": "256 MB buffer written between timed steps; path state > L2",

@@ -756,7 +756,6 @@ uint32_t shuffle_stride(uint32_t n) {
 double train_records(wr_scene &s, const float4 *records, uint32_t n, uint32_t batch, int max_steps, float lr,
                      float c_max, std::vector<double> *per_step, unsigned long long *steps_out) {
     cudaStream_t st = s.stream;
-    const int sms = sm_count(s);
     s.g_loss.alloc(8 * 2);
     const uint32_t stride = shuffle_stride(n);
     const int steps = max_steps > 0 ? max_steps : int((n + batch - 1) / batch);
@@ -766,9 +765,9 @@ double train_records(wr_scene &s, const float4 *records, uint32_t n, uint32_t ba
         const uint32_t first = uint32_t((uint64_t(k) * batch) % n);
         const uint32_t cnt = std::min(batch, n - first);
         if (per_step) WR_CUDA(cudaMemsetAsync(s.g_loss.p, 0, 8, st));
-        wrg::guide_gradient(s.guide, records, nullptr, first + cnt, first, n, stride, c_max, s.g_loss.as<double>(),
-                            sms, st);
-        wrg::guide_adam(s.guide, lr, 1.f / float(cnt), ++s.guide_step, st);
+        const int nslots = wrg::guide_gradient(s.guide, records, first + cnt, first, n, stride, c_max,
+                                               s.g_loss.as<double>(), st);
+        wrg::guide_adam(s.guide, lr, 1.f / float(cnt), ++s.guide_step, nslots, st);
         if (per_step) {
             double l = 0.0;
             WR_CUDA(cudaMemcpyAsync(&l, s.g_loss.p, 8, cudaMemcpyDeviceToHost, st));
@@ -1337,9 +1336,9 @@ int wr_guide_gradient(wr_scene *s, const float *records, int n, float c_max, flo
         s->g_loss.alloc(16);
         if (n) WR_CUDA(cudaMemcpyAsync(s->g_scratch.p, records, size_t(n) * 80, cudaMemcpyHostToDevice, st));
         WR_CUDA(cudaMemsetAsync(s->g_loss.p, 0, 8, st));
-        wrg::guide_gradient(s->guide, s->g_scratch.as<float4>(), nullptr, uint32_t(n), 0, uint32_t(n), 1u, c_max,
-                            s->g_loss.as<double>(), sm_count(*s), st);
-        wrg::guide_sum_gradient(s->guide, st);
+        const int nslots = wrg::guide_gradient(s->guide, s->g_scratch.as<float4>(), uint32_t(n), 0, uint32_t(n), 1u,
+                                               c_max, s->g_loss.as<double>(), st);
+        wrg::guide_sum_gradient(s->guide, nslots, st);
         WR_CUDA(cudaMemcpyAsync(grad, s->guide.grad, size_t(wrg::kGuideParams) * 4, cudaMemcpyDeviceToHost, st));
         double l = 0.0;
         WR_CUDA(cudaMemcpyAsync(&l, s->g_loss.p, 8, cudaMemcpyDeviceToHost, st));

@@ -17,6 +17,7 @@
 //                   dX = dH W (M128 N64 K64), dW += dH^T X (M64 N64 K128, MN-major operands,
 //                   accumulated in TMEM across all tiles of the CTA), one atomic flush per CTA
 //   k_guide_adam    Adam on the FP32 master weights, BF16 copies (W and W^T) for the kernels
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <string>
@@ -185,8 +186,8 @@ __device__ __forceinline__ float loss_grad(const float *o, f3 d, float c, float 
 // training records: kRecordFloat4 float4 each (layout in wr_guide.h)
 // rows [first, count) of the minibatch map to records (row * stride) % total (a fixed shuffle
 // when stride and total are coprime)
-__global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 *records, const uint32_t *count_dev,
-                                                      uint32_t count_host, uint32_t first, uint32_t total,
+__global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 *records, uint32_t count,
+                                                      uint32_t first, uint32_t total,
                                                       uint32_t stride, float c_max, double *loss_out) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *wt = smem;                       // W tiles   5 x 8 KB
@@ -210,8 +211,7 @@ __global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 
     const uint32_t tmem = *slot;
     const uint32_t tD = tmem, tdW = tmem + 64;       // columns [0,64) scratch, [64, 384) dW of layers 0..4
     const uint32_t lane_base = uint32_t(warp * 32) << 16;
-    uint32_t n = count_dev ? *count_dev : count_host;
-    n = n > first ? n - first : 0u;
+    const uint32_t n = count > first ? count - first : 0u;
     const uint32_t ntiles = (n + kTile - 1) / kTile;
     const uint32_t id_fwd = idesc_bf16(128, 64, 0, 0);
     const uint32_t id_dw = idesc_bf16(64, 64, 1, 1);
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 
                              ks > 0 ? 1u : 0u);
                 mma_commit(smem_addr(mbar));
             }
-            const bool ok = mbar_wait(smem_addr(mbar), phase, kWaitIters);
+            const bool ok = warp != 0 || mbar_wait(smem_addr(mbar), phase, kWaitIters);   // warp 0 polls
             phase ^= 1u;
             if (__syncthreads_or(!ok)) { failed = true; break; }
             fence_after_sync();
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 
                 }
                 mma_commit(smem_addr(mbar));
             }
-            const bool ok = mbar_wait(smem_addr(mbar), phase, kWaitIters);
+            const bool ok = warp != 0 || mbar_wait(smem_addr(mbar), phase, kWaitIters);   // warp 0 polls
             phase ^= 1u;
             if (__syncthreads_or(!ok)) { failed = true; break; }
             fence_after_sync();
@@ -314,20 +314,16 @@ __global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 
     }
     if (failed) {
         if (tid == 0) atomicExch(g.err, 1u);
-    } else {
+    } else if (any_tile) {
         // this CTA's dW into its own partial slot (summed in a fixed order by the optimiser, so
         // the gradient is deterministic). M = 64 accumulator row n lives in TMEM lane
-        // (n % 16) + 32 (n / 16); a CTA without tiles writes zeros.
+        // (n % 16) + 32 (n / 16). CTA b has tiles exactly when b < ceil(rows / 128), and only
+        // those slots are summed.
         const int lane = tid & 31;
         float *slot_base = g.partial + size_t(blockIdx.x) * kParams;
         for (int l = 0; l < kLayers; ++l) {
             float v[kW];
-            if (any_tile) {
-                tmem_ld64(tdW + 64 * l + lane_base, v);
-            } else {
-#pragma unroll
-                for (int k = 0; k < kW; ++k) v[k] = 0.f;
-            }
+            tmem_ld64(tdW + 64 * l + lane_base, v);
             if (lane < 16) {
                 float4 *gr = reinterpret_cast<float4 *>(slot_base + l * kW * kW + (16 * warp + lane) * kW);
 #pragma unroll
@@ -353,38 +349,64 @@ __global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 
 }
 
 // ------------------------------------------------------------- optimiser ----
-__device__ __forceinline__ float sum_partials(const GuideNet &g, int i) {
-    float s = 0.f;
-    for (int k = 0; k < g.slots; ++k) s += g.partial[size_t(k) * kParams + i];
-    return s;
+// Deterministic sum of the per-CTA partial gradients: a block covers kRedParams consecutive
+// parameters with kRedGroups groups of threads; group j adds slots j, j + kRedGroups, ... (two
+// accumulators), then group 0 adds the group sums in order. Returns the total on group-0 threads.
+constexpr int kRedParams = 64;
+constexpr int kRedGroups = 8;
+constexpr int kRedThreads = kRedParams * kRedGroups;
+
+__device__ __forceinline__ float reduce_partials(const GuideNet &g, int i, int nslots) {
+    __shared__ float red[kRedGroups][kRedParams];
+    const int p = threadIdx.x % kRedParams, grp = threadIdx.x / kRedParams;
+    const float *part = g.partial + i;
+    float s0 = 0.f, s1 = 0.f;
+    int k = grp;
+    for (; k + kRedGroups < nslots; k += 2 * kRedGroups) {
+        s0 += part[size_t(k) * kParams];
+        s1 += part[size_t(k + kRedGroups) * kParams];
+    }
+    if (k < nslots) s0 += part[size_t(k) * kParams];
+    red[grp][p] = s0 + s1;
+    __syncthreads();
+    float total = 0.f;
+    if (grp == 0)
+#pragma unroll
+        for (int j = 0; j < kRedGroups; ++j) total += red[j][p];
+    return total;
 }
 
 // the summed gradient into g.grad (for callers that read it)
-__global__ void k_guide_sum(GuideNet g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x)
-        g.grad[i] = sum_partials(g, i);
+__global__ void __launch_bounds__(kRedThreads) k_guide_sum(GuideNet g, int nslots) {
+    const int i = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
+    const float total = reduce_partials(g, i, nslots);
+    if (threadIdx.x < kRedParams) g.grad[i] = total;
 }
 
-__global__ void k_guide_adam(GuideNet g, float lr, float scale, int step, int apply) {
+// one Adam step on the summed gradient (apply = 0: only the constant-unit rows and the bf16
+// copies are refreshed from the master weights)
+__global__ void __launch_bounds__(kRedThreads) k_guide_adam(GuideNet g, float lr, float scale, int step, int apply,
+                                                            int nslots) {
+    const int i = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
+    const float gsum = apply ? reduce_partials(g, i, nslots) : 0.f;
+    if (threadIdx.x >= kRedParams) return;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
-        const int l = i / (kW * kW), nrow = (i / kW) % kW, k = i % kW;
-        float w = g.master[i];
-        if (apply) {
-            const float gr = sum_partials(g, i) * scale;
-            const float m = b1 * g.m[i] + (1.f - b1) * gr;
-            const float v = b2 * g.v[i] + (1.f - b2) * gr * gr;
-            g.m[i] = m;
-            g.v[i] = v;
-            w -= lr * (m / c1) / (sqrtf(v / c2) + eps);
-        }
-        if (l < kLayers - 1 && nrow == kW - 1) w = (k == kW - 1) ? 1.f : 0.f;   // the constant unit
-        g.master[i] = w;
-        const __nv_bfloat16 h = __float2bfloat16_rn(w);
-        g.w[i] = h;
-        g.wt[l * kW * kW + k * kW + nrow] = h;
+    const int l = i / (kW * kW), nrow = (i / kW) % kW, k = i % kW;
+    float w = g.master[i];
+    if (apply) {
+        const float gr = gsum * scale;
+        const float m = b1 * g.m[i] + (1.f - b1) * gr;
+        const float v = b2 * g.v[i] + (1.f - b2) * gr * gr;
+        g.m[i] = m;
+        g.v[i] = v;
+        w -= lr * (m / c1) / (sqrtf(v / c2) + eps);
     }
+    if (l < kLayers - 1 && nrow == kW - 1) w = (k == kW - 1) ? 1.f : 0.f;   // the constant unit
+    g.master[i] = w;
+    const __nv_bfloat16 h = __float2bfloat16_rn(w);
+    g.w[i] = h;
+    g.wt[l * kW * kW + k * kW + nrow] = h;
 }
 
 // sum of c and number of records with c > 0 over records [0, n)
@@ -467,13 +489,13 @@ void guide_free(GuideNet &g) {
 
 void guide_init(GuideNet &g, uint32_t seed, cudaStream_t st) {
     k_guide_init<<<40, 512, 0, st>>>(g, seed);
-    k_guide_adam<<<40, 512, 0, st>>>(g, 0.f, 0.f, 1, 0);   // constant unit, bf16 copies
+    k_guide_adam<<<kParams / kRedParams, kRedThreads, 0, st>>>(g, 0.f, 0.f, 1, 0, 0);   // constant unit, bf16 copies
     check(cudaGetLastError(), "guide init");
 }
 
 void guide_set_master(GuideNet &g, const float *host_w, cudaStream_t st) {
     check(cudaMemcpyAsync(g.master, host_w, kParams * 4, cudaMemcpyHostToDevice, st), "guide set");
-    k_guide_adam<<<40, 512, 0, st>>>(g, 0.f, 0.f, 1, 0);
+    k_guide_adam<<<kParams / kRedParams, kRedThreads, 0, st>>>(g, 0.f, 0.f, 1, 0, 0);
     check(cudaGetLastError(), "guide set");
 }
 
@@ -500,13 +522,13 @@ void guide_infer_wavefront(const GuideNet &g, const float4 *o, const float4 *d, 
     k_guide_infer<<<infer_grid(sms), kTile * kGroups, kInferSmem, st>>>(g, s, nullptr, lobes_packed, stride);
 }
 
-void guide_gradient(GuideNet &g, const float4 *records_dev, const uint32_t *count_dev, uint32_t count_host,
-                    uint32_t first, uint32_t total, uint32_t stride, float c_max, double *loss_dev, int sms,
-                    cudaStream_t st) {
+int guide_gradient(GuideNet &g, const float4 *records_dev, uint32_t count, uint32_t first, uint32_t total,
+                   uint32_t stride, float c_max, double *loss_dev, cudaStream_t st) {
     // one CTA per partial-gradient slot (the shared memory allows one CTA per SM)
-    k_guide_train<<<g.slots, kTile, kTrainSmem, st>>>(g, records_dev, count_dev, count_host, first, total, stride,
-                                                      c_max, loss_dev);
+    k_guide_train<<<g.slots, kTile, kTrainSmem, st>>>(g, records_dev, count, first, total, stride, c_max, loss_dev);
     check(cudaGetLastError(), "guide train");
+    const uint32_t rows = count > first ? count - first : 0u;
+    return int(std::min<uint32_t>(uint32_t(g.slots), (rows + kTile - 1) / kTile));
 }
 
 void guide_cstats(const float4 *records_dev, uint32_t n, double *out_dev, int sms, cudaStream_t st) {
@@ -515,13 +537,13 @@ void guide_cstats(const float4 *records_dev, uint32_t n, double *out_dev, int sm
     check(cudaGetLastError(), "guide cstats");
 }
 
-void guide_sum_gradient(GuideNet &g, cudaStream_t st) {
-    k_guide_sum<<<40, 512, 0, st>>>(g);
+void guide_sum_gradient(GuideNet &g, int nslots, cudaStream_t st) {
+    k_guide_sum<<<kParams / kRedParams, kRedThreads, 0, st>>>(g, nslots);
     check(cudaGetLastError(), "guide sum");
 }
 
-void guide_adam(GuideNet &g, float lr, float scale, int step, cudaStream_t st) {
-    k_guide_adam<<<40, 512, 0, st>>>(g, lr, scale, step, 1);
+void guide_adam(GuideNet &g, float lr, float scale, int step, int nslots, cudaStream_t st) {
+    k_guide_adam<<<kParams / kRedParams, kRedThreads, 0, st>>>(g, lr, scale, step, 1, nslots);
     check(cudaGetLastError(), "guide adam");
 }
 

@@ -70,17 +70,18 @@ void guide_infer_rows(const GuideNet &g, const float *rows_dev, uint32_t n, floa
 void guide_infer_wavefront(const GuideNet &g, const float4 *o, const float4 *d, const float4 *hit, const uint32_t *count,
                            const float4 *tris, const uint32_t *tri_mat, uint4 *lobes_packed, size_t stride, int sms,
                            cudaStream_t st);
-// the loss gradient of minibatch rows [first, count) into the partial slots (and the summed loss
-// added to *loss_dev when given); count comes from count_dev when it is not null, else
-// count_host; row r reads record (r * stride) % total
-void guide_gradient(GuideNet &g, const float4 *records_dev, const uint32_t *count_dev, uint32_t count_host,
-                    uint32_t first, uint32_t total, uint32_t stride, float c_max, double *loss_dev, int sms,
-                    cudaStream_t st);
+// the loss gradient of minibatch rows [first, count) into the per-CTA partial slots (and the
+// summed loss added to *loss_dev when given); row r reads record (r * stride) % total. Returns
+// the number of partial slots written (pass it to guide_sum_gradient / guide_adam).
+int guide_gradient(GuideNet &g, const float4 *records_dev, uint32_t count, uint32_t first, uint32_t total,
+                   uint32_t stride, float c_max, double *loss_dev, cudaStream_t st);
 // out_dev[0] = sum of c over records [0, n) with c > 0, out_dev[1] = their number (FP64)
 void guide_cstats(const float4 *records_dev, uint32_t n, double *out_dev, int sms, cudaStream_t st);
-// the gradient of the last guide_gradient call, summed over the partial slots, into g.grad
-void guide_sum_gradient(GuideNet &g, cudaStream_t st);
-// one Adam step on the gradient of the last guide_gradient call, scaled by `scale`
-void guide_adam(GuideNet &g, float lr, float scale, int step, cudaStream_t st);
+// the gradient of the last guide_gradient call, summed over its nslots partial slots in a fixed
+// order, into g.grad
+void guide_sum_gradient(GuideNet &g, int nslots, cudaStream_t st);
+// one Adam step on the gradient of the last guide_gradient call (nslots partial slots), scaled by
+// `scale`
+void guide_adam(GuideNet &g, float lr, float scale, int step, int nslots, cudaStream_t st);
 
 }  // namespace wrg

@@ -30,10 +30,11 @@ constexpr int kActBytes = kTile * kW * 2;    // one 128 x 64 bf16 activation til
 
 // ------------------------------------------------------------------ encoding ----
 // 64 features: p in [0,1]^3, sin/cos(2^f pi p) for f = 0..5, n, wo, sin/cos(pi n),
-// sin/cos(pi wo), six zeros, the constant 1. sincospif gives sin/cos(pi p); the
+// sin/cos(pi wo), six zeros, the constant 1. The base frequency uses the hardware
+// sine/cosine (__sincosf: arguments within [-pi, pi], absolute error about 4e-7); the
 // higher frequencies follow by the double-angle identities (sin 2a = 2 sin a cos a,
-// cos 2a = 1 - 2 sin^2 a), whose error (a few 1e-6 after five doublings) is far
-// below the bf16 rounding of the features.
+// cos 2a = 1 - 2 sin^2 a), whose error (a few 1e-5 after five doublings) is far below
+// the bf16 rounding of the features (4e-3 relative).
 __device__ __forceinline__ void encode(f3 p, f3 n, f3 wo, const GuideNet &g, float *x) {
     const float q[3] = {(p.x - g.box_lo[0]) * g.box_inv[0], (p.y - g.box_lo[1]) * g.box_inv[1],
                         (p.z - g.box_lo[2]) * g.box_inv[2]};
@@ -41,7 +42,7 @@ __device__ __forceinline__ void encode(f3 p, f3 n, f3 wo, const GuideNet &g, flo
     for (int a = 0; a < 3; ++a) {
         x[a] = q[a];
         float sn, cs;
-        sincospif(q[a], &sn, &cs);
+        __sincosf(wrd::kPi * q[a], &sn, &cs);
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
             x[3 + 6 * f + a] = sn;
@@ -56,8 +57,8 @@ __device__ __forceinline__ void encode(f3 p, f3 n, f3 wo, const GuideNet &g, flo
     for (int a = 0; a < 3; ++a) {
         x[39 + a] = nv[a];
         x[42 + a] = wv[a];
-        sincospif(nv[a], &x[45 + a], &x[48 + a]);
-        sincospif(wv[a], &x[51 + a], &x[54 + a]);
+        __sincosf(wrd::kPi * nv[a], &x[45 + a], &x[48 + a]);
+        __sincosf(wrd::kPi * wv[a], &x[51 + a], &x[54 + a]);
     }
 #pragma unroll
     for (int k = 57; k < 63; ++k) x[k] = 0.f;
@@ -95,14 +96,16 @@ __device__ __forceinline__ void relu_mask_row(const unsigned char *tile, int row
     }
 }
 
-// bf16 weights [l][n][k] -> canonical tiles (rows n, columns k), 16 bytes at a time;
-// rows >= last_rows of the last layer are not loaded
+// bf16 weights [l][n][k] -> canonical tiles (rows n, columns k), 16 bytes at a time; consecutive
+// threads take consecutive rows n of one 8-column chunk, so each group of 8 threads fills one
+// 128-byte core-matrix row set without shared-memory bank conflicts. Rows >= last_rows of the
+// last layer are not loaded.
 __device__ __forceinline__ void load_weights(unsigned char *dst, const __nv_bfloat16 *src, int last_rows = kW) {
     const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
     for (int i = threadIdx.x; i < kParams / 8; i += blockDim.x) {
-        const int l = i / (kW * kW / 8), n = (i / (kW / 8)) % kW, k = (i % (kW / 8)) * 8;
+        const int n = i % kW, kc = (i / kW) % (kW / 8), l = i / (kW * kW / 8);
         if (l == kLayers - 1 && n >= last_rows) continue;
-        *reinterpret_cast<uint4 *>(dst + l * 8192 + tile_offset(n, k)) = __ldg(s4 + i);
+        *reinterpret_cast<uint4 *>(dst + l * 8192 + tile_offset(n, 8 * kc)) = __ldg(s4 + (l * kW + n) * (kW / 8) + kc);
     }
 }
 
@@ -146,7 +149,8 @@ __device__ __forceinline__ bool mlp_forward_tile(unsigned char *at, const unsign
                          ks > 0 ? 1u : 0u);
             mma_commit(smem_addr(mbar));
         }
-        const bool ok = mbar_wait(smem_addr(mbar), phase, kWaitIters);
+        // one warp polls the mbarrier; the others wait on the group barrier without issuing
+        const bool ok = r >= 32 || mbar_wait(smem_addr(mbar), phase, kWaitIters);
         phase ^= 1u;
         if (group_any(bar, !ok)) return false;
         fence_after_sync();
@@ -174,7 +178,9 @@ struct Lobes {
     float mu[8][3], lam[8], w[8];
 };
 
-__device__ __forceinline__ float softplus(float s) { return s > 20.f ? s : log1pf(__expf(s)); }
+// softplus with the hardware exp / log (relative error ~1e-6, far below the half rounding of
+// the stored sharpness)
+__device__ __forceinline__ float softplus(float s) { return s > 20.f ? s : __logf(1.f + __expf(s)); }
 
 __device__ __forceinline__ void raw_to_lobes(const float *o, Lobes &L) {
     float amax = -1e30f;
@@ -184,15 +190,20 @@ __device__ __forceinline__ void raw_to_lobes(const float *o, Lobes &L) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const float rx = o[5 * k], ry = o[5 * k + 1], rz = o[5 * k + 2];
-        const float nr = sqrtf(rx * rx + ry * ry + rz * rz);
-        if (nr > 1e-12f) { L.mu[k][0] = rx / nr; L.mu[k][1] = ry / nr; L.mu[k][2] = rz / nr; }
-        else { L.mu[k][0] = 0.f; L.mu[k][1] = 1.f; L.mu[k][2] = 0.f; }
+        const float n2 = rx * rx + ry * ry + rz * rz;
+        if (n2 > 1e-24f) {
+            const float inv = rsqrtf(n2);
+            L.mu[k][0] = rx * inv; L.mu[k][1] = ry * inv; L.mu[k][2] = rz * inv;
+        } else {
+            L.mu[k][0] = 0.f; L.mu[k][1] = 1.f; L.mu[k][2] = 0.f;
+        }
         L.lam[k] = fminf(softplus(o[5 * k + 3]) + kLambdaMin, kLambdaMax);
         L.w[k] = __expf(o[5 * k + 4] - amax);
         wsum += L.w[k];
     }
+    const float inv_sum = 1.f / wsum;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) L.w[k] /= wsum;
+    for (int k = 0; k < 8; ++k) L.w[k] *= inv_sum;
 }
 
 // ------------------------------------------------------------ packed lobes ----
