@@ -228,7 +228,7 @@ def guided_vs_plain(wr, plain_spp=256, seeds=2):
     gdir = os.path.join(ROOT, "tests", "golden")
     meta_p = os.path.join(gdir, "door_crop_meta.json")
     if not os.path.exists(meta_p):
-        return {"unavailable": "door-room reference crop not generated (tests/golden/make_door_golden.py)"}
+        return {"unavailable": "door-room reference crop not generated (tests/golden/make_crop_golden.py)"}
     meta = json.load(open(meta_p))
     ref_a = np.load(os.path.join(gdir, "door_crop_ref_a.npy")).astype(np.float64)
     ref_b = np.load(os.path.join(gdir, "door_crop_ref_b.npy")).astype(np.float64)

@@ -50,7 +50,7 @@ typedef struct wr_render_desc {
                                 2: timing + traversal counters (node visits, triangle tests) */
     int trace_block;         /* threads per block of the traversal kernels: 64, 128 or 256; 0 = 128 */
     int integrator;          /* 0: the render entry's "integrator" (default nextevent_path_tracer);
-                                1: nextevent_path_tracer; 2: primitive_path_tracer */
+                                1: nextevent_path_tracer; 2: primitive_path_tracer; 3: light_splatting */
     int guiding;             /* learned proposal (no counterpart in the reference; NEE+MIS only):
                                 0: off (plain NEE+MIS);
                                 1: train a fresh network online on the first guide_train_spp samples per
@@ -149,12 +149,13 @@ int wr_scene_get_info(const wr_scene *scene, wr_scene_info *info);
 int wr_scene_set_camera_json(wr_scene *scene, const char *camera_json);
 
 /* Renders with the NEE+MIS integrator ("nextevent_path_tracer",
- * PathNeeRenderer::render, src/renderer/pathnextevent.h:152-191), or with the
- * BSDF-only "primitive_path_tracer" (PrimitivePathRenderer::render,
- * src/renderer/primitivepath.h:60-101) when the render entry or desc->integrator
- * selects it, and copies
- * the W*H*3 image (base/spp + splat/(spp*W*H)) into host memory. desc may be
- * NULL (defaults). */
+ * PathNeeRenderer::render, src/renderer/pathnextevent.h:152-191), or, when the
+ * render entry or desc->integrator selects it, with the BSDF-only
+ * "primitive_path_tracer" (PrimitivePathRenderer::render,
+ * src/renderer/primitivepath.h:60-101) or the light tracer "light_splatting"
+ * (LightSplattingRenderer::render, src/renderer/lightsplatting.h:38-112), and
+ * copies the W*H*3 image (base/spp + splat/(spp*W*H)) into host memory. desc may
+ * be NULL (defaults). */
 int wr_render(wr_scene *scene, const wr_render_desc *desc, double *out_rgb);
 
 /* Same, writing the image to device memory (W*H*3 doubles on the scene's

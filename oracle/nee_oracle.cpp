@@ -363,7 +363,7 @@ struct Scene {
     RayCaster rc;
     Camera cam;
     int spp = 16, nverts = 10;
-    int integrator = 0;   // 0 nextevent_path_tracer, 1 primitive_path_tracer
+    int integrator = 0;   // 0 nextevent_path_tracer, 1 primitive_path_tracer, 2 light_splatting
     std::string output;
 };
 
@@ -711,6 +711,156 @@ static void eval_primitive(const Scene &s, Sampler &smp, int px, int py, Splat *
     }
 }
 
+// LightSplattingRenderer::render's per-sample body (src/renderer/lightsplatting.h:47-108) with
+// GeneralSubpathSampler(scene, false): no camera stratification, no volumetric sample per
+// segment. A lens vertex c0 is sampled (createCameraSubpath with one vertex, which still draws
+// the direction sample, generalsubpathsampler.h:286-304), then a light subpath of
+// num_path_vertices - 1 vertices (createLightSubpath + randomWalk, :185-268, :13-160); the light
+// vertex and every surface vertex of it are connected to c0 and splatted with weight
+// 1 / (spp * W * H) (`inv`). Splats are appended to `out`.
+struct CameraConnection { double rx = 0.0, ry = 0.0; Spectrum c; bool ok = false; };
+
+// c0->mPathContrib * c0->scatter(raster, CameraImaginary, v) * G(v, c0) * transmittance(v, c0) * lscatter
+static CameraConnection connect_camera(const Scene &s, const Vertex &c0, const Vertex &v, const Spectrum &lscatter) {
+    CameraConnection r;
+    const Camera &cam = s.cam;
+    const double G = GeometryTerm(v, c0);
+    if (G == 0.0) return r;
+    // evalWe1 (thinlens.h:63-80) toward v
+    const V3 w = Normalize(diff(v, c0));
+    const V3 position = cam.frame.toLocal(c0.pos - cam.origin);
+    const V3 direction = cam.frame.toLocal(w);
+    const double cosTheta = direction.z;
+    if (Dot(w, cam.frame.z) < 0.0) return r;
+    const V3 fpp = direction / cosTheta * cam.focal + position;
+    const V3 film = -fpp / cam.focal * cam.dist;
+    const double rx = (film.x / cam.filmW + 0.5) * double(cam.W);
+    const double ry = (film.y / cam.filmH + 0.5) * double(cam.H);
+    if (rx < 0.0 || rx >= double(cam.W) || ry < 0.0 || ry >= double(cam.H)) return r;
+    const double cos4 = (cosTheta * cosTheta) * (cosTheta * cosTheta);
+    const Spectrum c0scatter(cam.perFilm / cos4);
+    if (IsZero(c0scatter)) return r;
+    if (IsZero(lscatter)) return r;
+    const Spectrum T = transmittance(s, v, c0);
+    if (IsZero(T)) return r;
+    r.rx = rx; r.ry = ry;
+    r.c = c0.contrib * c0scatter * G * T * lscatter * v.contrib;
+    r.ok = true;
+    return r;
+}
+
+static void eval_light_splat(const Scene &s, Sampler &smp, double inv, std::vector<Splat> &out) {
+    if (s.nverts < 2) return;
+    const Camera &cam = s.cam;
+    // ---- camera vertex: sampleWe0ByPdf, then the unused sampleWe1CosByPdf draw
+    Vertex c0;
+    {
+        double a, b; smp.get2d(&a, &b);
+        double lx = 0.0, ly = 0.0;
+        double abx = a * 2.0 - 1.0, aby = b * 2.0 - 1.0;
+        if (!(abx == 0 && aby == 0)) {
+            double r, phi;
+            if (abx * abx > aby * aby) { r = abx; phi = (Pi / 4.0) * (aby / abx); }
+            else { r = aby; phi = (Pi / 2.0) - (Pi / 4.0) * (abx / aby); }
+            lx = r * std::cos(phi); ly = r * std::sin(phi);
+        }
+        lx = lx * cam.aperture; ly = ly * cam.aperture;
+        c0.type = V_CAMERA;
+        c0.normal = cam.frame.z;
+        c0.pos = cam.frame.toWorld(V3(lx, ly, 0.0)) + cam.origin;
+        c0.contrib = Spectrum(1.0);
+        double d0, d1; smp.get2d(&d0, &d1);
+    }
+    auto splat = [&](const CameraConnection &cc) {
+        if (!cc.ok) return;
+        Splat sp; sp.rx = cc.rx; sp.ry = cc.ry; sp.c = cc.c * inv;
+        out.push_back(sp);
+    };
+    // ---- light vertex
+    const int numVertices = s.nverts - 1;
+    Vertex l;
+    Ray ray;
+    Spectrum contrib1(1.0);
+    {
+        double u0, u1; smp.get2d(&u0, &u1);
+        double pdfLight;
+        const int li = s.light_cdf.sample(&pdfLight, &u0, u0);
+        if (li >= int(s.lights.size())) {
+            V3 dir; double pdfDir;
+            Spectrum r = s.env->sample(&dir, &pdfDir, u0, u1);
+            l.type = V_ENV; l.geom = -1; l.frame = Frame(); l.pos = dir;
+            l.contrib = r / pdfLight;
+            splat(connect_camera(s, c0, l, Spectrum(1.0)));
+            // sampleLe1CosByPdf: a point on the disk of the scene's bounding sphere (envmap.h:83-101)
+            double a, b; smp.get2d(&a, &b);
+            double px = 0.0, py = 0.0;
+            const double abx = a * 2.0 - 1.0, aby = b * 2.0 - 1.0;
+            if (!(abx == 0 && aby == 0)) {
+                double r2, phi;
+                if (abx * abx > aby * aby) { r2 = abx; phi = (Pi / 4.0) * (aby / abx); }
+                else { r2 = aby; phi = (Pi / 2.0) - (Pi / 4.0) * (abx / aby); }
+                px = r2 * std::cos(phi); py = r2 * std::sin(phi);
+            }
+            px = px * s.env->radius; py = py * s.env->radius;
+            const V3 q(px, -s.env->radius, py);
+            const Frame frame(-l.pos);
+            const double area = Pi * (s.env->radius * s.env->radius);
+            ray.o = frame.toWorld(q) + s.env->center;
+            ray.d = -l.pos;
+            contrib1 = Spectrum(area);
+        } else {
+            const AreaLight &al = s.lights[li];
+            const Geometry &g = s.geoms[al.geometry];
+            double ls0 = u0;
+            const int ti = g.tri_cdf.sample(nullptr, &ls0, ls0);
+            const double sq = std::sqrt(ls0);
+            const double b1 = sq * (1.0 - u1), b2 = u1 * sq;
+            const V3 p0 = g.pos[g.tri[3 * ti]], p1 = g.pos[g.tri[3 * ti + 1]], p2 = g.pos[g.tri[3 * ti + 2]];
+            const V3 w0 = V3(1.0 - b1 - b2);
+            l.type = V_LIGHT; l.geom = al.geometry;
+            l.pos = w0 * p0 + b1 * p1 + b2 * p2;
+            l.normal = Normalize(Cross(p1 - p0, p2 - p0));
+            l.frame = Frame(l.normal);
+            l.contrib = al.intensity * Pi / g.inv_area / pdfLight;
+            splat(connect_camera(s, c0, l, Spectrum(light_le1(l, c0))));
+            if (numVertices == 1) return;
+            double a, b; smp.get2d(&a, &b);   // sampleLe1CosByPdf: cosine-weighted about the normal
+            const V3 outLocal = CosineHemisphere(a, b);
+            ray.o = l.pos;
+            ray.d = l.frame.toWorld(outLocal);
+        }
+    }
+    // ---- randomWalk(numVertices - 1) with the camera-connection callback
+    const int walkVertices = numVertices - 1;
+    if (walkVertices == 0) return;
+    Spectrum prevContrib = contrib1;
+    Vertex prev = l;
+    int countVertices = 0;
+    while (true) {
+        Vertex v;
+        if (!intersect(s, &ray, &v)) break;
+        v.contrib = prevContrib * prev.contrib;
+        if (v.type == V_SURFACE) {
+            const Material &m = s.materials[s.geoms[v.geom].material];
+            const V3 wi = Normalize(diff(prev, v)), wo = Normalize(diff(c0, v));
+            splat(connect_camera(s, c0, v, bsdf_eval(m, v.frame.toLocal(wi), v.frame.toLocal(wo))));
+        }
+        if (++countVertices == walkVertices) break;
+        if (v.type != V_SURFACE) break;
+        const Material &m = s.materials[s.geoms[v.geom].material];
+        const V3 inLocal = v.frame.toLocal(-ray.d);
+        V3 outLocal;
+        double b0, b1; smp.get2d(&b0, &b1);
+        const Spectrum w = bsdf_sample(m, &outLocal, nullptr, inLocal, b0, b1);
+        if (IsZero(w)) break;
+        prevContrib = w;
+        ray = Ray();
+        ray.o = v.pos;
+        ray.d = v.frame.toWorld(outLocal);
+        prev = v;
+    }
+}
+
 // -------------------------------------------------------------- loading ----
 static V3 vec3_of(const Json &j) {
     if (j.type == Json::Arr && j.arr.size() == 3) return V3(j.arr[0].number(), j.arr[1].number(), j.arr[2].number());
@@ -842,6 +992,7 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
         s->output = rj.get("output", std::string(""));
         const std::string integ = rj.get("integrator", std::string("nextevent_path_tracer"));
         if (integ == "primitive_path_tracer") s->integrator = 1;
+        else if (integ == "light_splatting") s->integrator = 2;
         else if (integ != "nextevent_path_tracer") throw std::runtime_error("integrator not restated by the oracle: " + integ);
     }
     return s.release();
@@ -879,6 +1030,9 @@ static RenderStats render(const Scene &s, int spp, int nverts, unsigned salt, in
     for (auto &a : splat) a.store(0.0);
     long long npix = 0;
     for (const Tile &t : tiles) npix += (long long)(t.x1 - t.x0) * (t.y1 - t.y0);
+    // light splatting weights every splat by 1/(spp * W * H) (lightsplatting.h:42); over a crop the
+    // pixels rendered take the place of W * H
+    const double lsInv = 1.0 / double(spp) / double(npix);
     std::atomic<int> next(0);
     auto t0 = std::chrono::steady_clock::now();
     auto worker = [&]() {
@@ -888,9 +1042,23 @@ static RenderStats render(const Scene &s, int spp, int nverts, unsigned salt, in
             const Tile &t = tiles[ti];
             const int tileSeed = t.x0 * H + t.y0;
             Sampler smp(unsigned(tileSeed) + salt * 0x9E3779B1u);
+            std::vector<Splat> ls;
             for (int y = t.y0; y < t.y1; ++y)
                 for (int x = t.x0; x < t.x1; ++x)
                     for (int i = 0; i < spp; ++i) {
+                        if (s.integrator == 2) {   // light splatting: only atomic splats, already scaled
+                            ls.clear();
+                            eval_light_splat(s, smp, lsInv, ls);
+                            for (const Splat &sp : ls) {
+                                std::atomic<double> *a = &splat[3 * (size_t(int(sp.ry)) * W + int(sp.rx))];
+                                const double c[3] = {sp.c.x, sp.c.y, sp.c.z};
+                                for (int k = 0; k < 3; ++k) {
+                                    double prev = a[k].load();
+                                    while (!a[k].compare_exchange_weak(prev, prev + c[k])) {}
+                                }
+                            }
+                            continue;
+                        }
                         Splat sp[2];
                         if (s.integrator == 1) eval_primitive(s, smp, x, y, sp);
                         else if (nverts > 1) eval_contribution(s, smp, x, y, sp);
@@ -916,7 +1084,7 @@ static RenderStats render(const Scene &s, int spp, int nverts, unsigned salt, in
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     st.paths = npix * spp;
     const double baseScale = 1.0 / double(spp);
-    const double atomicScale = 1.0 / double(spp) / double(npix);
+    const double atomicScale = s.integrator == 2 ? 1.0 : 1.0 / double(spp) / double(npix);
     for (size_t i = 0; i < base.size(); ++i) {
         double c = 0.0;
         c += base[i] * baseScale;

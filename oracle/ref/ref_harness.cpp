@@ -28,6 +28,7 @@
 #include "common/util/json.h"
 #include "renderer/pathnextevent.h"
 #include "renderer/primitivepath.h"
+#include "renderer/lightsplatting.h"
 #include "camera/thinlens.h"
 #include "bsdf/lambertdiffuse.h"
 #include "bsdf/orennayar.h"
@@ -193,8 +194,11 @@ int cmd_render(int argc, char **argv) {
     const double loadSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl0).count();
     json rj = L.root["render"][renderIndex];
     const bool primitive = rj["integrator"] == "primitive_path_tracer";
-    if (rj["integrator"] != "nextevent_path_tracer" && !primitive)
-        throw std::runtime_error("integrator is neither nextevent_path_tracer nor primitive_path_tracer");
+    const bool splatting = rj["integrator"] == "light_splatting";
+    if (rj["integrator"] != "nextevent_path_tracer" && !primitive && !splatting)
+        throw std::runtime_error("integrator is not nextevent_path_tracer, primitive_path_tracer or light_splatting");
+    if (splatting && (serial || crop))
+        throw std::runtime_error("light_splatting runs through LightSplattingRenderer::render() only (no --serial/--crop)");
     if (spp > 0) rj["num_spp"] = spp;
     if (nverts > 0) rj["num_path_vertices"] = nverts;
     shared_ptr<Sampler> sampler = make_shared<SaltedSampler>(salt);
@@ -202,17 +206,19 @@ int cmd_render(int argc, char **argv) {
     shared_ptr<const Scene> scene = L.scene;
     shared_ptr<PathNeeRenderer> r;
     shared_ptr<PrimitivePathRenderer> rp;
+    shared_ptr<LightSplattingRenderer> rs;
     if (primitive) rp = PrimitivePathRenderer::FromSimple2Json(camera, scene, sampler, rj, L.dir);
+    else if (splatting) rs = LightSplattingRenderer::FromSimple2Json(camera, scene, sampler, rj, L.dir);
     else r = PathNeeRenderer::FromSimple2Json(camera, scene, sampler, rj, L.dir);
-    const int numSpp = primitive ? rp->mNumSpp : r->mNumSpp;
-    const int numVerts = primitive ? rp->mNumPathVertices : r->mNumPathVertices;
+    const int numSpp = primitive ? rp->mNumSpp : splatting ? rs->mNumSamples : r->mNumSpp;
+    const int numVerts = primitive ? rp->mNumPathVertices : splatting ? rs->mNumPathVertices : r->mNumPathVertices;
     const Ivec2 res = camera->mFilm->mResolution;
     const int W = res[0], H = res[1];
     long long paths = 0;
     auto t0 = std::chrono::steady_clock::now();
     std::vector<double> img(size_t(W) * H * 3);
     if (!serial && !crop) {
-        if (primitive) rp->render(); else r->render();
+        if (primitive) rp->render(); else if (splatting) rs->render(); else r->render();
         paths = (long long)W * H * numSpp;
         Fimage<Spectrum> im = camera->mFilm->getImage();
         for (int y = 0; y < H; ++y)

@@ -5,7 +5,8 @@ reference's own ``PathNeeRenderer`` / ``EmbreeAccel`` code; see
 oracle/ref/ref_harness.cpp). For each fixture scene it writes:
 
   scenes/<name>/...            the scene (simple2 JSON + OBJ/MTL [+ PFM envmap])
-  <name>_ref_spp4.npy          reference render, 4 spp, one thread, seed salt 0 (float64)
+  <name>_ref_spp4.npy          reference render, 4 spp, one thread (light_splatting: all threads),
+                               seed salt 0 (float64)
   <name>_ref_hi_a.npy/_b.npy   two independent reference renders at HI_SPP (float32)
   <name>_rays.npy              seeded ray batch (float32 n x 8)
   <name>_hits.npy              reference closest hits for the batch: geomID, primID, t bits (int32 n x 3)
@@ -29,7 +30,7 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from wurstrenderer_b200 import scenes  # noqa: E402
 
-FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt"]
+FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt", "cornell_ls", "hf_ls"]
 
 
 def with_integrator(path, integrator):
@@ -45,6 +46,8 @@ def with_integrator(path, integrator):
 def write_fixture_scene(name, out_dir):
     if name.endswith("_pt"):   # the same scene rendered by primitive_path_tracer
         return with_integrator(write_fixture_scene(name[:-3], out_dir), "primitive_path_tracer")
+    if name.endswith("_ls"):   # the same scene rendered by light_splatting
+        return with_integrator(write_fixture_scene(name[:-3], out_dir), "light_splatting")
     if name == "cornell":
         return scenes.write_cornell(out_dir, name="cornell", resolution=(48, 48), spp=4, num_path_vertices=10)
     if name == "zoo":
@@ -86,7 +89,8 @@ def main():
     args = ap.parse_args()
     if not oracle.reference_available():
         oracle.build(with_reference=True)
-    for name in FIXTURES:
+    # env_ls (light tracing under the sky: very noisy, kept for the oracle check and a flux test)
+    for name in FIXTURES + ["env_ls"]:
         if args.only and name != args.only:
             continue
         sdir = os.path.join(HERE, "scenes", name)
@@ -95,7 +99,9 @@ def main():
         raw = os.path.join(sdir, "_tmp.f64")
         sc = oracle.OracleScene(path)
         shape = (sc.height, sc.width, 3)
-        oracle.run_reference(path, tmp, serial=True, raw=raw)
+        # light_splatting runs through the reference's own multi-threaded render() only, so its
+        # 4-spp fixture is exact up to the order of the FP64 atomic splat sums
+        oracle.run_reference(path, tmp, serial=not name.endswith("_ls"), raw=raw)
         np.save(os.path.join(HERE, name + "_ref_spp4.npy"), np.fromfile(raw, np.float64).reshape(shape))
         for tag, salt in (("a", 11), ("b", 22)):
             rep = oracle.run_reference(path, tmp, spp=args.hi_spp, salt=salt, raw=raw)

@@ -11,7 +11,7 @@ import pytest
 from conftest import FIXTURES, GOLDEN, golden_scene
 
 
-@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("name", FIXTURES + ["env_ls"])
 def test_oracle_render_matches_reference_bit_exact(oracle_lib, name):
     path, meta = golden_scene(name)
     ref = np.load("%s/%s_ref_spp4.npy" % (GOLDEN, name))
@@ -19,7 +19,12 @@ def test_oracle_render_matches_reference_bit_exact(oracle_lib, name):
     img, _, paths = sc.render(threads=1)
     assert paths == sc.width * sc.height * 4
     assert img.shape == ref.shape
-    assert np.array_equal(img, ref), "max abs diff %g" % np.abs(img - ref).max()
+    if name.endswith("_ls"):
+        # the reference's light_splatting render is multi-threaded: exact up to the order of the
+        # FP64 atomic splat sums
+        assert np.allclose(img, ref, rtol=1e-12, atol=1e-15), "max abs diff %g" % np.abs(img - ref).max()
+    else:
+        assert np.array_equal(img, ref), "max abs diff %g" % np.abs(img - ref).max()
 
 
 @pytest.mark.parametrize("name", FIXTURES)

@@ -214,7 +214,8 @@ class Scene:
         d.use_graph = 1 if use_graph else 0
         d.profile = int(profile)
         d.trace_block = int(trace_block or 0)
-        d.integrator = {None: 0, "nextevent_path_tracer": 1, "primitive_path_tracer": 2}[integrator]
+        d.integrator = {None: 0, "nextevent_path_tracer": 1, "primitive_path_tracer": 2,
+                        "light_splatting": 3}[integrator]
         d.guiding = {False: 0, True: 1, 0: 0, 1: 1, 2: 2, "off": 0, "train": 1, "frozen": 2}[guiding]
         d.guide_train_spp = int(guide_train_spp or 0)
         d.guide_pass_spp = int(guide_pass_spp or 0)
@@ -228,7 +229,8 @@ class Scene:
                integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
                guide_batch=None, guide_steps=None, guide_clamp=None) -> np.ndarray:
         """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top).
-        integrator: None (the render entry's), "nextevent_path_tracer" or "primitive_path_tracer".
+        integrator: None (the render entry's), "nextevent_path_tracer", "primitive_path_tracer" or
+        "light_splatting".
         guiding: 0 / "off" (plain NEE+MIS), 1 / "train" (learned proposal trained online on the first
         guide_train_spp samples, default 32), 2 / "frozen" (the scene's current network, no training)."""
         inf = self.info

@@ -157,12 +157,17 @@ void build_device_scene(wr_scene &s) {
                 lo[k] = std::min(lo[k], verts[i + k]);
                 hi[k] = std::max(hi[k], verts[i + k]);
             }
+        double d2 = 0.0;
         for (int k = 0; k < 3; ++k) {
             if (!(lo[k] <= hi[k])) { lo[k] = 0.f; hi[k] = 1.f; }
             const float ext = std::max(hi[k] - lo[k], 1e-6f);
             s.box_lo[k] = lo[k] - 0.01f * ext;
             s.box_inv[k] = 1.f / (1.02f * ext);
+            s.dev.scene_center[k] = float((double(lo[k]) + double(hi[k])) * 0.5);
+            d2 += (double(hi[k]) - double(lo[k])) * (double(hi[k]) - double(lo[k]));
         }
+        // the bounding sphere of EmbreeAccel::boundingSphere (src/accel/embreeaccel.h:326-334)
+        s.dev.scene_radius = float(std::sqrt(d2) * 0.5);
     }
     wr::BvhBuildResult bvh;
     const auto tb = std::chrono::steady_clock::now();
@@ -428,6 +433,7 @@ void ensure_guide_wave(wr_scene &s, uint32_t capacity, uint32_t record_capacity)
 int integrator_of(const std::string &name) {
     if (name.empty() || name == "nextevent_path_tracer") return wrd::INTEGRATOR_NEE;
     if (name == "primitive_path_tracer") return wrd::INTEGRATOR_PRIMITIVE;
+    if (name == "light_splatting") return wrd::INTEGRATOR_LIGHT;
     throw Error(WR_ERR_UNSUPPORTED, "integrator '" + name + "' is not provided by this build");
 }
 
@@ -698,6 +704,7 @@ HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
     j.seed = desc.seed;
     j.integrator = desc.integrator == 1 ? wrd::INTEGRATOR_NEE
                  : desc.integrator == 2 ? wrd::INTEGRATOR_PRIMITIVE
+                 : desc.integrator == 3 ? wrd::INTEGRATOR_LIGHT
                                         : integrator_of(re.integrator);
     return j;
 }

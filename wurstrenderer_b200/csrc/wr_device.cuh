@@ -87,6 +87,7 @@ struct DevJob {
 };
 constexpr int INTEGRATOR_NEE = 0;        // nextevent_path_tracer (src/renderer/pathnextevent.h)
 constexpr int INTEGRATOR_PRIMITIVE = 1;  // primitive_path_tracer (src/renderer/primitivepath.h)
+constexpr int INTEGRATOR_LIGHT = 2;      // light_splatting (src/renderer/lightsplatting.h)
 
 struct DevScene {
     const float4 *nodes;
@@ -99,6 +100,8 @@ struct DevScene {
     const float *light_cdf;         // num_lights (+1 when env) entries
     int num_lights;
     int num_select;                 // num_lights + has_env
+    float scene_center[3];          // bounding sphere of all triangles (EmbreeAccel::boundingSphere,
+    float scene_radius;             //   src/accel/embreeaccel.h:326-334)
     // environment
     int has_env, env_w, env_h;
     float env_select_pdf;

@@ -389,6 +389,78 @@ __global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
     }
 }
 
+// lens point of a sample's camera vertex (ThinlensCamera::sampleWe0ByPdf, thinlens.h:121-136; the
+// pinhole origin when the aperture is zero) from the sample's dimension group 1
+__device__ __forceinline__ f3 lens_point(const DevCamera &cam, uint32_t lpix, uint32_t sample, uint32_t seed) {
+    const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), corg = ld3(cam.origin);
+    if (!(cam.aperture > 0.f)) return corg;
+    const Rand4 r1 = rand4(lpix, sample, 1, seed);
+    const float ax = 2.f * r1.a - 1.f, ay = 2.f * r1.b - 1.f;
+    float rr = 0.f, phi = 0.f;
+    if (ax != 0.f || ay != 0.f) {
+        if (ax * ax > ay * ay) { rr = ax; phi = (kPi / 4.f) * (ay / ax); }
+        else { rr = ay; phi = (kPi / 2.f) - (kPi / 4.f) * (ax / ay); }
+    }
+    float sn, cs;
+    sincosf(phi, &sn, &cs);
+    return corg + cfx * (rr * cs * cam.aperture) + cfy * (rr * sn * cam.aperture);
+}
+
+// Connection of a vertex to the lens point c0: direction and distance camera -> vertex, the
+// geometry term (cosine at the vertex only when it is not an environment vertex), the camera
+// importance evalWe1 with its raster position (thinlens.h:63-80) and the camera's area pdf of
+// the vertex (for MIS). Returns false when the vertex is behind the camera or off the film.
+struct CamLink {
+    f3 w;            // unit direction camera -> vertex
+    float len;       // distance (0 for an environment vertex)
+    float G;         // geometry term
+    float we;        // camera importance We1
+    float camPdfA;   // per-pixel camera pdf of the vertex in area measure
+    uint32_t slot;   // splat film slot (SPLAT_BIT set)
+};
+
+__device__ __forceinline__ bool camera_link(const DevJob &J, f3 c0, f3 p, f3 n, bool env, CamLink &k) {
+    const DevCamera &cam = J.cam;
+    const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), cfz = ld3(cam.fz), corg = ld3(cam.origin);
+    float conv;
+    if (env) {
+        k.w = p;
+        k.len = 0.f;
+        k.G = fabsf(dot(cfz, k.w));
+        conv = 1.f;
+    } else {
+        const f3 uv = p - c0;
+        const float d2 = len2(uv);
+        k.len = sqrtf(d2);
+        k.w = uv / k.len;
+        conv = fabsf(dot(n, k.w)) / d2;
+        k.G = fabsf(dot(cfz, k.w)) * conv;
+    }
+    const float cosT = dot(k.w, cfz);
+    if (!(k.G > 0.f) || !(cosT > 0.f)) return false;
+    const f3 cp = c0 - corg;
+    const f3 pl = mk(dot(cp, cfx), dot(cp, cfy), dot(cp, cfz));
+    const f3 dl = mk(dot(k.w, cfx), dot(k.w, cfy), cosT);
+    const f3 fpp = dl * (cam.focal / cosT) + pl;
+    const float fxp = -fpp.x / cam.focal * cam.dist, fyp = -fpp.y / cam.focal * cam.dist;
+    const float rx = (fxp / float(cam.width) + 0.5f) * float(cam.width);
+    const float ry = (fyp / float(cam.height) + 0.5f) * float(cam.height);
+    if (!(rx >= 0.f && rx < float(cam.width) && ry >= 0.f && ry < float(cam.height))) return false;
+    const float c2 = cosT * cosT;
+    k.we = cam.per_film / (c2 * c2);
+    k.camPdfA = cam.per_pixel / (c2 * cosT) * conv;
+    const uint32_t sx = min(uint32_t(rx), uint32_t(cam.width - 1));
+    const uint32_t sy = min(uint32_t(ry), uint32_t(cam.height - 1));
+    k.slot = (J.pix_offset + sy * uint32_t(cam.width) + sx) | SPLAT_BIT;
+    return true;
+}
+
+// a ray that leaves the scene's bounding sphere upward (a slot with no path to trace)
+__device__ __forceinline__ void dead_ray(const DevScene &s, f3 &o, f3 &d) {
+    o = mk(s.scene_center[0], s.scene_center[1] + 2.f * s.scene_radius + 1.f, s.scene_center[2]);
+    d = mk(0.f, 1.f, 0.f);
+}
+
 // One path of the current wavefront: emitter hit (strategy B) or NEE at a surface
 // (strategy A, one shadow ray), then BSDF sampling -- or, with lobes `gl` of the learned
 // proposal, one-sample MIS between the guide and the BSDF -- and compaction of the
@@ -402,6 +474,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
     f3 no = mk(0, 0, 0), nd = mk(0, 0, 1), nthr = mk(0, 0, 0);
     float npdf = 0.f;
     uint32_t pixel = 0, sample = 0, meta = 0;
+    uint32_t shadow_slot = MISS;        // film slot of the shadow record when it is not the path's pixel
     uint32_t rec = wrg::kNoRecord;      // newest training record of this path
     uint32_t nrec = wrg::kNoRecord;     // record of the continued path
     bool want_rec = false;              // a record is created for this vertex
@@ -420,7 +493,48 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
         const uint32_t tri = __float_as_uint(h.w);
         const float t = h.x;
         const bool primitive = J.integrator == INTEGRATOR_PRIMITIVE;
-        if (tri == MISS) {
+        if (J.integrator == INTEGRATOR_LIGHT) {
+            // light_splatting: a vertex of the light subpath (randomWalk callback,
+            // lightsplatting.h:85-104); emitter hits and misses end the subpath
+            if (tri != MISS && !(__ldg(s.tri_mat + tri) & LIGHT_BIT)) {
+                const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
+                const f3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(cc);
+                const f3 ng = normalize(cross(p1 - p0, p2 - p0));
+                const f3 pos = o + d * t;
+                const DevMaterial mm = s.materials[__ldg(s.tri_mat + tri)];
+                const Frame fr(ng);
+                const f3 inL = fr.to_local(-d);
+                const uint32_t lpix = pixel - J.pix_offset, seed = job_seed(J, job);
+                // connection to the sample's lens point: We1 * G * transmittance * bsdf(previous -> here
+                // -> camera) * path contribution, splatted with weight 1 / (spp * W * H) by the resolve
+                const f3 c0 = lens_point(J.cam, lpix, sample, seed);
+                CamLink cl;
+                if (camera_link(J, c0, pos, ng, false, cl)) {
+                    const f3 f = bsdf_eval(mm, inL, fr.to_local(-cl.w));
+                    const f3 c = thr * f * (cl.we * cl.G);
+                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                        shadow = true;
+                        so = pos; sd = -cl.w; sc = c;
+                        stmax = cl.len - kRayEps;
+                        shadow_slot = cl.slot;   // splat film (the path keeps its own pixel key)
+                    }
+                }
+                // the subpath has num_path_vertices - 2 walk vertices; this is walk vertex depth + 1
+                if (int(depth) + 3 < J.nverts) {
+                    const Rand4 rb = rand4(lpix, sample, 2 + depth, seed);
+                    f3 outL;
+                    float pdfW;
+                    const f3 wgt = bsdf_sample(mm, inL, rb.a, rb.b, outL, pdfW);
+                    if (!is_zero(wgt) && isfinite(wgt.x + wgt.y + wgt.z)) {
+                        alive = true;
+                        no = pos;
+                        nd = normalize(fr.to_world(outL));
+                        nthr = thr * wgt;
+                        npdf = pdfW;
+                    }
+                }
+            }
+        } else if (tri == MISS) {
             if (s.has_env) {
                 // strategy B on the environment (pathnextevent.h:128-146); the primitive tracer
                 // takes the emission with weight one (primitivepath.h:49-53)
@@ -541,7 +655,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
             }
         }
     }
-    push_shadow(w, shadow, so, sd, stmax, pixel, sc, rec);
+    push_shadow(w, shadow, so, sd, stmax, shadow_slot == MISS ? pixel : shadow_slot, sc, rec);
     if (w.records) {   // training record of this vertex (parent: the path's previous record)
         uint32_t nr;
         const uint32_t r = warp_append(w.rec_count, want_rec, nr);
@@ -601,6 +715,8 @@ __device__ __forceinline__ uint32_t new_samples(const WaveArgs &w, uint32_t fill
 }
 
 // new camera samples into the free tail of the next wavefront
+// new camera samples into the free tail of the next wavefront; for light_splatting the sample's
+// light subpath starts there instead
 __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) {
     const uint32_t filled = w.ctr[CTR_NEXT];
     const unsigned long long issued = *w.sample_next;
@@ -631,80 +747,85 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
             if (J.integrator == INTEGRATOR_PRIMITIVE) l.pdfA = 0.f;   // camera subpath only
             else l = sample_light(s, r0.a, r0.b);
             // camera vertex: lens point (pinhole when the aperture is zero)
-            f3 c0 = corg;
-            if (cam.aperture > 0.f) {
-                const Rand4 r1 = rand4(lpix, sample, 1, seed);
-                const float ax = 2.f * r1.a - 1.f, ay = 2.f * r1.b - 1.f;
-                float rr = 0.f, phi = 0.f;
-                if (ax != 0.f || ay != 0.f) {
-                    if (ax * ax > ay * ay) { rr = ax; phi = (kPi / 4.f) * (ay / ax); }
-                    else { rr = ay; phi = (kPi / 2.f) - (kPi / 4.f) * (ax / ay); }
-                }
-                float sn, cs;
-                sincosf(phi, &sn, &cs);
-                c0 = corg + cfx * (rr * cs * cam.aperture) + cfy * (rr * sn * cam.aperture);
-            }
-            // strategy C: connect the light vertex to the camera (pathnextevent.h:75-99)
-            if (l.pdfA > 0.f) {
-                f3 wl;          // direction camera -> light
-                float G, conv, len = 0.f;
-                if (l.env) {
-                    wl = l.pos;
-                    G = fabsf(dot(cfz, wl));
-                    conv = 1.f;
-                } else {
-                    const f3 uv = l.pos - c0;
-                    const float d2 = len2(uv);
-                    len = sqrtf(d2);
-                    wl = uv / len;
-                    conv = fabsf(dot(l.n, wl)) / d2;
-                    G = fabsf(dot(cfz, wl)) * conv;
-                }
-                const bool front = l.env || dot(l.n, wl) <= 0.f;
-                const float cosT = dot(wl, cfz);
-                if (G > 0.f && front && cosT > 0.f) {
-                    // evalWe1 (thinlens.h:63-80): project through the lens onto the film
-                    const f3 cp = c0 - corg;
-                    const f3 pl = mk(dot(cp, cfx), dot(cp, cfy), dot(cp, cfz));
-                    const f3 dl = mk(dot(wl, cfx), dot(wl, cfy), cosT);
-                    const f3 fpp = dl * (cam.focal / cosT) + pl;
-                    const float fxp = -fpp.x / cam.focal * cam.dist, fyp = -fpp.y / cam.focal * cam.dist;
-                    const float rx = (fxp / float(cam.width) + 0.5f) * float(cam.width);
-                    const float ry = (fyp / float(cam.height) + 0.5f) * float(cam.height);
-                    if (rx >= 0.f && rx < float(cam.width) && ry >= 0.f && ry < float(cam.height)) {
-                        const float c2 = cosT * cosT;
-                        const float we = cam.per_film / (c2 * c2);
-                        const float camPdfA = cam.per_pixel / (c2 * cosT) * conv;
-                        const float mis = l.pdfA / (l.pdfA + camPdfA);
-                        const float le1 = l.env ? 1.f : kInvPi;
-                        const f3 c = l.contrib * (mis * we * G * le1);
-                        const uint32_t sx = min(uint32_t(rx), uint32_t(cam.width - 1));
-                        const uint32_t sy = min(uint32_t(ry), uint32_t(cam.height - 1));
-                        if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
-                            shadow = true;
-                            slot = (J.pix_offset + sy * uint32_t(cam.width) + sx) | SPLAT_BIT;
-                            sc = c;
-                            if (l.env) { so = c0; sd = wl; stmax = __int_as_float(0x7f800000); }
-                            else { so = l.pos; sd = -wl; stmax = len - kRayEps; }
-                        }
+            const f3 c0 = lens_point(cam, lpix, sample, seed);
+            const uint32_t j = filled + k;
+            if (J.integrator == INTEGRATOR_LIGHT) {
+                // light_splatting (lightsplatting.h:47-108): the light vertex connected to the lens
+                // point with weight one, then the light subpath's first ray
+                CamLink cl;
+                if (l.pdfA > 0.f && camera_link(J, c0, l.pos, l.n, l.env, cl)) {
+                    const float le1 = l.env ? 1.f : (dot(l.n, -cl.w) >= 0.f ? kInvPi : 0.f);
+                    const f3 c = l.contrib * (cl.we * cl.G * le1);
+                    if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                        shadow = true;
+                        slot = cl.slot;
+                        sc = c;
+                        if (l.env) { so = c0; sd = cl.w; stmax = __int_as_float(0x7f800000); }
+                        else { so = l.pos; sd = -cl.w; stmax = cl.len - kRayEps; }
                     }
                 }
+                f3 o, d, thr = mk(0.f, 0.f, 0.f);
+                dead_ray(s, o, d);
+                if (l.pdfA > 0.f && !l.env && J.nverts > 2) {
+                    // sampleLe1CosByPdf (diffusearealight.h:73-81): cosine-weighted about the normal
+                    const Frame lf(l.n);
+                    o = l.pos;
+                    d = normalize(lf.to_world(cosine_hemisphere(r0.c, r0.d)));
+                    thr = l.contrib;
+                } else if (l.pdfA > 0.f && l.env && J.nverts > 2) {
+                    // sampleLe1CosByPdf (envmap.h:83-101): a point on the disk of the scene's bounding
+                    // sphere facing the sampled direction
+                    const float ax = 2.f * r0.c - 1.f, ay = 2.f * r0.d - 1.f;
+                    float rr = 0.f, phi = 0.f;
+                    if (ax != 0.f || ay != 0.f) {
+                        if (ax * ax > ay * ay) { rr = ax; phi = (kPi / 4.f) * (ay / ax); }
+                        else { rr = ay; phi = (kPi / 2.f) - (kPi / 4.f) * (ax / ay); }
+                    }
+                    float sn, cs;
+                    sincosf(phi, &sn, &cs);
+                    const float R = s.scene_radius;
+                    const Frame df(-l.pos);
+                    o = df.to_world(mk(rr * cs * R, -R, rr * sn * R)) +
+                        mk(s.scene_center[0], s.scene_center[1], s.scene_center[2]);
+                    d = -l.pos;
+                    thr = l.contrib * (kPi * R * R);
+                }
+                w.nxt.o[j] = make_float4(o.x, o.y, o.z, 0.f);
+                w.nxt.d[j] = make_float4(d.x, d.y, d.z, __uint_as_float(J.pix_offset + lpix));
+                w.nxt.thr[j] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(sample));
+                w.nxt.meta[j] = job << 8;
+                if (w.records) w.nxt.rec[j] = wrg::kNoRecord;
+            } else {
+                // strategy C: connect the light vertex to the camera (pathnextevent.h:75-99)
+                CamLink cl;
+                if (l.pdfA > 0.f && camera_link(J, c0, l.pos, l.n, l.env, cl)) {
+                    const bool front = l.env || dot(l.n, cl.w) <= 0.f;   // the light emits toward the camera
+                    const float mis = l.pdfA / (l.pdfA + cl.camPdfA);
+                    const float le1 = l.env ? 1.f : kInvPi;
+                    const f3 c = l.contrib * (mis * cl.we * cl.G * le1);
+                    if (front && !is_zero(c) && isfinite(c.x + c.y + c.z)) {
+                        shadow = true;
+                        slot = cl.slot;
+                        sc = c;
+                        if (l.env) { so = c0; sd = cl.w; stmax = __int_as_float(0x7f800000); }
+                        else { so = l.pos; sd = -cl.w; stmax = cl.len - kRayEps; }
+                    }
+                }
+                // primary ray through the jittered pixel position (thinlens.h:138-165)
+                const float nsx = (float(px) + r0.c) / float(cam.width), nsy = (float(py) + r0.d) / float(cam.height);
+                const f3 film = mk((nsx - 0.5f) * float(cam.width), (nsy - 0.5f) * float(cam.height), -cam.dist);
+                const f3 fpp = film * (cam.focal / film.z);
+                const f3 cpl = mk(dot(c0 - corg, cfx), dot(c0 - corg, cfy), dot(c0 - corg, cfz));
+                const f3 dir = normalize(fpp - cpl);
+                const float ct = dir.z;
+                const float pdfW = cam.per_film / (ct * ct * ct) / float(J.npix);
+                const f3 dw = normalize(cfx * dir.x + cfy * dir.y + cfz * dir.z);
+                w.nxt.o[j] = make_float4(c0.x, c0.y, c0.z, pdfW);
+                w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(J.pix_offset + lpix));
+                w.nxt.thr[j] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sample));
+                w.nxt.meta[j] = job << 8;
+                if (w.records) w.nxt.rec[j] = wrg::kNoRecord;
             }
-            // primary ray through the jittered pixel position (thinlens.h:138-165)
-            const float nsx = (float(px) + r0.c) / float(cam.width), nsy = (float(py) + r0.d) / float(cam.height);
-            const f3 film = mk((nsx - 0.5f) * float(cam.width), (nsy - 0.5f) * float(cam.height), -cam.dist);
-            const f3 fpp = film * (cam.focal / film.z);
-            const f3 cpl = mk(dot(c0 - corg, cfx), dot(c0 - corg, cfy), dot(c0 - corg, cfz));
-            const f3 dir = normalize(fpp - cpl);
-            const float ct = dir.z;
-            const float pdfW = cam.per_film / (ct * ct * ct) / float(J.npix);
-            const f3 dw = normalize(cfx * dir.x + cfy * dir.y + cfz * dir.z);
-            const uint32_t j = filled + k;
-            w.nxt.o[j] = make_float4(c0.x, c0.y, c0.z, pdfW);
-            w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(J.pix_offset + lpix));
-            w.nxt.thr[j] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sample));
-            w.nxt.meta[j] = job << 8;
-            if (w.records) w.nxt.rec[j] = wrg::kNoRecord;
         }
         push_shadow(w, shadow, so, sd, stmax, slot, sc);
     }

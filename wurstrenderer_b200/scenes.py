@@ -490,3 +490,64 @@ def write_env_scene(out_dir, name="env_scene", resolution=(128, 96), spp=8, num_
 def write_spec(out_dir, name, spec, camera, resolution, spp, num_path_vertices):
     cam = dict(camera, resolution=list(resolution))
     return write_scene(out_dir, name, spec, cam, [nee_render(name + ".pfm", spp, num_path_vertices)])
+
+
+def full_combination_spec(seed=1005, n_grid=2048, n_spheres=20000, sphere_subdiv=1, extent=24.0, n_lights=16):
+    """Workload C5: 2048^2-vertex fBm floor (8,380,418 triangles) + 20000 icospheres of 80 faces
+    (1,600,000) + 16 area lights (32): 9,980,450 triangles. Materials: 50 % Oren-Nayar, 50 %
+    Lambert + modified Phong with exponents log-uniform in [10, 2000]. Lit by the equirectangular
+    sky of `full_combination_envmap` as well."""
+    rng = np.random.default_rng(seed)
+    spec = SceneSpec()
+    pos, tris, h = fbm_heightfield(n_grid, extent, 0.6, 6, rng)
+    spec.add("floor", Material("m_floor", kd=(0.42, 0.40, 0.36), sigma=0.25), pos, tris)
+
+    def height_at(x, z):
+        u = (x + extent) / (2 * extent) * (n_grid - 1)
+        v = (z + extent) / (2 * extent) * (n_grid - 1)
+        return h[int(np.clip(round(u), 0, n_grid - 1)), int(np.clip(round(v), 0, n_grid - 1))]
+
+    n_mat = 256      # spheres share a pool of materials (one mesh per object, as the reference loads it)
+    mats = []
+    for i in range(n_mat):
+        name = "m_s%03d" % i
+        if i % 2 == 0:
+            mats.append(Material(name, kd=tuple(rng.uniform(0.2, 0.8, 3)), sigma=float(rng.uniform(0.0, 0.5))))
+        else:
+            kd = rng.uniform(0.05, 0.5, 3)
+            ks_scalar = rng.uniform(0.1, 0.9 - kd.max())
+            ks = np.clip(ks_scalar * rng.uniform(0.8, 1.0, 3), 0.0, 0.9 - kd)
+            n = math.exp(rng.uniform(math.log(10.0), math.log(2000.0)))
+            mats.append(Material(name, kd=tuple(kd), ks=tuple(ks), exponent=n))
+    for i in range(n_spheres):
+        r = math.exp(rng.uniform(math.log(0.05), math.log(0.5)))
+        x, z = rng.uniform(-extent * 0.95, extent * 0.95, 2)
+        cy = height_at(x, z) + r * rng.uniform(0.6, 1.4)
+        p, t = icosphere((x, cy, z), r, sphere_subdiv)
+        spec.add("sphere%05d" % i, mats[int(rng.integers(n_mat))], p, t)
+
+    for i in range(n_lights):
+        a = 2 * math.pi * (i + 0.5) / n_lights
+        rad = (0.3 + 0.4 * (i % 4) / 3.0) * extent
+        cx, cz = rad * math.cos(a), rad * math.sin(a)
+        y = 5.0 + 0.5 * (i % 3)
+        s = 0.6
+        p, t = quad((cx - s, y, cz - s), (cx + s, y, cz - s), (cx + s, y, cz + s), (cx - s, y, cz + s))
+        spec.add("light%02d" % i, Material("m_light%02d" % i, ke=(40.0, 36.0, 30.0)), p, t)
+    return spec
+
+
+FULL_COMBINATION_CAMERA = {"pos": [0.0, 4.5, 20.0], "lookat": [0.0, 0.5, 0.0], "up": [0.0, 1.0, 0.0],
+                           "fovy": 50.0, "resolution": [3840, 2160]}
+
+
+def write_full_combination(out_dir, name="full_combination", resolution=(3840, 2160), spp=1024,
+                           num_path_vertices=26, env_size=(2048, 1024), seed=1005, **kw):
+    """Workload C5 at its full size: 3840x2160, 1024 spp, max depth 24 (26 vertices), a
+    2048x1024 FP32 sky (3 Gaussian suns + gradient) plus 16 area lights, ~10M triangles."""
+    os.makedirs(out_dir, exist_ok=True)
+    env_name = name + "_sky.pfm"
+    write_pfm(os.path.join(out_dir, env_name), envmap_image(env_size[0], env_size[1], seed))
+    cam = dict(FULL_COMBINATION_CAMERA, resolution=list(resolution))
+    return write_scene(out_dir, name, full_combination_spec(seed, **kw), cam,
+                       [nee_render(name + ".pfm", spp, num_path_vertices)], envmap=env_name)
