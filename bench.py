@@ -53,11 +53,9 @@ def scene_path(rank, world, dist, workload="heightfield"):
         d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_cornell_v1")
         p = os.path.join(d, "cornell.json")
         writer = lambda: scenes.write_cornell(d)
-    elif workload == "door":
-        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_door_v1")
-        p = os.path.join(d, "door.json")
-        writer = lambda: scenes.write_spec(d, "door", scenes.door_room_spec(seed=1004), scenes.DOOR_ROOM_CAMERA,
-                                           (1024, 1024), 256, 10)
+    elif workload in ("door", "c5"):
+        d, p = workload_dir(workload)
+        writer = lambda: scenes.write_guided_workload(workload, d, spp=WORKLOAD_SPP[workload])
     else:
         d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_v1")
         p = os.path.join(d, "heightfield_spheres.json")
@@ -216,37 +214,53 @@ def relmse(x, ref, eps=1e-2):
 
 DOOR_WORKLOAD = ("door_room_200k: closed 6x3x6 m room, 1x1 emitter behind a partition with a 0.2 m door gap, "
                  "300 seeded Phong / Oren-Nayar boxes (197,782 triangles), 1024x1024, num_path_vertices 10")
+C5_WORKLOAD = ("full_combination_10M: 2048^2 fBm floor + 20000 icospheres (80 faces) + 16 area lights "
+               "(9,980,450 triangles), 2048x1024 FP32 sky (3 Gaussian suns + gradient), Phong exponents up "
+               "to 2000, 3840x2160, num_path_vertices 26 (max depth 24)")
+STUDY_WORKLOADS = {"door": DOOR_WORKLOAD, "c5": C5_WORKLOAD}
 
 
-def guided_vs_plain(wr, plain_spp=256, seeds=2):
-    """Equal-time relMSE of the learned proposal against plain NEE+MIS on the door-gap room, both
-    measured against the reference's own FP64 render of a 128x128 crop at 16384 spp
-    (tests/golden/door_crop_ref_{a,b}.npy, two independent 8192-spp halves). The guided render
+WORKLOAD_SPP = {"door": 256, "c5": 1024}
+
+
+def workload_dir(name):
+    d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_%s_v1" % name)
+    return d, os.path.join(d, "door.json" if name == "door" else "full_combination.json")
+
+
+def workload_scene(name):
+    """Writes (once per box) the full-size scene of a guided-vs-plain workload; returns its JSON path."""
+    from wurstrenderer_b200 import scenes
+    d, p = workload_dir(name)
+    if not os.path.exists(p + ".done"):
+        scenes.write_guided_workload(name, d, spp=WORKLOAD_SPP[name])
+        open(p + ".done", "w").write("ok")
+    return p
+
+
+def guided_vs_plain(wr, name="door", plain_spp=256, seeds=2):
+    """Equal-time relMSE of the learned proposal against plain NEE+MIS on a full-size workload,
+    both measured against the reference's own FP64 render of a crop at 16384 spp
+    (tests/golden/<name>_crop_ref_{a,b}.npy, two independent 8192-spp halves). The guided render
     (training on its first 32 spp included) gets the device time of the plain render."""
     import numpy as np
-    from wurstrenderer_b200 import scenes
     gdir = os.path.join(ROOT, "tests", "golden")
-    meta_p = os.path.join(gdir, "door_crop_meta.json")
+    meta_p = os.path.join(gdir, "%s_crop_meta.json" % name)
     if not os.path.exists(meta_p):
-        return {"unavailable": "door-room reference crop not generated (tests/golden/make_crop_golden.py)"}
+        return {"unavailable": "reference crop not generated (tests/golden/make_crop_golden.py)"}
     meta = json.load(open(meta_p))
-    ref_a = np.load(os.path.join(gdir, "door_crop_ref_a.npy")).astype(np.float64)
-    ref_b = np.load(os.path.join(gdir, "door_crop_ref_b.npy")).astype(np.float64)
+    ref_a = np.load(os.path.join(gdir, "%s_crop_ref_a.npy" % name)).astype(np.float64)
+    ref_b = np.load(os.path.join(gdir, "%s_crop_ref_b.npy" % name)).astype(np.float64)
     ref = 0.5 * (ref_a + ref_b)
     x0, y0, x1, y1 = meta["crop"]
-    d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_door_v1")
-    p = os.path.join(d, "door.json")
-    if not os.path.exists(p + ".done"):
-        res = tuple(meta["resolution"])
-        scenes.write_spec(d, "door", scenes.door_room_spec(seed=1004), dict(scenes.DOOR_ROOM_CAMERA, resolution=list(res)),
-                          res, 64, meta["num_path_vertices"])
-        open(p + ".done", "w").write("ok")
-    out = {"workload": DOOR_WORKLOAD, "oracle": "reference PathNeeRenderer (FP64 CPU), 16384 spp, crop %s" % meta["crop"],
+    p = workload_scene(name)
+    out = {"workload": STUDY_WORKLOADS[name],
+           "oracle": "reference PathNeeRenderer (FP64 CPU), 16384 spp, crop %s" % meta["crop"],
            "relmse_def": "mean over crop pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)",
            "oracle_noise_relmse": relmse(ref_a, ref_b) / 4.0}
     with wr.Scene.from_file(p) as sc:
-        sc.render(spp=4, seed=1)                       # warm-up (allocations, graph paths)
-        sc.render(spp=8, seed=2, guiding=1, guide_train_spp=8, guide_steps=16)
+        sc.render(spp=1, seed=1)                       # warm-up (allocations, graph paths)
+        sc.render(spp=2, seed=2, guiding=1, guide_train_spp=2, guide_steps=16)
         plain_err, plain_ms = [], []
         for i in range(seeds):
             img = sc.render(spp=plain_spp, seed=100 + i)
@@ -291,10 +305,12 @@ def main():
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven launches instead of one graph per render (profiling runs: ncu does not "
                          "profile kernels inside conditional graph nodes)")
-    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128", "door"],
+    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128", "door", "c5"],
                     help="heightfield: the 1M-triangle single render (headline); jobs128: 128 batched jobs "
                          "over the Cornell box, one graph launch per step; door: one guided render (learned "
-                         "proposal trained on its first 32 spp) of the 200k-triangle door-gap room")
+                         "proposal trained on its first 32 spp) of the 200k-triangle door-gap room at 256 spp; "
+                         "c5: one plain render of the 10M-triangle full combination at 3840x2160, 1024 spp, "
+                         "with the guided-vs-plain study on it")
     args = ap.parse_args()
 
     world = env_int("WORLD_SIZE", 1)
@@ -451,8 +467,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 film + CDF build)", "data": "synthetic (seeded procedural scene)",
             "config": {"workload": {"heightfield": WORKLOAD, "jobs128": WORKLOAD_JOBS,
-                                    "door": DOOR_WORKLOAD + ", guided (learned proposal trained on its first 32 spp)"}[
-                                        args.workload],
+                                    "door": DOOR_WORKLOAD + ", 256 spp, guided (learned proposal trained on its "
+                                                            "first 32 spp)",
+                                    "c5": C5_WORKLOAD + ", 1024 spp, plain NEE+MIS"}[args.workload],
                        "parallelism": "replicas x%d, FP64 film reduce" % world,
                        "autotuned": tune, "autotune_probe_ms": tune_ms,
                        "l2": "256 MB buffer written between timed steps; path state > L2",
@@ -467,8 +484,10 @@ def main():
             "mrays_per_s": (k_items["extend"] + k_items["shadow"]) * world * args.steps / (max_ms / 1e3) / 1e6}
     if rank == 0 and not args.no_cpu_baseline and batch_jobs is None:
         line["cpu_baseline"] = cpu_baseline(path)
-    if world == 1 and not args.no_guiding and batch_jobs is None:
-        line["equal_time_relmse"] = guided_vs_plain(wr)
+    if world == 1 and not args.no_guiding and args.workload in ("heightfield", "c5"):
+        study = "c5" if args.workload == "c5" else "door"
+        line["equal_time_relmse"] = guided_vs_plain(wr, study, plain_spp=1024 if study == "c5" else 256,
+                                                    seeds=1 if study == "c5" else 2)
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()

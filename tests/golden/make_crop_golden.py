@@ -34,21 +34,15 @@ import oracle  # noqa: E402
 from wurstrenderer_b200 import scenes  # noqa: E402
 
 WORKLOADS = {
-    "door": {"crop": (448, 448, 576, 576), "resolution": (1024, 1024), "num_path_vertices": 10,
-             "scene": "scenes.door_room_spec(seed=1004)", "camera": scenes.DOOR_ROOM_CAMERA},
-    "c5": {"crop": (1856, 1056, 1984, 1120), "resolution": (3840, 2160), "num_path_vertices": 26,
-           "scene": "scenes.write_full_combination(seed=1005)", "camera": scenes.FULL_COMBINATION_CAMERA},
+    "door": {"scene": "scenes.door_room_spec(seed=1004)", "camera": scenes.DOOR_ROOM_CAMERA},
+    "c5": {"scene": "scenes.write_full_combination(seed=1005)", "camera": scenes.FULL_COMBINATION_CAMERA},
 }
+for _name, _w in WORKLOADS.items():
+    _w.update(scenes.GUIDED_WORKLOADS[_name])
 
 
 def write_workload_scene(name, out_dir, spp=64):
-    w = WORKLOADS[name]
-    if name == "door":
-        cam = dict(scenes.DOOR_ROOM_CAMERA, resolution=list(w["resolution"]))
-        return scenes.write_spec(out_dir, "door", scenes.door_room_spec(seed=1004), cam, w["resolution"], spp,
-                                 w["num_path_vertices"])
-    return scenes.write_full_combination(out_dir, resolution=w["resolution"], spp=spp,
-                                         num_path_vertices=w["num_path_vertices"], seed=1005)
+    return scenes.write_guided_workload(name, out_dir, spp)
 
 
 def main():

@@ -284,6 +284,37 @@ def test_door_room_crop_matches_reference(wr_lib, tmp_path, guiding):
     floor = relmse(ref_a, ref_b)
     err = relmse(img, ref)
     assert err <= 2.0 * floor, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
-    z = block_z(runs, ref)
+    z = block_z(runs, ref, ref_pair=(ref_a, ref_b))
+    assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
+    assert abs(img.mean() / ref.mean() - 1.0) < 0.01
+
+
+@pytest.mark.parametrize("guiding", [0, 1])
+def test_full_combination_crop_matches_reference(wr_lib, tmp_path, guiding):
+    """The 10M-triangle full combination (config 5: sky + 16 area lights, Phong exponents up to
+    2000, 3840x2160, 26 vertices) against the reference's FP64 render of a 128x64 crop at 16384
+    spp: plain and guided GPU renders (4 x 640 spp) within 2 x the crop's noise floor, every 8x8
+    block |z| < 4, crop mean within 1 %."""
+    import json
+    from test_gpu_render import block_z
+    from wurstrenderer_b200 import scenes
+    meta_p = os.path.join(GOLDEN, "c5_crop_meta.json")
+    if not os.path.exists(meta_p):
+        pytest.skip("full-combination reference crop not generated")
+    meta = json.load(open(meta_p))
+    ref_a = np.load(os.path.join(GOLDEN, "c5_crop_ref_a.npy")).astype(np.float64)
+    ref_b = np.load(os.path.join(GOLDEN, "c5_crop_ref_b.npy")).astype(np.float64)
+    path = scenes.write_guided_workload("c5", str(tmp_path))
+    x0, y0, x1, y1 = meta["crop"]
+    K = 4
+    with wr_lib.Scene.from_file(path, bvh_builder=wr_lib.BVH_DEVICE_LBVH) as sc:
+        assert sc.info["num_triangles"] == 9980450
+        runs = np.stack([sc.render(spp=640, seed=900 + i, guiding=guiding)[y0:y1, x0:x1] for i in range(K)])
+    ref = 0.5 * (ref_a + ref_b)
+    img = runs.mean(axis=0)
+    floor = relmse(ref_a, ref_b)
+    err = relmse(img, ref)
+    assert err <= 2.0 * floor, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
+    z = block_z(runs, ref, ref_pair=(ref_a, ref_b))
     assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
     assert abs(img.mean() / ref.mean() - 1.0) < 0.01

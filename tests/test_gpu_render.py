@@ -27,8 +27,14 @@ def relmse(x, ref, eps=1e-2):
     return float(np.mean((x - ref) ** 2 / (ref ** 2 + eps)))
 
 
-def block_z(runs, ref, block=8):
-    """z scores of 8x8 block means; runs: K x H x W x 3 independent renders."""
+def block_z(runs, ref, block=8, ref_pair=None):
+    """z scores of 8x8 block means; runs: K x H x W x 3 independent renders.
+
+    Without ref_pair the reference's variance is taken equal to the GPU's (same spp, same
+    estimator): z = (gpu - ref) / sqrt(2 var_gpu). With ref_pair = (ref_a, ref_b), two independent
+    halves whose mean is `ref`, the reference's own variance is estimated from them per pixel,
+    (a - b)^2 / 4, and z = (gpu - ref) / sqrt(var_gpu + var_ref) -- needed when the GPU estimator
+    is much less noisy than the reference (the learned proposal)."""
     k, h, w, _ = runs.shape
     hb, wb = h // block, w // block
     r = runs[:, :hb * block, :wb * block].reshape(k, hb, block, wb, block, 3)
@@ -36,7 +42,12 @@ def block_z(runs, ref, block=8):
     pix_var = runs[:, :hb * block, :wb * block].var(axis=0, ddof=1) / k      # variance of the K-run mean, per pixel
     var_b = pix_var.reshape(hb, block, wb, block, 3).sum(axis=(1, 3)) / (block * block) ** 2
     mean_b = r.mean(axis=0).mean(axis=(1, 3))
-    return (mean_b - ref_b) / np.sqrt(2.0 * var_b + 1e-30)
+    if ref_pair is None:
+        return (mean_b - ref_b) / np.sqrt(2.0 * var_b + 1e-30)
+    a, b = ref_pair
+    ref_var = ((a - b) ** 2 / 4.0)[:hb * block, :wb * block]
+    var_r = ref_var.reshape(hb, block, wb, block, 3).sum(axis=(1, 3)) / (block * block) ** 2
+    return (mean_b - ref_b) / np.sqrt(var_b + var_r + 1e-30)
 
 
 @pytest.mark.parametrize("name", FIXTURES)

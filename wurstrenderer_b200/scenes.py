@@ -551,3 +551,21 @@ def write_full_combination(out_dir, name="full_combination", resolution=(3840, 2
     cam = dict(FULL_COMBINATION_CAMERA, resolution=list(resolution))
     return write_scene(out_dir, name, full_combination_spec(seed, **kw), cam,
                        [nee_render(name + ".pfm", spp, num_path_vertices)], envmap=env_name)
+
+
+# the full-size guided-vs-plain workloads whose FP64 reference crops live in tests/golden
+GUIDED_WORKLOADS = {
+    "door": {"resolution": (1024, 1024), "num_path_vertices": 10, "crop": (448, 448, 576, 576)},
+    "c5": {"resolution": (3840, 2160), "num_path_vertices": 26, "crop": (1856, 1056, 1984, 1120)},
+}
+
+
+def write_guided_workload(name, out_dir, spp=64):
+    """Writes the door-gap room (config 4) or the full combination (config 5) at full size."""
+    w = GUIDED_WORKLOADS[name]
+    if name == "door":
+        cam = dict(DOOR_ROOM_CAMERA, resolution=list(w["resolution"]))
+        return write_spec(out_dir, "door", door_room_spec(seed=1004), cam, w["resolution"], spp,
+                          w["num_path_vertices"])
+    return write_full_combination(out_dir, resolution=w["resolution"], spp=spp,
+                                  num_path_vertices=w["num_path_vertices"], seed=1005)
