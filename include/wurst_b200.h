@@ -255,8 +255,8 @@ int wr_write_pfm(const char *path, const double *rgb, int width, int height);
 /* Whole simple2 flow of the reference CLI (src/main.cpp:5-15,
  * src/sceneio/simple2parser.h:102-223): load the scene, render every
  * "nextevent_path_tracer" entry of "render" and write its "output" PFM next
- * to the scene JSON; "primitive_path_tracer" entries likewise. Other
- * integrators return WR_ERR_UNSUPPORTED. */
+ * to the scene JSON; "primitive_path_tracer" and "light_splatting" entries
+ * likewise. Other integrators return WR_ERR_UNSUPPORTED. */
 int wr_run_simple2(const char *scene_json_path);
 int wr_run_jsimple2(const char *json_text);
 

@@ -1004,7 +1004,7 @@ void run_scene(wr_scene &s) {
     const wr::Scene &h = s.host;
     for (size_t i = 0; i < h.renders.size(); ++i) {
         const wr::RenderEntry &re = h.renders[i];
-        integrator_of(re.integrator);   // nextevent_path_tracer or primitive_path_tracer
+        integrator_of(re.integrator);   // nextevent_path_tracer, primitive_path_tracer or light_splatting
         wr_render_desc d{};
         d.render_index = int(i);
         d.use_graph = 1;
