@@ -347,7 +347,7 @@ def main():
     tune = {}
     tune_ms = None
     if not args.no_autotune:
-        tune, tune_ms = scene.autotune(probe_spp=4)
+        tune, tune_ms = scene.autotune(probe_spp=16)
         tune = {k: v for k, v in tune.items() if k != "use_graph"}
     if args.queue_capacity:
         tune["queue_capacity"] = args.queue_capacity

@@ -43,7 +43,9 @@ enum Counter {
     CTR_SHADOW_MAX = 5,  // largest shadow queue seen
     CTR_OVERFLOW = 6,    // shadow queue overflowed (not expected: its capacity is 2x the wavefront)
     CTR_TIMEOUT = 7,     // the iteration bound was reached before the wavefront drained
-    CTR_COUNT = 8
+    CTR_EXTEND_FETCH = 8,   // next ray of the current extend launch (dynamic fetching)
+    CTR_SHADOW_FETCH = 9,   // next shadow ray of the current shadow launch
+    CTR_COUNT = 10
 };
 
 struct DevMaterial {

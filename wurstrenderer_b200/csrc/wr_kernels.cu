@@ -368,25 +368,80 @@ __device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c)
     atomicAdd(f + 2, double(c.z));
 }
 
+// Persistent traversal of a ray queue with dynamic ray fetching: every lane keeps one ray
+// in flight; a warp whose traversing lanes drop below kFetchThreshold leaves the traversal
+// loop and its idle lanes take the next rays of the queue (one atomic per warp), so that
+// SIMD lanes are not left idle while a few long rays finish (Aila & Laine, HPG 2009). Once
+// the queue is exhausted the remaining rays run to completion.
+//   SHADOW = false: extend -- closest hit of every live path into the hit records
+//   SHADOW = true:  shadow -- any hit of every queued shadow ray; unoccluded contributions
+//                   are added to the FP64 film (and to the path's training records)
+constexpr int kFetchThreshold = 20;
+
+template <int BLOCK, bool SHADOW>
+__device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w, uint32_t *stack) {
+    const uint32_t n = SHADOW ? min(w.ctr[CTR_SHADOW], w.shadow_capacity) : w.ctr[CTR_ACTIVE];
+    uint32_t *fetch = w.ctr + (SHADOW ? CTR_SHADOW_FETCH : CTR_EXTEND_FETCH);
+    TraceStack st;
+    st.smem = stack + threadIdx.x;
+    st.stride = BLOCK;
+    st.sp = 0;
+    RayPre r{};
+    float t = 0.f, bu = 0.f, bv = 0.f;
+    uint32_t tri = MISS, ray = 0, nv = 0, nt = 0;
+    int node = kTraceDone, leaf = 0;
+    bool busy = false, exhausted = false;
+    const uint32_t lane = lane_id();
+    while (true) {
+        const uint32_t need = __ballot_sync(0xffffffffu, !busy && !exhausted);
+        if (need) {
+            const uint32_t leader = __ffs(need) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(fetch, uint32_t(__popc(need)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!busy && !exhausted) {
+                ray = base + uint32_t(__popc(need & ((1u << lane) - 1u)));
+                if (ray < n) {
+                    float4 o, d;
+                    float tmax;
+                    if (SHADOW) { o = w.sq.o[ray]; d = w.sq.d[ray]; tmax = o.w; }
+                    else { o = w.cur.o[ray]; d = w.cur.d[ray]; tmax = __int_as_float(0x7f800000); }
+                    r = ray_setup(xyz(o), xyz(d));
+                    t = tmax; tri = MISS; bu = 0.f; bv = 0.f;
+                    node = 0; leaf = 0; st.sp = 0;
+                    busy = true;
+                } else {
+                    exhausted = true;   // the queue counter only grows: no lane gets another ray
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) break;
+        const int min_active = __any_sync(0xffffffffu, exhausted) ? 0 : kFetchThreshold;
+        if (busy && traverse_steps<SHADOW>(s.nodes, s.tris, r, kRayEps, t, tri, bu, bv, node, leaf, st, nv, nt,
+                                           min_active)) {
+            busy = false;
+            if (SHADOW) {
+                if (tri == MISS) {   // unoccluded
+                    const float4 c = w.sq.c[ray];
+                    film_add(w, __float_as_uint(w.sq.d[ray].w), mk(c.x, c.y, c.z));
+                    if (w.records) record_contribution(w.records, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+                }
+            } else {
+                w.hit[ray] = make_float4(t, bu, bv, __uint_as_float(tri));
+            }
+        }
+    }
+    if (w.prof) {
+        atomicAdd(w.prof + (SHADOW ? 8 : 6), (unsigned long long)nv);
+        atomicAdd(w.prof + (SHADOW ? 9 : 7), (unsigned long long)nt);
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + (SHADOW ? 3 : 0), (unsigned long long)n);
+    }
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    const uint32_t n = w.ctr[CTR_ACTIVE];
-    uint32_t nv = 0, nt = 0;
-    uint32_t *pv = w.prof ? &nv : nullptr, *pt = w.prof ? &nt : nullptr;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = w.cur.o[i], d = w.cur.d[i];
-        float t, bu = 0.f, bv = 0.f;
-        uint32_t tri;
-        traverse<false>(s.nodes, s.tris, xyz(o), xyz(d), kRayEps, __int_as_float(0x7f800000), stack, t, tri, bu, bv,
-                        pv, pt);
-        w.hit[i] = make_float4(t, bu, bv, __uint_as_float(tri));
-    }
-    if (w.prof) {
-        atomicAdd(w.prof + 6, (unsigned long long)nv);
-        atomicAdd(w.prof + 7, (unsigned long long)nt);
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 0, (unsigned long long)n);
-    }
+    trace_queue<BLOCK, false>(s, w, stack);
 }
 
 // lens point of a sample's camera vertex (ThinlensCamera::sampleWe0ByPdf, thinlens.h:121-136; the
@@ -834,25 +889,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    const uint32_t n = min(w.ctr[CTR_SHADOW], w.shadow_capacity);
-    uint32_t nv = 0, nt = 0;
-    uint32_t *pv = w.prof ? &nv : nullptr, *pt = w.prof ? &nt : nullptr;
-    if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 3, (unsigned long long)n);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = w.sq.o[i], d = w.sq.d[i];
-        float t, bu, bv;
-        uint32_t tri;
-        const bool occ = traverse<true>(s.nodes, s.tris, xyz(o), xyz(d), kRayEps, o.w, stack, t, tri, bu, bv, pv, pt);
-        if (!occ) {
-            const float4 c = w.sq.c[i];
-            film_add(w, __float_as_uint(d.w), mk(c.x, c.y, c.z));
-            if (w.records) record_contribution(w.records, __float_as_uint(c.w), mk(c.x, c.y, c.z));
-        }
-    }
-    if (w.prof) {
-        atomicAdd(w.prof + 8, (unsigned long long)nv);
-        atomicAdd(w.prof + 9, (unsigned long long)nt);
-    }
+    trace_queue<BLOCK, true>(s, w, stack);
 }
 
 // queue bookkeeping between iterations (one thread); also drives the graph's while loop
@@ -865,6 +902,8 @@ __global__ void k_advance(WaveArgs w) {
     w.ctr[CTR_ACTIVE] = filled + n_new;
     w.ctr[CTR_NEXT] = 0;
     w.ctr[CTR_SHADOW] = 0;
+    w.ctr[CTR_EXTEND_FETCH] = 0;
+    w.ctr[CTR_SHADOW_FETCH] = 0;
     const uint32_t iter = w.ctr[CTR_ITER] + 1;
     w.ctr[CTR_ITER] = iter;
     *w.sample_next = issued + n_new;

@@ -199,4 +199,78 @@ __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const
     return tri != MISS;
 }
 
+// Resumable form of `traverse` for persistent kernels with dynamic ray fetching (Aila &
+// Laine 2009, "replace terminated rays"): the per-ray state (node, postponed leaf, stack,
+// best hit) lives in the caller and survives between calls. The while-while loop runs as in
+// `traverse`, but after each leaf pass the warp leaves it when fewer than `min_active` of its
+// lanes are still traversing, so that the caller can hand new rays to the finished lanes.
+// Returns true when this lane's ray is finished (any hit found for ANY_HIT, or the tree
+// exhausted); the result is the same as `traverse`'s, only the schedule differs.
+constexpr int kTraceDone = 0x7fffffff;
+
+template <bool ANY_HIT>
+__device__ __forceinline__ bool traverse_steps(const float4 *__restrict__ nodes, const float4 *__restrict__ tris,
+                                               const RayPre &r, float tmin, float &t, uint32_t &tri, float &bu,
+                                               float &bv, int &node, int &leaf, TraceStack &st, uint32_t &nv,
+                                               uint32_t &nt, int min_active) {
+    while (node != kTraceDone) {
+        while (node >= 0 && node != kTraceDone) {
+            const float4 n0 = __ldg(nodes + 4 * node + 0);
+            const float4 n1 = __ldg(nodes + 4 * node + 1);
+            const float4 n2 = __ldg(nodes + 4 * node + 2);
+            const float4 n3 = __ldg(nodes + 4 * node + 3);
+            ++nv;
+            const float e0 = box_entry(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, tmin, t);
+            const float e1 = box_entry(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, tmin, t);
+            const int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            const bool h0 = e0 != __int_as_float(0x7f800000), h1 = e1 != __int_as_float(0x7f800000);
+            if (h0 && h1) {
+                int near = c0, far = c1;
+                if (e1 < e0) { near = c1; far = c0; }
+                st.push(far);
+                node = near;
+            } else if (h0) {
+                node = c0;
+            } else if (h1) {
+                node = c1;
+            } else {
+                node = st.sp ? st.pop() : kTraceDone;
+            }
+            if (node < 0 && leaf == 0) {   // postpone the first leaf found, keep descending
+                leaf = node;
+                node = st.sp ? st.pop() : kTraceDone;
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;
+        }
+        while (leaf < 0) {
+            const uint32_t code = uint32_t(leaf);
+            const uint32_t first = code & 0x07ffffffu;
+            const uint32_t count = ((code >> 27) & 0xfu) + 1u;
+            for (uint32_t i = first; i < first + count; ++i) {
+                const float4 a = __ldg(tris + 3 * i + 0);
+                const float4 b = __ldg(tris + 3 * i + 1);
+                const float4 c = __ldg(tris + 3 * i + 2);
+                ++nt;
+                float th, uh, vh;
+                if (tri_test(r, a, b, c, tmin, t, th, uh, vh)) {
+                    if (ANY_HIT) {
+                        t = th; tri = i; bu = uh; bv = vh;
+                        node = kTraceDone;
+                        leaf = 0;
+                        return true;
+                    }
+                    if (th < t || tri == MISS) { t = th; tri = i; bu = uh; bv = vh; }
+                }
+            }
+            leaf = 0;
+            if (node < 0 && node != kTraceDone) {   // the traversal is sitting on another leaf
+                leaf = node;
+                node = st.sp ? st.pop() : kTraceDone;
+            }
+        }
+        if (node != kTraceDone && __popc(__activemask()) < min_active) return false;
+    }
+    return true;
+}
+
 }  // namespace wrd
