@@ -353,7 +353,8 @@ def main():
         tune["queue_capacity"] = args.queue_capacity
     qc = tune.get("queue_capacity")
     knobs = dict(grid_trace=tune.get("grid_trace"), grid_shade=tune.get("grid_shade"),
-                 trace_block=tune.get("trace_block"), use_graph=not args.no_graph)
+                 trace_block=tune.get("trace_block"), fetch_threshold=tune.get("fetch_threshold"),
+                 use_graph=not args.no_graph)
 
     batch_jobs = None
     if args.workload == "jobs128":

@@ -65,7 +65,9 @@ typedef struct wr_render_desc {
                                 pass), 256 to 8192 steps */
     float guide_clamp;       /* loss weights are clamped at guide_clamp x their mean over the pass;
                                 0 = 1000, < 0 = no clamp */
-    int reserved[4];
+    int fetch_threshold;     /* traversal: a warp hands new rays to its idle lanes when fewer than this
+                                many of its 32 lanes are still traversing; 1..32, 0 = 20 */
+    int reserved[3];
 } wr_render_desc;
 
 typedef struct wr_render_stats {
@@ -196,8 +198,9 @@ int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc, double
 
 /* Autotuner (no counterpart in the reference): times short renders of the
  * scene's camera at probe_spp samples per pixel over traversal block sizes
- * {64, 128, 256}, wavefront capacities {2^19 .. 2^22} and persistent-CTA counts
- * {1/2, 1} x the occupancy limit (coordinate descent, starting from `base`), and
+ * {64, 128, 256}, wavefront capacities {2^19 .. 2^22}, persistent-CTA counts
+ * {1/2, 1} x the occupancy limit and ray-fetching thresholds {12 .. 28}
+ * (coordinate descent, starting from `base`), and
  * writes the fastest settings into *best (other fields copied from base) and
  * its time per render into *best_ms. */
 int wr_autotune(wr_scene *scene, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms);

@@ -43,7 +43,8 @@ class RenderDesc(ctypes.Structure):
                 ("grid_shade", ctypes.c_int), ("use_graph", ctypes.c_int), ("profile", ctypes.c_int),
                 ("trace_block", ctypes.c_int), ("integrator", ctypes.c_int), ("guiding", ctypes.c_int),
                 ("guide_train_spp", ctypes.c_int), ("guide_pass_spp", ctypes.c_int), ("guide_batch", ctypes.c_int),
-                ("guide_steps", ctypes.c_int), ("guide_clamp", ctypes.c_float), ("reserved", ctypes.c_int * 4)]
+                ("guide_steps", ctypes.c_int), ("guide_clamp", ctypes.c_float), ("fetch_threshold", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
 
 
 class Job(ctypes.Structure):
@@ -202,7 +203,7 @@ class Scene:
     @staticmethod
     def _desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
               profile=0, trace_block=None, integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
-              guide_batch=None, guide_steps=None, guide_clamp=None):
+              guide_batch=None, guide_steps=None, guide_clamp=None, fetch_threshold=None):
         d = RenderDesc()
         d.num_spp = int(spp or 0)
         d.num_path_vertices = int(num_path_vertices or 0)
@@ -222,12 +223,13 @@ class Scene:
         d.guide_batch = int(guide_batch or 0)
         d.guide_steps = int(guide_steps or 0)
         d.guide_clamp = float(guide_clamp or 0.0)
+        d.fetch_threshold = int(fetch_threshold or 0)
         return d
 
     def render(self, spp=None, num_path_vertices=None, seed=0, render_index=0, queue_capacity=None,
                grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0, trace_block=None,
                integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
-               guide_batch=None, guide_steps=None, guide_clamp=None) -> np.ndarray:
+               guide_batch=None, guide_steps=None, guide_clamp=None, fetch_threshold=None) -> np.ndarray:
         """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top).
         integrator: None (the render entry's), "nextevent_path_tracer", "primitive_path_tracer" or
         "light_splatting".
@@ -238,16 +240,16 @@ class Scene:
             out = np.empty((inf["height"], inf["width"], 3), np.float64)
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
                        profile, trace_block, integrator, guiding, guide_train_spp, guide_pass_spp, guide_batch,
-                       guide_steps, guide_clamp)
+                       guide_steps, guide_clamp, fetch_threshold)
         _check(load_library().wr_render(self._h, ctypes.byref(d), _ptr(out)))
         return out
 
     def render_device(self, out_device_ptr: int, spp=None, num_path_vertices=None, seed=0, render_index=0,
                       queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
-                      trace_block=None, guiding=0, guide_steps=None) -> None:
+                      trace_block=None, guiding=0, guide_steps=None, fetch_threshold=None) -> None:
         """Renders into device memory at `out_device_ptr` (W*H*3 doubles)."""
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
-                       profile, trace_block, None, guiding, None, None, None, guide_steps)
+                       profile, trace_block, None, guiding, None, None, None, guide_steps, None, fetch_threshold)
         _check(load_library().wr_render_device(self._h, ctypes.byref(d), ctypes.c_void_p(int(out_device_ptr))))
 
     def autotune(self, probe_spp=4, **base):
@@ -257,11 +259,11 @@ class Scene:
         best = RenderDesc()
         ms = ctypes.c_double(0.0)
         _check(load_library().wr_autotune(self._h, ctypes.byref(d0), int(probe_spp), ctypes.byref(best), ctypes.byref(ms)))
-        keys = ("queue_capacity", "grid_trace", "grid_shade", "trace_block", "use_graph")
+        keys = ("queue_capacity", "grid_trace", "grid_shade", "trace_block", "use_graph", "fetch_threshold")
         return {k: getattr(best, k) for k in keys}, ms.value
 
     def render_batch(self, jobs, queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
-                     trace_block=None):
+                     trace_block=None, fetch_threshold=None):
         """jobs: list of dicts {camera (dict or JSON text), num_spp, num_path_vertices, seed}.
         Returns one (H, W, 3) float64 image per job, rendered in one wavefront."""
         import json as _json
@@ -286,7 +288,8 @@ class Scene:
             arr[i].seed = int(j.get("seed", 0)) & 0xFFFFFFFF
         total = sum(h * w for h, w in shapes)
         out = np.empty(total * 3, np.float64)
-        d = self._desc(None, None, 0, 0, queue_capacity, grid_trace, grid_shade, use_graph, profile, trace_block)
+        d = self._desc(None, None, 0, 0, queue_capacity, grid_trace, grid_shade, use_graph, profile, trace_block,
+                       fetch_threshold=fetch_threshold)
         _check(load_library().wr_render_batch(self._h, arr, n, ctypes.byref(d), _ptr(out)))
         imgs, off = [], 0
         for h, w in shapes:

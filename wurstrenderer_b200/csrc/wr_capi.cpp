@@ -507,6 +507,9 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     r.guide = po.guide;
     r.record = po.record ? 1 : 0;
     r.guide_sms = sms;
+    if (desc.fetch_threshold < 0 || desc.fetch_threshold > 32)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "fetch_threshold must be 0..32");
+    r.fetch_min = desc.fetch_threshold > 0 ? desc.fetch_threshold : 20;
     r.num_jobs = int(table.size());
     r.job0 = table[0];
     if (table.size() > 1) {
@@ -1236,6 +1239,13 @@ int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_rende
         for (double f : {0.5, 1.0}) {
             wr_render_desc d = cur;
             d.grid_shade = std::max(sms, int(occ_s * f));
+            const double t = trial(d);
+            if (t < bt) { bt = t; cur = d; }
+        }
+        // 4) dynamic ray fetching threshold
+        for (int th : {12, 16, 24, 28}) {
+            wr_render_desc d = cur;
+            d.fetch_threshold = th;
             const double t = trial(d);
             if (t < bt) { bt = t; cur = d; }
         }

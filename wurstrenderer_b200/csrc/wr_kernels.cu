@@ -310,6 +310,7 @@ struct WaveArgs {
     float4 *records;       // training records (kRecordFloat4 float4 each), nullptr: not collected
     uint32_t *rec_count;
     uint32_t rec_capacity;
+    int fetch_min;         // traversal: refill idle lanes when fewer lanes than this still traverse
 };
 
 __device__ __forceinline__ const DevJob &job_at(const WaveArgs &w, uint32_t j) { return w.jobs ? w.jobs[j] : w.job0; }
@@ -369,14 +370,13 @@ __device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c)
 }
 
 // Persistent traversal of a ray queue with dynamic ray fetching: every lane keeps one ray
-// in flight; a warp whose traversing lanes drop below kFetchThreshold leaves the traversal
+// in flight; a warp whose traversing lanes drop below w.fetch_min leaves the traversal
 // loop and its idle lanes take the next rays of the queue (one atomic per warp), so that
 // SIMD lanes are not left idle while a few long rays finish (Aila & Laine, HPG 2009). Once
 // the queue is exhausted the remaining rays run to completion.
 //   SHADOW = false: extend -- closest hit of every live path into the hit records
 //   SHADOW = true:  shadow -- any hit of every queued shadow ray; unoccluded contributions
 //                   are added to the FP64 film (and to the path's training records)
-constexpr int kFetchThreshold = 20;
 
 template <int BLOCK, bool SHADOW>
 __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w, uint32_t *stack) {
@@ -416,7 +416,7 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
             }
         }
         if (!__any_sync(0xffffffffu, busy)) break;
-        const int min_active = __any_sync(0xffffffffu, exhausted) ? 0 : kFetchThreshold;
+        const int min_active = __any_sync(0xffffffffu, exhausted) ? 0 : w.fetch_min;
         if (busy && traverse_steps<SHADOW>(s.nodes, s.tris, r, kRayEps, t, tri, bu, bv, node, leaf, st, nv, nt,
                                            min_active)) {
             busy = false;
@@ -1056,6 +1056,7 @@ static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &
     w.records = r.record ? b.records : nullptr;
     w.rec_count = b.rec_count;
     w.rec_capacity = b.rec_capacity;
+    w.fetch_min = (r.fetch_min >= 1 && r.fetch_min <= 32) ? r.fetch_min : 20;
     return w;
 }
 

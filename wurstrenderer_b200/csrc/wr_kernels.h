@@ -42,6 +42,7 @@ struct RenderLaunch {
     const wrg::GuideNet *guide; // learned proposal used by shade (nullptr: plain NEE+MIS)
     int record;                 // 1: collect training records
     int guide_sms;              // SM count (grid of the inference kernel)
+    int fetch_min;              // dynamic ray fetching threshold (lanes still traversing)
 };
 
 enum KernelId { KERNEL_EXTEND = 0, KERNEL_SHADE = 1, KERNEL_RAYGEN = 2, KERNEL_SHADOW = 3, KERNEL_ADVANCE = 4,
