@@ -244,6 +244,13 @@ int wr_guide_train(wr_scene *scene, const float *records, int n, int steps, int 
  * (barycentric weights of vertices 1 and 2). uv may be NULL. */
 int wr_trace_closest(wr_scene *scene, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *uv);
 
+/* Closest hits with the unit geometry normal at the hit (n x 3 floats): the
+ * triangle's face normal, or on a Phong tessellation patch the patch normal
+ * (PhongMeshGeometry::intersect, src/geometry/phongmesh.h:178-368, reported to the
+ * renderer as Embree's Ng, src/accel/embreeaccel.h:101-127,419-420). Rays, ids and t
+ * as wr_trace_closest. */
+int wr_trace_hits(wr_scene *scene, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *normal);
+
 /* Occlusion queries (EmbreeAccel::isIntersect, src/accel/embreeaccel.h:336-351). */
 int wr_trace_occluded(wr_scene *scene, const float *rays, int n, int *occluded);
 

@@ -51,6 +51,8 @@ def lib():
         L.oracle_trace_closest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_trace_occluded.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.oracle_trace_hits.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -114,6 +116,15 @@ class OracleScene:
         lib().oracle_trace_closest(self._h, _ptr(rays), n, _ptr(g), _ptr(p), _ptr(t), _ptr(uv))
         return g, p, t, uv
 
+    def trace_hits(self, rays: np.ndarray):
+        """rays: (n, 8) float32 -> geom, prim, t, Ng (n, 3) as Embree reports them to the reference."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        g = np.zeros(n, np.int32); p = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32); ng = np.zeros((n, 3), np.float32)
+        lib().oracle_trace_hits(self._h, _ptr(rays), n, _ptr(g), _ptr(p), _ptr(t), _ptr(ng))
+        return g, p, t, ng
+
     def trace_occluded(self, rays: np.ndarray):
         rays = np.ascontiguousarray(rays, np.float32)
         occ = np.zeros(rays.shape[0], np.int32)
@@ -149,6 +160,21 @@ def run_reference(json_path, out_pfm, spp=None, vertices=None, salt=0, crop=None
     if r.returncode != 0:
         raise RuntimeError("wurst_ref failed: " + r.stderr.strip())
     return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_reference_trace(json_path, rays, work_dir, timeout=None):
+    """Closest hits and occlusion of `rays` ((n, 8) float32) through the reference's EmbreeAccel
+    scene (``wurst_ref trace2``): geom, prim, t, Ng (n, 3), occluded."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    rp = os.path.join(work_dir, "trace2_rays.f32")
+    hp = os.path.join(work_dir, "trace2_hits.bin")
+    rays.tofile(rp)
+    r = subprocess.run([REF_BIN, "trace2", json_path, rp, hp], capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("wurst_ref trace2 failed: " + r.stderr.strip())
+    out = np.fromfile(hp, np.float32).reshape(-1, 8)
+    ids = out[:, :2].copy().view(np.int32)
+    return ids[:, 0], ids[:, 1], out[:, 2].copy(), out[:, 3:6].copy(), out[:, 6] > 0.5
 
 
 def read_pfm(path):

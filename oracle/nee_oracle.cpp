@@ -34,6 +34,7 @@
 #include <random>
 #include <thread>
 
+#include "oracle_phong.h"
 #include "oracle_raycast.h"
 #include "oracle_scene.h"
 
@@ -275,9 +276,10 @@ static Spectrum bsdf_sample(const Material &m, V3 *out, double *pdfW, V3 in, dou
 }
 
 // --------------------------------------------------------------- scene ----
-struct Geometry {               // one reference TriangleMeshGeometry
+struct Geometry {               // one reference TriangleMeshGeometry (or PhongMeshGeometry)
     std::vector<V3> pos;
     std::vector<int> tri;       // 3 per triangle
+    std::vector<phong::Patch> patches;   // Phong tessellation surfaces: one patch per triangle
     int material = -1;          // index into Scene::materials (surfaces)
     int light = -1;             // index into Scene::lights (emitters)
     int geom_id = -1;           // Embree geomID (attach order)
@@ -902,7 +904,8 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
     int next_geom_id = 0;
     if (root.has("meshes")) {
         for (const Json &mj : root.at("meshes").arr) {
-            ObjFile of = load_obj(dir + "/" + mj.get("path", std::string("")));
+            const bool phong_file = mj.getb("phong_tessellation", false);
+            ObjFile of = load_obj(dir + "/" + mj.get("path", std::string("")), phong_file);
             std::map<std::string, double> sigma;
             if (mj.has("oren_nayar_sigma"))
                 for (auto &kv : mj.at("oren_nayar_sigma").obj) sigma[kv.first] = kv.second.number();
@@ -957,6 +960,27 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
                 } else {
                     g.material = mat_index[om.material];
                     file_surfaces.push_back(gi);
+                    if (phong_file) {
+                        // PhongMeshGeometry from the Assimp mesh (simple2parser.h:41-52); normals as
+                        // AssimpInOut stores them (assimpio.h:211-223): zero when of ~zero length,
+                        // else normalised in FP64
+                        if (om.missing_normals)
+                            throw std::runtime_error("phong_tessellation mesh without per-vertex normals");
+                        std::vector<phong::D3> nrm(g.pos.size());
+                        for (size_t k = 0; k < nrm.size(); ++k) {
+                            const phong::D3 n = phong::d3(om.normals[3 * k], om.normals[3 * k + 1], om.normals[3 * k + 2]);
+                            nrm[k] = phong::is_approx_zero(phong::length(n)) ? phong::D3() : phong::normalize(n);
+                        }
+                        for (size_t t = 0; t < g.tri.size(); t += 3) {
+                            phong::Patch P;
+                            for (int c = 0; c < 3; ++c) {
+                                const V3 &q = g.pos[g.tri[t + c]];
+                                P.p[c] = phong::d3(q.x, q.y, q.z);
+                                P.n[c] = nrm[g.tri[t + c]];
+                            }
+                            g.patches.push_back(P);
+                        }
+                    }
                 }
                 s->geoms.push_back(std::move(g));
             }
@@ -968,10 +992,44 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
     s->surface_of_geom.assign(next_geom_id, -1);
     for (size_t gi = 0; gi < s->geoms.size(); ++gi) s->surface_of_geom[s->geoms[gi].geom_id] = int(gi);
     for (int id = 0; id < next_geom_id; ++id) {
-        const Geometry &g = s->geoms[s->surface_of_geom[id]];
+        const int gi = s->surface_of_geom[id];
+        const Geometry &g = s->geoms[gi];
+        if (!g.patches.empty()) {
+            // user geometry: Embree keeps the float-rounded patch bounds (embreeaccel.h:63-75)
+            for (size_t t = 0; t < g.patches.size(); ++t) {
+                double lo[3], hi[3];
+                phong::bound(g.patches[t], lo, hi);
+                RcUser u;
+                for (int k = 0; k < 3; ++k) { u.lo[k] = float(lo[k]); u.hi[k] = float(hi[k]); }
+                u.geom = id;
+                u.prim = int(t);
+                u.ref = gi;
+                s->rc.add_user(u);
+            }
+            continue;
+        }
         std::vector<float> pf(g.pos.size() * 3);
         for (size_t k = 0; k < g.pos.size(); ++k) { pf[3 * k] = float(g.pos[k].x); pf[3 * k + 1] = float(g.pos[k].y); pf[3 * k + 2] = float(g.pos[k].z); }
         s->rc.add_mesh(pf.data(), g.tri.data(), int(g.tri.size() / 3), id);
+    }
+    {
+        // the user intersect / occluded callbacks (embreeaccel.h:77-180) around PhongMeshGeometry::intersect
+        const Scene *sc = s.get();
+        s->rc.user_closest = [sc](const RcUser &u, const float o[3], const float d[3], float tnear, float tfar, RcHit *h) {
+            double tmax = tfar;
+            phong::D3 n;
+            if (!phong::intersect(sc->geoms[u.ref].patches[u.prim], o, d, tnear, &tmax, &n)) return false;
+            h->t = float(tmax);
+            h->u = 0.f; h->v = 0.f;   // the patch leaves the texture coordinate at zero
+            h->ng[0] = float(n.x); h->ng[1] = float(n.y); h->ng[2] = float(n.z);
+            h->geom = u.geom; h->prim = u.prim;
+            return true;
+        };
+        s->rc.user_any = [sc](const RcUser &u, const float o[3], const float d[3], float tnear, float tfar) {
+            double tmax = tfar;
+            phong::D3 n;
+            return phong::intersect(sc->geoms[u.ref].patches[u.prim], o, d, tnear, &tmax, &n);
+        };
     }
     s->rc.build();
     if (s->env) {   // Scene ctor: envmap->updateSceneRadius(bounding sphere of the accel)
@@ -1119,7 +1177,7 @@ void oracle_scene_info(void *sp, int *info4, double *bbox6, int *counts3) {
     auto *s = static_cast<oracle::Scene *>(sp);
     info4[0] = s->cam.W; info4[1] = s->cam.H; info4[2] = s->spp; info4[3] = s->nverts;
     for (int k = 0; k < 3; ++k) { bbox6[k] = s->rc.scene_lo[k]; bbox6[3 + k] = s->rc.scene_hi[k]; }
-    counts3[0] = int(s->rc.tris.size()); counts3[1] = int(s->geoms.size()); counts3[2] = int(s->lights.size());
+    counts3[0] = int(s->rc.tris.size() + s->rc.users.size()); counts3[1] = int(s->geoms.size()); counts3[2] = int(s->lights.size());
 }
 
 // Overrides the camera with a simple2 camera JSON object (used for batched jobs).
@@ -1154,6 +1212,21 @@ void oracle_trace_closest(void *sp, const float *rays, int n, int *geom_id, int 
         prim_id[i] = hit ? h.prim : -1;
         t[i] = hit ? h.t : INFINITY;
         uv[2 * i] = h.u; uv[2 * i + 1] = h.v;
+    }
+}
+
+// Closest hits with the hit's geometry normal as the reference receives it from Embree
+// (Ng: unnormalised for triangles, the float-rounded unit patch normal for Phong patches).
+void oracle_trace_hits(void *sp, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *ng) {
+    auto *s = static_cast<oracle::Scene *>(sp);
+    for (int i = 0; i < n; ++i) {
+        const float *r = rays + 8 * size_t(i);
+        oracle::RcHit h;
+        const bool hit = s->rc.closest(r, r + 4, r[3], r[7], &h);
+        geom_id[i] = hit ? h.geom : -1;
+        prim_id[i] = hit ? h.prim : -1;
+        t[i] = hit ? h.t : INFINITY;
+        for (int k = 0; k < 3; ++k) ng[3 * i + k] = hit ? h.ng[k] : 0.f;
     }
 }
 

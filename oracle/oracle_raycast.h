@@ -18,12 +18,19 @@
 // The acceleration structure is a plain binary BVH (binned SAH, <= 4
 // triangles per leaf) built on the host: it changes only the speed of the
 // query, never its result (other than which of two exactly tied hits wins).
+//
+// User primitives (Embree's RTC_GEOMETRY_TYPE_USER, which the reference uses for
+// Phong tessellation patches, src/accel/embreeaccel.h:242-257) are held as float
+// boxes in a second BVH; a ray that enters a primitive's box calls the owner's
+// test with the closest distance found so far as its far limit, as Embree calls
+// the user intersect / occluded function.
 #pragma once
 
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 namespace oracle {
@@ -44,10 +51,33 @@ struct RcHit {
     int geom = -1, prim = -1;
 };
 
+struct RcUser {          // a user primitive: its float box and the owner's handle
+    float lo[3], hi[3];
+    int geom, prim;
+    int ref;             // index into the owner's primitive store
+};
+
+// closest: on a hit with t <= tfar fills *hit (t, ng, u, v, geom, prim) and returns true
+using RcUserClosest = std::function<bool(const RcUser &, const float o[3], const float d[3], float tnear, float tfar, RcHit *hit)>;
+// any hit in [tnear, tfar]
+using RcUserAny = std::function<bool(const RcUser &, const float o[3], const float d[3], float tnear, float tfar)>;
+
 struct RayCaster {
     std::vector<RcTri> tris;
     std::vector<RcNode> nodes;
+    std::vector<RcUser> users;
+    std::vector<RcNode> unodes;
+    RcUserClosest user_closest;
+    RcUserAny user_any;
     float scene_lo[3] = {INFINITY, INFINITY, INFINITY}, scene_hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+
+    void add_user(const RcUser &u) {
+        users.push_back(u);
+        for (int k = 0; k < 3; ++k) {
+            scene_lo[k] = std::min(scene_lo[k], u.lo[k]);
+            scene_hi[k] = std::max(scene_hi[k], u.hi[k]);
+        }
+    }
 
     // positions: float xyz per vertex; triangles: 3 indices per triangle
     void add_mesh(const float *positions, const int *triangles, int ntri, int geom_id) {
@@ -84,15 +114,38 @@ struct RayCaster {
     }
 
     void build() {
-        nodes.clear();
-        const int n = int(tris.size());
-        if (n == 0) return;
-        std::vector<float> clo(3 * size_t(n)), chi(3 * size_t(n)), cen(3 * size_t(n));
-        for (int i = 0; i < n; ++i) {
-            tri_bounds(tris[i], &clo[3 * i], &chi[3 * i]);
-            for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5f * (clo[3 * i + k] + chi[3 * i + k]);
+        {
+            const int n = int(tris.size());
+            std::vector<float> clo(3 * size_t(n)), chi(3 * size_t(n));
+            for (int i = 0; i < n; ++i) tri_bounds(tris[i], &clo[3 * i], &chi[3 * i]);
+            std::vector<int> idx;
+            build_nodes(clo, chi, n, nodes, idx);
+            std::vector<RcTri> sorted(n);
+            for (int i = 0; i < n; ++i) sorted[i] = tris[idx[i]];
+            tris.swap(sorted);
         }
-        std::vector<int> idx(n);
+        {
+            const int n = int(users.size());
+            std::vector<float> clo(3 * size_t(n)), chi(3 * size_t(n));
+            for (int i = 0; i < n; ++i)
+                for (int k = 0; k < 3; ++k) { clo[3 * i + k] = users[i].lo[k]; chi[3 * i + k] = users[i].hi[k]; }
+            std::vector<int> idx;
+            build_nodes(clo, chi, n, unodes, idx);
+            std::vector<RcUser> sorted(n);
+            for (int i = 0; i < n; ++i) sorted[i] = users[idx[i]];
+            users.swap(sorted);
+        }
+    }
+
+    // binned-SAH BVH over n boxes; idx receives the leaf order of the boxes
+    static void build_nodes(const std::vector<float> &clo, const std::vector<float> &chi, int n,
+                            std::vector<RcNode> &nodes, std::vector<int> &idx) {
+        nodes.clear();
+        idx.assign(n, 0);
+        if (n == 0) return;
+        std::vector<float> cen(3 * size_t(n));
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5f * (clo[3 * i + k] + chi[3 * i + k]);
         for (int i = 0; i < n; ++i) idx[i] = i;
         nodes.reserve(2 * size_t(n) / 2 + 1);
         struct Job { int node, first, count; };
@@ -183,9 +236,6 @@ struct RayCaster {
             stack.push_back({nd.left, j.first, nl});
             stack.push_back({nd.right, j.first + nl, j.count - nl});
         }
-        std::vector<RcTri> sorted(n);
-        for (int i = 0; i < n; ++i) sorted[i] = tris[idx[i]];
-        tris.swap(sorted);
     }
 
     // Moeller-Trumbore as in triangle_intersector_moeller.h:78-111.
@@ -218,7 +268,44 @@ struct RayCaster {
         return t0 <= t1 * 1.0000005f + 1e-30f;
     }
 
+    static inline bool user_box_hit(const RcUser &u, const float o[3], const float inv[3], float tnear, float tfar) {
+        RcNode nd;
+        for (int k = 0; k < 3; ++k) { nd.lo[k] = u.lo[k]; nd.hi[k] = u.hi[k]; }
+        float te;
+        return box_hit(nd, o, inv, tnear, tfar, &te);
+    }
+
     bool closest(const float o[3], const float d[3], float tnear, float tfar, RcHit *hit) const {
+        bool found = closest_tris(o, d, tnear, tfar, hit);
+        if (found) tfar = hit->t;
+        if (unodes.empty() || !user_closest) return found;
+        float inv[3];
+        for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];
+        int stack[128]; int sp = 0;
+        stack[sp++] = 0;
+        while (sp) {
+            const RcNode &nd = unodes[stack[--sp]];
+            float te;
+            if (!box_hit(nd, o, inv, tnear, tfar, &te)) continue;
+            if (nd.left < 0) {
+                for (int i = nd.first; i < nd.first + nd.count; ++i) {
+                    if (!user_box_hit(users[i], o, inv, tnear, tfar)) continue;
+                    RcHit h;
+                    if (user_closest(users[i], o, d, tnear, tfar, &h)) {
+                        *hit = h;
+                        tfar = h.t;
+                        found = true;
+                    }
+                }
+            } else {
+                stack[sp++] = nd.right;
+                stack[sp++] = nd.left;
+            }
+        }
+        return found;
+    }
+
+    bool closest_tris(const float o[3], const float d[3], float tnear, float tfar, RcHit *hit) const {
         if (nodes.empty()) return false;
         float inv[3];
         for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];
@@ -258,6 +345,28 @@ struct RayCaster {
     }
 
     bool occluded(const float o[3], const float d[3], float tnear, float tfar) const {
+        if (occluded_tris(o, d, tnear, tfar)) return true;
+        if (unodes.empty() || !user_any) return false;
+        float inv[3];
+        for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];
+        int stack[128]; int sp = 0;
+        stack[sp++] = 0;
+        while (sp) {
+            const RcNode &nd = unodes[stack[--sp]];
+            float te;
+            if (!box_hit(nd, o, inv, tnear, tfar, &te)) continue;
+            if (nd.left < 0) {
+                for (int i = nd.first; i < nd.first + nd.count; ++i)
+                    if (user_box_hit(users[i], o, inv, tnear, tfar) && user_any(users[i], o, d, tnear, tfar)) return true;
+            } else {
+                stack[sp++] = nd.right;
+                stack[sp++] = nd.left;
+            }
+        }
+        return false;
+    }
+
+    bool occluded_tris(const float o[3], const float d[3], float tnear, float tfar) const {
         if (nodes.empty()) return false;
         float inv[3];
         for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];

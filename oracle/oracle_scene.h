@@ -143,6 +143,10 @@ struct ObjMesh {
     int material = 0;                   // index into ObjFile::materials
     std::vector<float> positions;       // 3 floats per vertex (local to the mesh)
     std::vector<int> triangles;         // 3 local indices per triangle
+    // with load_obj(path, true): one vertex per distinct (position, normal) pair and the `vn`
+    // normal of each vertex as read (zero where a face corner has none)
+    std::vector<float> normals;
+    bool missing_normals = false;       // some face corner has no `vn`
 };
 
 struct ObjFile {
@@ -174,7 +178,9 @@ inline void load_mtl(const std::string &path, ObjFile &of, std::map<std::string,
     }
 }
 
-inline ObjFile load_obj(const std::string &path) {
+// `pairs`: key vertices by (position, normal) pair, as Assimp's JoinIdenticalVertices does
+// for meshes that carry normals (the Phong tessellation input); otherwise by position.
+inline ObjFile load_obj(const std::string &path, bool pairs = false) {
     std::ifstream f(path);
     if (!f) throw std::runtime_error("cannot open file " + path);
     ObjFile of;
@@ -182,10 +188,10 @@ inline ObjFile load_obj(const std::string &path) {
     of.materials[0].name = "DefaultMaterial";
     std::map<std::string, int> byname;
     byname["DefaultMaterial"] = 0;
-    std::vector<float> v;              // global vertex list
+    std::vector<float> v, vn;          // global vertex and normal lists
     int cur_mat = 0;
     ObjMesh *mesh = nullptr;
-    std::map<int, int> remap;          // global -> local vertex index of the current mesh
+    std::map<std::pair<int, int>, int> remap;   // global (vertex, normal) -> local index of the current mesh
     auto new_mesh = [&](const std::string &name) {
         of.meshes.push_back(ObjMesh());
         of.meshes.back().name = name;
@@ -200,6 +206,9 @@ inline ObjFile load_obj(const std::string &path) {
         if (s[0] == 'v' && (s[1] == ' ' || s[1] == '\t')) {
             char *end = const_cast<char *>(s + 1);
             for (int i = 0; i < 3; ++i) v.push_back(strtof(end, &end));
+        } else if (s[0] == 'v' && s[1] == 'n' && (s[2] == ' ' || s[2] == '\t')) {
+            char *end = const_cast<char *>(s + 2);
+            for (int i = 0; i < 3; ++i) vn.push_back(strtof(end, &end));
         } else if ((s[0] == 'o' || s[0] == 'g') && (s[1] == ' ' || s[1] == '\t')) {
             std::string name(s + 2);
             new_mesh(name);
@@ -226,17 +235,32 @@ inline ObjFile load_obj(const std::string &path) {
             std::istringstream ls(s + 1);
             std::string tok;
             std::vector<int> poly;
-            const int nv = int(v.size() / 3);
+            const int nv = int(v.size() / 3), nn = int(vn.size() / 3);
             while (ls >> tok) {
                 int gi = atoi(tok.c_str());
                 gi = gi < 0 ? nv + gi : gi - 1;
                 if (gi < 0 || gi >= nv) throw std::runtime_error("obj: bad vertex index");
-                auto it = remap.find(gi);
+                int ni = -1;   // v, v/vt, v//vn, v/vt/vn
+                const size_t s1 = tok.find('/');
+                if (s1 != std::string::npos) {
+                    const size_t s2 = tok.find('/', s1 + 1);
+                    if (s2 != std::string::npos && s2 + 1 < tok.size()) {
+                        ni = atoi(tok.c_str() + s2 + 1);
+                        ni = ni < 0 ? nn + ni : ni - 1;
+                        if (ni < 0 || ni >= nn) throw std::runtime_error("obj: bad normal index");
+                    }
+                }
+                const std::pair<int, int> key(gi, pairs ? ni : -1);
+                auto it = remap.find(key);
                 int li;
                 if (it == remap.end()) {
                     li = int(mesh->positions.size() / 3);
-                    remap[gi] = li;
+                    remap[key] = li;
                     for (int k = 0; k < 3; ++k) mesh->positions.push_back(v[3 * gi + k]);
+                    if (pairs) {
+                        for (int k = 0; k < 3; ++k) mesh->normals.push_back(ni >= 0 ? vn[3 * ni + k] : 0.f);
+                        if (ni < 0) mesh->missing_normals = true;
+                    }
                 } else li = it->second;
                 poly.push_back(li);
             }

@@ -9,8 +9,15 @@
 // queries with the oracle's restatement of Embree's triangle test
 // (oracle/oracle_raycast.h). Alpha filter callbacks are not invoked: the
 // scenes carry no alpha textures, for which the reference's filters
-// (embreeaccel.h:182-220) accept every hit. User geometries (phong
-// tessellation, analytic cubes and planes) are out of scope and rejected.
+// (embreeaccel.h:182-220) accept every hit.
+//
+// User geometries (RTC_GEOMETRY_TYPE_USER; the reference's Phong tessellation
+// patches, embreeaccel.h:242-257) are supported as Embree 3 runs them: the
+// bounds callback is asked once per primitive at commit, the boxes go into the
+// caster's user-primitive BVH, and a ray that reaches a primitive's box calls the
+// geometry's intersect (occluded) callback with the ray's current tfar, through
+// the same argument structs Embree passes. rtcFilterIntersection /
+// rtcFilterOcclusion do nothing: the reference sets no filter on user geometry.
 
 #include <cmath>
 #include <cstdio>
@@ -27,12 +34,21 @@ struct ShimGeometry {
     std::vector<float> attribs;      // float2 texture coordinates
     unsigned geom_id = RTC_INVALID_GEOMETRY_ID;
     int refs = 1;
+    // user geometry
+    void *user_data = nullptr;
+    unsigned prim_count = 0;
+    RTCBoundsFunction bounds = nullptr;
+    RTCIntersectFunctionN intersect = nullptr;
+    RTCOccludedFunctionN occluded = nullptr;
 };
 
 struct ShimScene {
     std::vector<ShimGeometry *> geoms;
     oracle::RayCaster rc;
 };
+
+// the context of the query in flight on this thread (the callbacks read it)
+static thread_local RTCIntersectContext *g_context = nullptr;
 
 struct ShimDevice { RTCErrorFunction err = nullptr; void *user = nullptr; };
 
@@ -62,7 +78,6 @@ RTCGeometry rtcNewGeometry(RTCDevice, enum RTCGeometryType type) {
 unsigned int rtcAttachGeometry(RTCScene s, RTCGeometry g) {
     ShimScene *sc = reinterpret_cast<ShimScene *>(s);
     ShimGeometry *sg = reinterpret_cast<ShimGeometry *>(g);
-    if (sg->type != RTC_GEOMETRY_TYPE_TRIANGLE) shim_fail("user geometry");
     sg->geom_id = unsigned(sc->geoms.size());
     sg->refs++;
     sc->geoms.push_back(sg);
@@ -94,15 +109,19 @@ void *rtcSetNewGeometryBuffer(RTCGeometry g, enum RTCBufferType type, unsigned i
 }
 
 void rtcSetGeometryVertexAttributeCount(RTCGeometry, unsigned int) {}
-void rtcSetGeometryUserData(RTCGeometry, void *) {}
+void rtcSetGeometryUserData(RTCGeometry g, void *ptr) { reinterpret_cast<ShimGeometry *>(g)->user_data = ptr; }
 void rtcSetGeometryIntersectFilterFunction(RTCGeometry, RTCFilterFunctionN) {}
 void rtcSetGeometryOccludedFilterFunction(RTCGeometry, RTCFilterFunctionN) {}
-void rtcSetGeometryUserPrimitiveCount(RTCGeometry, unsigned int) { shim_fail("rtcSetGeometryUserPrimitiveCount"); }
-void rtcSetGeometryBoundsFunction(RTCGeometry, RTCBoundsFunction, void *) { shim_fail("rtcSetGeometryBoundsFunction"); }
-void rtcSetGeometryIntersectFunction(RTCGeometry, RTCIntersectFunctionN) { shim_fail("rtcSetGeometryIntersectFunction"); }
-void rtcSetGeometryOccludedFunction(RTCGeometry, RTCOccludedFunctionN) { shim_fail("rtcSetGeometryOccludedFunction"); }
-void rtcFilterIntersection(const RTCIntersectFunctionNArguments *, const RTCFilterFunctionNArguments *) { shim_fail("rtcFilterIntersection"); }
-void rtcFilterOcclusion(const RTCOccludedFunctionNArguments *, const RTCFilterFunctionNArguments *) { shim_fail("rtcFilterOcclusion"); }
+void rtcSetGeometryUserPrimitiveCount(RTCGeometry g, unsigned int n) {
+    ShimGeometry *sg = reinterpret_cast<ShimGeometry *>(g);
+    if (sg->type != RTC_GEOMETRY_TYPE_USER) shim_fail("rtcSetGeometryUserPrimitiveCount on a non-user geometry");
+    sg->prim_count = n;
+}
+void rtcSetGeometryBoundsFunction(RTCGeometry g, RTCBoundsFunction f, void *) { reinterpret_cast<ShimGeometry *>(g)->bounds = f; }
+void rtcSetGeometryIntersectFunction(RTCGeometry g, RTCIntersectFunctionN f) { reinterpret_cast<ShimGeometry *>(g)->intersect = f; }
+void rtcSetGeometryOccludedFunction(RTCGeometry g, RTCOccludedFunctionN f) { reinterpret_cast<ShimGeometry *>(g)->occluded = f; }
+void rtcFilterIntersection(const RTCIntersectFunctionNArguments *, const RTCFilterFunctionNArguments *) {}
+void rtcFilterOcclusion(const RTCOccludedFunctionNArguments *, const RTCFilterFunctionNArguments *) {}
 void rtcCommitGeometry(RTCGeometry) {}
 
 void rtcReleaseGeometry(RTCGeometry g) {
@@ -114,9 +133,74 @@ void rtcCommitScene(RTCScene s) {
     ShimScene *sc = reinterpret_cast<ShimScene *>(s);
     sc->rc = oracle::RayCaster();
     for (ShimGeometry *g : sc->geoms) {
+        if (g->type == RTC_GEOMETRY_TYPE_USER) {
+            if (!g->bounds || !g->intersect || !g->occluded) shim_fail("user geometry without callbacks");
+            for (unsigned p = 0; p < g->prim_count; ++p) {
+                RTCBounds b;
+                RTCBoundsFunctionArguments a;
+                a.geometryUserPtr = g->user_data;
+                a.primID = p;
+                a.timeStep = 0;
+                a.bounds_o = &b;
+                g->bounds(&a);
+                oracle::RcUser u;
+                u.lo[0] = b.lower_x; u.lo[1] = b.lower_y; u.lo[2] = b.lower_z;
+                u.hi[0] = b.upper_x; u.hi[1] = b.upper_y; u.hi[2] = b.upper_z;
+                u.geom = int(g->geom_id);
+                u.prim = int(p);
+                u.ref = int(g->geom_id);
+                sc->rc.add_user(u);
+            }
+            continue;
+        }
         std::vector<int> tri(g->indices.begin(), g->indices.end());
         sc->rc.add_mesh(g->vertices.data(), tri.data(), int(tri.size() / 3), int(g->geom_id));
     }
+    sc->rc.user_closest = [sc](const oracle::RcUser &u, const float o[3], const float d[3], float tnear, float tfar,
+                               oracle::RcHit *h) {
+        ShimGeometry *g = sc->geoms[size_t(u.ref)];
+        RTCRayHit rh;
+        rh.ray.org_x = o[0]; rh.ray.org_y = o[1]; rh.ray.org_z = o[2];
+        rh.ray.dir_x = d[0]; rh.ray.dir_y = d[1]; rh.ray.dir_z = d[2];
+        rh.ray.tnear = tnear; rh.ray.tfar = tfar;
+        rh.ray.time = 0.f; rh.ray.mask = ~0u; rh.ray.id = 0; rh.ray.flags = 0;
+        rh.hit.geomID = RTC_INVALID_GEOMETRY_ID;
+        rh.hit.primID = RTC_INVALID_GEOMETRY_ID;
+        int valid = -1;
+        RTCIntersectFunctionNArguments a;
+        a.valid = &valid;
+        a.geometryUserPtr = g->user_data;
+        a.primID = unsigned(u.prim);
+        a.context = g_context;
+        a.rayhit = reinterpret_cast<RTCRayHitN *>(&rh);
+        a.N = 1;
+        g->intersect(&a);
+        if (rh.hit.geomID == RTC_INVALID_GEOMETRY_ID) return false;
+        h->t = rh.ray.tfar;
+        h->u = rh.hit.u; h->v = rh.hit.v;
+        h->ng[0] = rh.hit.Ng_x; h->ng[1] = rh.hit.Ng_y; h->ng[2] = rh.hit.Ng_z;
+        h->geom = int(rh.hit.geomID);
+        h->prim = int(rh.hit.primID);
+        return true;
+    };
+    sc->rc.user_any = [sc](const oracle::RcUser &u, const float o[3], const float d[3], float tnear, float tfar) {
+        ShimGeometry *g = sc->geoms[size_t(u.ref)];
+        RTCRay r;
+        r.org_x = o[0]; r.org_y = o[1]; r.org_z = o[2];
+        r.dir_x = d[0]; r.dir_y = d[1]; r.dir_z = d[2];
+        r.tnear = tnear; r.tfar = tfar;
+        r.time = 0.f; r.mask = ~0u; r.id = 0; r.flags = 0;
+        int valid = -1;
+        RTCOccludedFunctionNArguments a;
+        a.valid = &valid;
+        a.geometryUserPtr = g->user_data;
+        a.primID = unsigned(u.prim);
+        a.context = g_context;
+        a.ray = reinterpret_cast<RTCRayN *>(&r);
+        a.N = 1;
+        g->occluded(&a);
+        return r.tfar == -INFINITY;
+    };
     sc->rc.build();
 }
 
@@ -127,8 +211,9 @@ void rtcGetSceneBounds(RTCScene s, struct RTCBounds *b) {
     b->align0 = b->align1 = 0.f;
 }
 
-void rtcIntersect1(RTCScene s, struct RTCIntersectContext *, struct RTCRayHit *rh) {
+void rtcIntersect1(RTCScene s, struct RTCIntersectContext *ctx, struct RTCRayHit *rh) {
     ShimScene *sc = reinterpret_cast<ShimScene *>(s);
+    g_context = ctx;
     const float o[3] = {rh->ray.org_x, rh->ray.org_y, rh->ray.org_z};
     const float d[3] = {rh->ray.dir_x, rh->ray.dir_y, rh->ray.dir_z};
     oracle::RcHit h;
@@ -142,8 +227,9 @@ void rtcIntersect1(RTCScene s, struct RTCIntersectContext *, struct RTCRayHit *r
     }
 }
 
-void rtcOccluded1(RTCScene s, struct RTCIntersectContext *, struct RTCRay *r) {
+void rtcOccluded1(RTCScene s, struct RTCIntersectContext *ctx, struct RTCRay *r) {
     ShimScene *sc = reinterpret_cast<ShimScene *>(s);
+    g_context = ctx;
     const float o[3] = {r->org_x, r->org_y, r->org_z};
     const float d[3] = {r->dir_x, r->dir_y, r->dir_z};
     if (sc->rc.occluded(o, d, r->tnear, r->tfar)) r->tfar = -INFINITY;

@@ -18,6 +18,7 @@
 //   wurst_ref render <scene.json> <out.pfm> [--spp N] [--vertices V] [--salt S]
 //            [--crop x0 y0 x1 y1] [--serial] [--threads T] [--raw out.f64] [--camera '<json>']
 //   wurst_ref trace <scene.json> <rays.f32> <hits.bin>
+//   wurst_ref trace2 <scene.json> <rays.f32> <hits.bin>   (any geometry type; 8 words per ray)
 // `render` without --crop/--serial calls PathNeeRenderer::render() itself
 // (all hardware threads). --serial/--crop run the same per-tile loop as
 // render() (pathnextevent.h:152-191) over the selected tiles on --threads
@@ -35,6 +36,7 @@
 #include "bsdf/phong.h"
 #include "bsdf/mixed.h"
 #include "bsdf/twosided.h"
+#include "geometry/phongmesh.h"
 #include "light/diffusearealight.h"
 #include "light/envmap.h"
 #include "sphericalrepresentation/equirectangular.h"
@@ -70,7 +72,8 @@ shared_ptr<const Scene> parse_scene(const json &meshesJson, const shared_ptr<Env
     std::vector<shared_ptr<const Geometry>> geometries, lightGeometries;
     for (const json &mj : meshesJson) {
         const std::string rel = Util::Json::GetValue<std::string>(mj, "path", "");
-        oracle::ObjFile of = oracle::load_obj((dir / rel).string());
+        const bool doUsePhongTessellation = Util::Json::GetValue<bool>(mj, "phong_tessellation", false);
+        oracle::ObjFile of = oracle::load_obj((dir / rel).string(), doUsePhongTessellation);
         std::map<std::string, double> sigma;
         if (mj.find("oren_nayar_sigma") != mj.end())
             for (auto it = mj["oren_nayar_sigma"].begin(); it != mj["oren_nayar_sigma"].end(); ++it)
@@ -104,11 +107,18 @@ shared_ptr<const Scene> parse_scene(const json &meshesJson, const shared_ptr<Env
         }
         std::vector<shared_ptr<TriangleMeshGeometry>> geoms, lights;
         for (const oracle::ObjMesh &om : of.meshes) {
+            if (doUsePhongTessellation && om.missing_normals && areaLights[om.material] == nullptr)
+                throw std::runtime_error("phong_tessellation mesh without per-vertex normals");
             auto tm = make_shared<TriangleMeshGeometry>();
             const size_t nv = om.positions.size() / 3;
             for (size_t k = 0; k < nv; ++k) {
                 tm->mPositions.emplace_back(om.positions[3 * k], om.positions[3 * k + 1], om.positions[3 * k + 2]);
                 tm->mTextureCoords.emplace_back(0, 0);
+                if (!om.normals.empty()) {   // assimpio.h:211-223
+                    const float x = om.normals[3 * k], y = om.normals[3 * k + 1], z = om.normals[3 * k + 2];
+                    if (Math::IsApprox(Math::Length(Vec3(x, y, z)), 0.0)) tm->mNormals.emplace_back(Vec3(0.0, 0.0, 0.0));
+                    else tm->mNormals.emplace_back(Math::Normalize(Vec3(x, y, z)));
+                }
             }
             for (size_t t = 0; t < om.triangles.size(); t += 3)
                 tm->mTriangles.emplace_back(om.triangles[t], om.triangles[t + 1], om.triangles[t + 2]);
@@ -122,7 +132,24 @@ shared_ptr<const Scene> parse_scene(const json &meshesJson, const shared_ptr<Env
                 geoms.push_back(tm);
             }
         }
-        for (auto &p : geoms) accel->addGeometry(p);
+        // Simple2Parser::ParseScene (simple2parser.h:37-58): surfaces of a phong_tessellation
+        // entry become PhongMeshGeometry user geometry, emitters stay triangle meshes
+        for (auto &p : geoms) {
+            if (doUsePhongTessellation) {
+                shared_ptr<PhongMeshGeometry> q = make_shared<PhongMeshGeometry>();
+                std::swap(q->mPositions, p->mPositions);
+                std::swap(q->mNormals, p->mNormals);
+                std::swap(q->mTextureCoords, p->mTextureCoords);
+                std::swap(q->mTriangles, p->mTriangles);
+                q->mAlpha = p->mAlpha;
+                q->mBsdf = p->mBsdf;
+                q->mMediumBackface = p->mMediumBackface;
+                q->mMediumFrontface = p->mMediumFrontface;
+                accel->addUserGeometry(q);
+            } else {
+                accel->addGeometry(p);
+            }
+        }
         for (auto &p : lights) accel->addGeometry(p);
         geometries.insert(geometries.end(), geoms.begin(), geoms.end());
         lightGeometries.insert(lightGeometries.end(), lights.begin(), lights.end());
@@ -314,12 +341,57 @@ int cmd_trace(int argc, char **argv) {
     return 0;
 }
 
+// Closest hits through rtcIntersect1 on the accel's scene, for every geometry type (user
+// geometry included, which intersectTriangleInfo does not report): per ray geomID, primID,
+// tfar and the hit's Ng as the reference's intersect() reads them (embreeaccel.h:353-422).
+int cmd_trace2(int argc, char **argv) {
+    Loaded L = load(argv[2], "");
+    std::string bytes = oracle::read_file(argv[3]);
+    const size_t n = bytes.size() / 32;
+    const float *r = reinterpret_cast<const float *>(bytes.data());
+    std::vector<float> out(8 * n);
+    const EmbreeAccel &accel = *L.scene->mAccel;
+    for (size_t i = 0; i < n; ++i) {
+        const float *q = r + 8 * i;
+        RTCRayHit query;
+        query.ray.org_x = q[0]; query.ray.org_y = q[1]; query.ray.org_z = q[2]; query.ray.tnear = q[3];
+        query.ray.dir_x = q[4]; query.ray.dir_y = q[5]; query.ray.dir_z = q[6]; query.ray.tfar = q[7];
+        query.ray.time = 0.f;
+        query.hit.geomID = RTC_INVALID_GEOMETRY_ID;
+        query.hit.primID = RTC_INVALID_GEOMETRY_ID;
+        RTCIntersectContext ctx;
+        rtcInitIntersectContext(&ctx);
+        rtcIntersect1(accel.mRtcScene, &ctx, &query);
+        const bool hit = query.hit.geomID != RTC_INVALID_GEOMETRY_ID;
+        int32_t gid = hit ? int32_t(query.hit.geomID) : -1, pid = hit ? int32_t(query.hit.primID) : -1;
+        memcpy(&out[8 * i + 0], &gid, 4);
+        memcpy(&out[8 * i + 1], &pid, 4);
+        out[8 * i + 2] = hit ? query.ray.tfar : INFINITY;
+        out[8 * i + 3] = hit ? query.hit.Ng_x : 0.f;
+        out[8 * i + 4] = hit ? query.hit.Ng_y : 0.f;
+        out[8 * i + 5] = hit ? query.hit.Ng_z : 0.f;
+        RTCRay occ;
+        occ.org_x = q[0]; occ.org_y = q[1]; occ.org_z = q[2]; occ.tnear = q[3];
+        occ.dir_x = q[4]; occ.dir_y = q[5]; occ.dir_z = q[6]; occ.tfar = q[7];
+        occ.time = 0.f;
+        rtcOccluded1(accel.mRtcScene, &ctx, &occ);
+        out[8 * i + 6] = occ.tfar < 0.f ? 1.f : 0.f;
+        out[8 * i + 7] = 0.f;
+    }
+    FILE *f = fopen(argv[4], "wb");
+    fwrite(out.data(), 4, out.size(), f);
+    fclose(f);
+    printf("{\"rays\": %zu}\n", n);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
     try {
         if (argc >= 4 && std::string(argv[1]) == "render") return cmd_render(argc, argv);
         if (argc >= 5 && std::string(argv[1]) == "trace") return cmd_trace(argc, argv);
+        if (argc >= 5 && std::string(argv[1]) == "trace2") return cmd_trace2(argc, argv);
         fprintf(stderr, "usage: wurst_ref render <scene.json> <out.pfm> [options] | trace <scene.json> <rays> <hits>\n");
         return 2;
     } catch (const std::exception &e) {

@@ -10,6 +10,8 @@ oracle/ref/ref_harness.cpp). For each fixture scene it writes:
   <name>_ref_hi_a.npy/_b.npy   two independent reference renders at HI_SPP (float32)
   <name>_rays.npy              seeded ray batch (float32 n x 8)
   <name>_hits.npy              reference closest hits for the batch: geomID, primID, t bits (int32 n x 3)
+  <name>_hits_ng.npy           the same hits with Embree's Ng and the occlusion answer
+                               (float32 n x 5: t, Ng xyz, occluded), for every geometry type
 
 Usage: python tests/golden/make_golden.py [--hi-spp 4096]
 """
@@ -30,7 +32,8 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from wurstrenderer_b200 import scenes  # noqa: E402
 
-FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt", "cornell_ls", "hf_ls"]
+FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt", "cornell_ls", "hf_ls", "phong", "phong_pt",
+            "phong_ls"]
 
 
 def with_integrator(path, integrator):
@@ -60,6 +63,8 @@ def write_fixture_scene(name, out_dir):
                                                n_lights=4, light_ke=(30.0, 28.0, 25.0))
         cam = dict(scenes.HEIGHTFIELD_CAMERA, pos=[0.0, 2.2, 5.5])
         return scenes.write_spec(out_dir, "hf", spec, cam, (48, 24), 4, 12)
+    if name == "phong":   # Phong tessellation surfaces (a "phong_tessellation": true mesh entry)
+        return scenes.write_phong_cornell(out_dir, name="phong", resolution=(48, 48), spp=4, num_path_vertices=8)
     raise KeyError(name)
 
 
@@ -112,12 +117,15 @@ def main():
         rays_path = os.path.join(HERE, name + "_rays.npy")
         np.save(rays_path, rays)
         rays.tofile(os.path.join(sdir, "_rays.f32"))
-        subprocess.run([oracle.REF_BIN, "trace", path, os.path.join(sdir, "_rays.f32"),
-                        os.path.join(sdir, "_hits.bin")], check=True, capture_output=True)
-        hits = np.fromfile(os.path.join(sdir, "_hits.bin"), np.int32).reshape(-1, 4)[:, :3]
+        # rtcIntersect1 / rtcOccluded1 on the reference's accel (user geometry included)
+        g, p, t, ng, occ = oracle.run_reference_trace(path, rays, sdir)
+        hits = np.stack([g, p, t.view(np.int32)], 1).astype(np.int32)
         np.save(os.path.join(HERE, name + "_hits.npy"), hits)
-        for f in ("_tmp.pfm", "_tmp.f64", "_rays.f32", "_hits.bin"):
-            os.remove(os.path.join(sdir, f))
+        np.save(os.path.join(HERE, name + "_hits_ng.npy"),
+                np.concatenate([t[:, None], ng, occ[:, None].astype(np.float32)], 1).astype(np.float32))
+        for f in ("_tmp.pfm", "_tmp.f64", "_rays.f32", "trace2_rays.f32", "trace2_hits.bin"):
+            if os.path.exists(os.path.join(sdir, f)):
+                os.remove(os.path.join(sdir, f))
         with open(os.path.join(HERE, name + "_meta.json"), "w") as f:
             json.dump({"scene": os.path.relpath(path, HERE), "hi_spp": args.hi_spp, "salts": [11, 22],
                        "width": sc.width, "height": sc.height,

@@ -105,6 +105,31 @@ def test_obj_semantics(wr_lib, oracle_lib, tmp_path):
     assert (sc.num_triangles, sc.num_meshes, sc.num_lights) == (5, 4, 3)
 
 
+def test_phong_mesh_entries(wr_lib, oracle_lib, tmp_path):
+    """"phong_tessellation": true turns the entry's surfaces into patches with one vertex per
+    (position, normal) pair (v//vn, v/vt/vn and negative indices); its emitters stay triangles;
+    a patch corner without a normal is rejected."""
+    (tmp_path / "m.mtl").write_text("newmtl a\nKd 0.5 0.5 0.5\nnewmtl l\nKe 5 5 5\n")
+    (tmp_path / "m.obj").write_text(
+        "mtllib m.mtl\n"
+        "v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\n"
+        "vn 0 0 1\nvn 0.1 0 1\nvn 0 0.1 1\nvt 0 0\n"
+        "o smooth\nusemtl a\nf 1//1 2//2 3//3\nf 1/1/1 3/1/3 4/1/-3\n"
+        "o light\nusemtl l\nf 1 2 4\n")
+    scene = ('{"camera": {"pos": [0,0,5], "lookat": [0,0,0], "up": [0,1,0], "resolution": [8, 6]},'
+             ' "meshes": [{"path": "m.obj", "phong_tessellation": true}],'
+             ' "render": [{"integrator": "nextevent_path_tracer"}]}')
+    (tmp_path / "s.json").write_text(scene)
+    info = wr_lib.inspect_scene(str(tmp_path / "s.json"))
+    assert (info["num_triangles"], info["num_meshes"], info["num_lights"]) == (3, 2, 1)
+    sc = oracle_lib.OracleScene(str(tmp_path / "s.json"))
+    assert (sc.num_triangles, sc.num_meshes, sc.num_lights) == (3, 2, 1)
+    (tmp_path / "n.obj").write_text("v 0 0 0\nv 1 0 0\nv 1 1 0\nvn 0 0 1\nf 1//1 2 3//1\n")
+    (tmp_path / "n.json").write_text(scene.replace("m.obj", "n.obj"))
+    with pytest.raises(wr_lib.WurstError, match="vertex normal"):
+        wr_lib.inspect_scene(str(tmp_path / "n.json"))
+
+
 def test_cli_reports_errors(wr_lib, tmp_path):
     r = subprocess.run([wr_lib.CLI_PATH, "--simple2parse", str(tmp_path / "nope.json")], capture_output=True,
                        text=True, cwd=str(tmp_path))

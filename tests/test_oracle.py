@@ -41,6 +41,53 @@ def test_oracle_trace_matches_reference(oracle_lib, name):
     assert 0.2 < hit.mean() <= 1.0
 
 
+def test_oracle_patch_normals_and_occlusion_match_reference(oracle_lib):
+    """Phong tessellation patches: the oracle's FP64 restatement of PhongMeshGeometry gives the
+    reference's own Ng (the float-rounded unit patch normal) and occlusion answers bit for bit."""
+    path, _ = golden_scene("phong")
+    rays = np.load("%s/phong_rays.npy" % GOLDEN)
+    hng = np.load("%s/phong_hits_ng.npy" % GOLDEN)
+    sc = oracle_lib.OracleScene(path)
+    g, p, t, ng = sc.trace_hits(rays)
+    hit = g >= 0
+    assert np.array_equal(ng[hit], hng[hit, 1:4])
+    assert np.array_equal(t[hit], hng[hit, 0])
+    occ = sc.trace_occluded(rays)
+    assert np.array_equal(occ.astype(bool), hng[:, 4] > 0.5)
+
+
+def test_oracle_patch_bounds_contain_the_surface(oracle_lib):
+    """The patch bound (phongmesh.h:61-164) gates the patch test, so it must enclose the patch:
+    a short ray aimed along the interpolated normal at a point sampled on the Phong surface of
+    each patch of the fixture's objects hits it (the box could only cut such hits off)."""
+    from wurstrenderer_b200 import scenes
+    path, _ = golden_scene("phong")
+    sc = oracle_lib.OracleScene(path)
+    alpha = 0.75
+    rng = np.random.default_rng(9)
+    rays = []
+    for m in scenes.phong_objects_spec().meshes:
+        P = m.positions.astype(np.float64)
+        N = m.normals.astype(np.float64)
+        N /= np.linalg.norm(N, axis=1, keepdims=True)
+        for a, b, c in m.triangles:
+            for _ in range(2):
+                u, v = rng.uniform(0.02, 0.96, 2)
+                if u + v > 0.98:
+                    u, v = 1 - u, 1 - v
+                w = 1 - u - v
+                puv = u * P[a] + v * P[b] + w * P[c]
+                ps = sum(wt * (puv - np.dot(puv - P[i], N[i]) * N[i]) for wt, i in ((u, a), (v, b), (w, c)))
+                q = (1 - alpha) * puv + alpha * ps
+                nrm = u * N[a] + v * N[b] + w * N[c]
+                nrm /= np.linalg.norm(nrm)
+                rays.append([*(q + 0.05 * nrm), 0.0, *(-nrm), 0.1])
+    rays = np.asarray(rays, np.float32)
+    g, _, t, _ = sc.trace_closest(rays)
+    assert (g >= 0).mean() > 0.995
+    assert np.median(t[g >= 0]) == pytest.approx(0.05, rel=1e-3)
+
+
 @pytest.mark.parametrize("name", FIXTURES)
 def test_reference_noise_floor_is_small(name):
     a = np.load("%s/%s_ref_hi_a.npy" % (GOLDEN, name)).astype(np.float64)

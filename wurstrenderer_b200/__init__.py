@@ -89,7 +89,7 @@ BVH_DEVICE_LBVH = 1
 # every function the C ABI exports (include/wurst_b200.h)
 EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
-           "wr_trace_closest", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
+           "wr_trace_closest", "wr_trace_hits", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
            "wr_render_batch_device", "wr_autotune", "wr_guide_reset", "wr_guide_get_params", "wr_guide_set_params",
            "wr_guide_box", "wr_guide_eval", "wr_guide_gradient", "wr_guide_train"]
@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH):
     L.wr_render_batch_device.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), fp]
     L.wr_get_render_stats.argtypes = [vp, ctypes.POINTER(RenderStats)]
     L.wr_trace_closest.argtypes = [vp, fp, ip, fp, fp, fp, fp]
+    L.wr_trace_hits.argtypes = [vp, fp, ip, fp, fp, fp, fp]
     L.wr_trace_occluded.argtypes = [vp, fp, ip, fp]
     L.wr_trace_stats.argtypes = [vp, fp, ip, ip, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
     L.wr_write_pfm.argtypes = [cp, fp, ip, ip]
@@ -363,6 +364,15 @@ class Scene:
         t = np.empty(n, np.float32); uv = np.empty((n, 2), np.float32)
         _check(load_library().wr_trace_closest(self._h, _ptr(rays), n, _ptr(g), _ptr(p), _ptr(t), _ptr(uv)))
         return g, p, t, uv
+
+    def trace_hits(self, rays: np.ndarray):
+        """Closest hits with the unit geometry normal: (geom_id, prim_id, t, normal (n, 3))."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        g = np.empty(n, np.int32); p = np.empty(n, np.int32)
+        t = np.empty(n, np.float32); nrm = np.empty((n, 3), np.float32)
+        _check(load_library().wr_trace_hits(self._h, _ptr(rays), n, _ptr(g), _ptr(p), _ptr(t), _ptr(nrm)))
+        return g, p, t, nrm
 
     def trace_occluded(self, rays: np.ndarray):
         rays = np.ascontiguousarray(rays, np.float32)

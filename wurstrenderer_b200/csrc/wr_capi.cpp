@@ -25,6 +25,7 @@
 #include "wr_guide.h"
 #include "wr_host.h"
 #include "wr_kernels.h"
+#include "wr_phong.cuh"
 
 using wr::Error;
 
@@ -77,7 +78,8 @@ struct wr_scene {
     cudaStream_t stream = nullptr;
     int device = 0;
     // scene data
-    DevBuf nodes, tris, tri_mat, materials, lights, light_tris, light_tri_cdf, light_tri_pdf, light_cdf, light_pdf;
+    DevBuf nodes, tris, patches, tri_mat, materials, lights, light_tris, light_tri_cdf, light_tri_pdf, light_cdf, light_pdf;
+    uint32_t num_patches = 0;
     DevBuf env_texels, env_pixel_pdf, env_row_cdf, env_row_pdf, env_col_cdf, env_col_pdf;
     wrd::DevScene dev{};
     wr_scene_options opts{};
@@ -133,11 +135,24 @@ void build_device_scene(wr_scene &s) {
     const uint32_t ntri = uint32_t(ntri64);
     std::vector<float> verts(size_t(ntri) * 9);
     std::vector<uint32_t> tri_mesh(ntri), tri_prim(ntri), tri_code(ntri);
+    // Phong tessellation patches: FP64 unit normals and boxes per patch (global order)
+    std::vector<uint8_t> is_patch(ntri, 0);
+    std::vector<double> patch_n;          // 9 per triangle (only patches are filled)
+    std::vector<float> box_near, box_out; // 6 per triangle: the bound rounded to nearest / outward
+    uint32_t npatch = 0;
+    for (const wr::Mesh &m : h.meshes) if (m.phong) npatch += m.num_triangles();
+    if (npatch) {
+        patch_n.assign(size_t(ntri) * 9, 0.0);
+        box_near.assign(size_t(ntri) * 6, 0.f);
+        box_out.assign(size_t(ntri) * 6, 0.f);
+    }
     {
         size_t g = 0;
         for (size_t mi = 0; mi < h.meshes.size(); ++mi) {
             const wr::Mesh &m = h.meshes[mi];
             const uint32_t code = m.light >= 0 ? (wrd::LIGHT_BIT | uint32_t(m.light)) : uint32_t(m.material);
+            if (m.phong && m.normals.size() != m.positions.size())
+                throw Error(WR_ERR_PARSE, "phong mesh '" + m.name + "' needs one normal per vertex");
             for (uint32_t t = 0; t < m.num_triangles(); ++t, ++g) {
                 for (int c = 0; c < 3; ++c) {
                     const uint32_t vi = m.indices[3 * t + c];
@@ -147,16 +162,55 @@ void build_device_scene(wr_scene &s) {
                 tri_mesh[g] = uint32_t(mi);
                 tri_prim[g] = t;
                 tri_code[g] = code;
+                if (!m.phong) continue;
+                // the PhongMeshGeometry of this triangle: normals as AssimpInOut stores them
+                // (zero when of ~zero length, else normalised in FP64; assimpio.h:211-223)
+                wrp::Patch<double> P;
+                for (int c = 0; c < 3; ++c) {
+                    const uint32_t vi = m.indices[3 * t + c];
+                    const float *q = &m.positions[3 * size_t(vi)];
+                    const float *nn = &m.normals[3 * size_t(vi)];
+                    P.p[c] = wrp::v3<double>(q[0], q[1], q[2]);
+                    const wrp::V<double> n = wrp::v3<double>(nn[0], nn[1], nn[2]);
+                    P.n[c] = wrp::is_approx_zero(wrp::length(n)) ? wrp::v3<double>(0.0, 0.0, 0.0) : wrp::normalize(n);
+                    patch_n[9 * g + 3 * c + 0] = P.n[c].x;
+                    patch_n[9 * g + 3 * c + 1] = P.n[c].y;
+                    patch_n[9 * g + 3 * c + 2] = P.n[c].z;
+                }
+                double lo[3], hi[3];
+                wrp::patch_bound(P, lo, hi);
+                for (int k = 0; k < 3; ++k) {
+                    // Embree keeps float(bound) (embreeaccel.h:63-75); the BVH uses the box
+                    // rounded outward so that it contains the FP64 bound
+                    float fl = float(lo[k]), fh = float(hi[k]);
+                    box_near[6 * g + k] = fl;
+                    box_near[6 * g + 3 + k] = fh;
+                    if (double(fl) > lo[k]) fl = std::nextafter(fl, -INFINITY);
+                    if (double(fh) < hi[k]) fh = std::nextafter(fh, INFINITY);
+                    box_out[6 * g + k] = fl;
+                    box_out[6 * g + 3 + k] = fh;
+                }
+                is_patch[g] = 1;
             }
         }
     }
-    {   // scene box of the guiding network's position feature (1% margin per side)
+    {   // scene box of the guiding network's position feature (1% margin per side), over the
+        // triangles and the patch bounds (the accel's bounds, rtcGetSceneBounds)
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (size_t i = 0; i + 2 < verts.size(); i += 3)
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], verts[i + k]);
-                hi[k] = std::max(hi[k], verts[i + k]);
+        for (uint32_t g = 0; g < ntri; ++g) {
+            if (is_patch[g]) {
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = std::min(lo[k], box_near[6 * size_t(g) + k]);
+                    hi[k] = std::max(hi[k], box_near[6 * size_t(g) + 3 + k]);
+                }
+                continue;
             }
+            for (int c = 0; c < 3; ++c)
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = std::min(lo[k], verts[9 * size_t(g) + 3 * c + k]);
+                    hi[k] = std::max(hi[k], verts[9 * size_t(g) + 3 * c + k]);
+                }
+        }
         double d2 = 0.0;
         for (int k = 0; k < 3; ++k) {
             if (!(lo[k] <= hi[k])) { lo[k] = 0.f; hi[k] = 1.f; }
@@ -169,12 +223,27 @@ void build_device_scene(wr_scene &s) {
         // the bounding sphere of EmbreeAccel::boundingSphere (src/accel/embreeaccel.h:326-334)
         s.dev.scene_radius = float(std::sqrt(d2) * 0.5);
     }
+    // the builders bound each primitive by the min/max of three points: a patch enters as the
+    // pseudo-triangle (lo, hi, hi) of its outward-rounded box
+    std::vector<float> bvh_verts;
+    if (npatch) {
+        bvh_verts = verts;
+        for (uint32_t g = 0; g < ntri; ++g) {
+            if (!is_patch[g]) continue;
+            float *o = &bvh_verts[9 * size_t(g)];
+            for (int k = 0; k < 3; ++k) {
+                o[k] = box_out[6 * size_t(g) + k];
+                o[3 + k] = o[6 + k] = box_out[6 * size_t(g) + 3 + k];
+            }
+        }
+    }
+    const std::vector<float> &build_in = npatch ? bvh_verts : verts;
     wr::BvhBuildResult bvh;
     const auto tb = std::chrono::steady_clock::now();
     if (s.opts.bvh_builder == WR_BVH_DEVICE_LBVH) {
-        bvh = wr::build_bvh_lbvh(verts, st, &s.bvh_ms);
+        bvh = wr::build_bvh_lbvh(build_in, st, &s.bvh_ms);
     } else {
-        bvh = wr::build_bvh_sah(verts, s.opts.max_leaf > 0 ? s.opts.max_leaf : 4, 0);
+        bvh = wr::build_bvh_sah(build_in, s.opts.max_leaf > 0 ? s.opts.max_leaf : 4, 0);
         s.bvh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
     }
     s.bvh_nodes = int(bvh.nodes.size() / 16);
@@ -183,19 +252,28 @@ void build_device_scene(wr_scene &s) {
     if (bvh.depth > wrd::kMaxStack) throw Error(WR_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
     std::vector<float> trisf(size_t(ntri) * 12);
     std::vector<uint32_t> leaf_mat(ntri);
+    std::vector<double> patchd(npatch ? size_t(ntri) * wrp::kPatchDoubles : 0, 0.0);
     for (uint32_t i = 0; i < ntri; ++i) {
         const uint32_t g = bvh.tri_order[i];
         float *o = &trisf[12 * size_t(i)];
         for (int c = 0; c < 3; ++c)
             for (int k = 0; k < 3; ++k) o[4 * c + k] = verts[9 * size_t(g) + 3 * c + k];
-        memcpy(&o[3], &g, 4);
+        const uint32_t gw = g | (is_patch[g] ? wrp::kPatchFlag : 0u);
+        memcpy(&o[3], &gw, 4);
         memcpy(&o[7], &tri_mesh[g], 4);
         memcpy(&o[11], &tri_prim[g], 4);
         leaf_mat[i] = tri_code[g];
+        if (is_patch[g]) {   // n1 n2 n3, then the outward box as 6 floats in the last 3 doubles
+            double *pd = &patchd[size_t(wrp::kPatchDoubles) * i];
+            for (int k = 0; k < 9; ++k) pd[k] = patch_n[9 * size_t(g) + k];
+            memcpy(pd + 9, &box_out[6 * size_t(g)], 24);
+        }
     }
     upload(s.nodes, bvh.nodes, st);
     upload(s.tris, trisf, st);
     upload(s.tri_mat, leaf_mat, st);
+    s.num_patches = npatch;
+    if (npatch) upload(s.patches, patchd, st);
 
     // materials
     std::vector<wrd::DevMaterial> mats(std::max<size_t>(h.materials.size(), 1));
@@ -289,6 +367,7 @@ void build_device_scene(wr_scene &s) {
     wrd::DevScene &d = s.dev;
     d.nodes = s.nodes.as<float4>();
     d.tris = s.tris.as<float4>();
+    d.patches = npatch ? s.patches.as<double>() : nullptr;
     d.tri_mat = s.tri_mat.as<uint32_t>();
     d.materials = s.materials.as<wrd::DevMaterial>();
     d.lights = s.lights.as<wrd::DevLight>();
@@ -522,7 +601,7 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     r.iter_limit = uint32_t(std::min<unsigned long long>((waves + 2) * (unsigned long long)(max_nverts + 2) + 64,
                                                          0xffffffffull));
     r.trace_block = (desc.trace_block == 64 || desc.trace_block == 256) ? desc.trace_block : 128;
-    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block));
+    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block, s.dev.patches != nullptr));
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * std::max(1, wrk::occupancy_blocks(1));
 
     const int profile = desc.profile;
@@ -970,11 +1049,11 @@ wrd::DevScene scene_for_queries(wr_scene &s) { return s.dev; }
 void trace_batch(wr_scene &s, const float *rays, int n, int any_hit, std::vector<float> &out, unsigned long long *nv,
                  unsigned long long *nt) {
     if (n < 0 || (n > 0 && !rays)) throw Error(WR_ERR_INVALID_ARGUMENT, "bad ray batch");
-    out.assign(size_t(n) * 8, 0.f);
+    out.assign(size_t(n) * 12, 0.f);
     if (n == 0) return;
     DevBuf dr, dout, dvis;
     dr.alloc(size_t(n) * 32);
-    dout.alloc(size_t(n) * 32);
+    dout.alloc(size_t(n) * 48);
     dvis.alloc(8);
     cudaStream_t st = s.stream;
     WR_CUDA(cudaMemcpyAsync(dr.p, rays, size_t(n) * 32, cudaMemcpyHostToDevice, st));
@@ -985,7 +1064,7 @@ void trace_batch(wr_scene &s, const float *rays, int n, int any_hit, std::vector
     wrk::launch_trace_batch(scene_for_queries(s), dr.as<float4>(), uint32_t(n), any_hit, dout.as<float4>(),
                             (nv || nt) ? dvis.as<uint32_t>() : nullptr, grid, st);
     WR_CUDA(cudaGetLastError());
-    WR_CUDA(cudaMemcpyAsync(out.data(), dout.p, size_t(n) * 32, cudaMemcpyDeviceToHost, st));
+    WR_CUDA(cudaMemcpyAsync(out.data(), dout.p, size_t(n) * 48, cudaMemcpyDeviceToHost, st));
     uint32_t vis[2] = {0, 0};
     WR_CUDA(cudaMemcpyAsync(vis, dvis.p, 8, cudaMemcpyDeviceToHost, st));
     WR_CUDA(cudaStreamSynchronize(st));
@@ -1228,7 +1307,7 @@ int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_rende
         }
         // 3) persistent-CTA count of the traversal and shading kernels
         const int blk = (cur.trace_block == 64 || cur.trace_block == 256) ? cur.trace_block : 128;
-        const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk));
+        const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk, s->dev.patches != nullptr));
         const int occ_s = sms * std::max(1, wrk::occupancy_blocks(1));
         for (double f : {0.5, 1.0}) {
             wr_render_desc d = cur;
@@ -1396,7 +1475,7 @@ int wr_trace_closest(wr_scene *s, const float *rays, int n, int *geom_id, int *p
         std::vector<float> out;
         trace_batch(*s, rays, n, 0, out, nullptr, nullptr);
         for (int i = 0; i < n; ++i) {
-            const float *o = &out[8 * size_t(i)];
+            const float *o = &out[12 * size_t(i)];
             uint32_t g, p;
             memcpy(&g, &o[0], 4);
             memcpy(&p, &o[1], 4);
@@ -1411,6 +1490,30 @@ int wr_trace_closest(wr_scene *s, const float *rays, int n, int *geom_id, int *p
     }
 }
 
+int wr_trace_hits(wr_scene *s, const float *rays, int n, int *geom_id, int *prim_id, float *t, float *normal) {
+    if (!s || (n > 0 && (!geom_id || !prim_id || !t || !normal))) {
+        g_last_error = "null argument";
+        return WR_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        std::vector<float> out;
+        trace_batch(*s, rays, n, 0, out, nullptr, nullptr);
+        for (int i = 0; i < n; ++i) {
+            const float *o = &out[12 * size_t(i)];
+            uint32_t g, p;
+            memcpy(&g, &o[0], 4);
+            memcpy(&p, &o[1], 4);
+            geom_id[i] = g == wrd::MISS ? -1 : int(g);
+            prim_id[i] = p == wrd::MISS ? -1 : int(p);
+            t[i] = o[2];
+            for (int k = 0; k < 3; ++k) normal[3 * i + k] = o[8 + k];
+        }
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
 int wr_trace_occluded(wr_scene *s, const float *rays, int n, int *occluded) {
     if (!s || (n > 0 && !occluded)) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
     try {
@@ -1418,7 +1521,7 @@ int wr_trace_occluded(wr_scene *s, const float *rays, int n, int *occluded) {
         trace_batch(*s, rays, n, 1, out, nullptr, nullptr);
         for (int i = 0; i < n; ++i) {
             uint32_t g;
-            memcpy(&g, &out[8 * size_t(i)], 4);
+            memcpy(&g, &out[12 * size_t(i)], 4);
             occluded[i] = g == wrd::MISS ? 0 : 1;
         }
         return WR_OK;

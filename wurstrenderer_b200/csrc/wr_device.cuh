@@ -93,7 +93,9 @@ constexpr int INTEGRATOR_LIGHT = 2;      // light_splatting (src/renderer/lights
 
 struct DevScene {
     const float4 *nodes;
-    const float4 *tris;
+    const float4 *tris;             // leaf order: p0, p1, p2 (.w: index | patch flag, mesh, primitive)
+    const double *patches;          // Phong tessellation patches (wrp::kPatchDoubles per leaf primitive),
+                                    // nullptr when the scene has none
     const uint32_t *tri_mat;
     const DevMaterial *materials;
     const DevLight *lights;

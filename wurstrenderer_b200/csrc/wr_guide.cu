@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "wr_device.cuh"
+#include "wr_trace.cuh"
 #include "wr_guide.h"
 #include "wr_host.h"
 #include "wr_guide_net.cuh"
@@ -62,13 +63,12 @@ __device__ __forceinline__ bool fetch_point(const InferSource &s, uint32_t i, f3
     const uint32_t tri = __float_as_uint(h.w);
     if (tri == wrd::MISS) return false;
     const uint32_t mat = __ldg(s.tri_mat + tri);
-    const f3 a = wrd::xyz(__ldg(s.tris + 3 * tri)), b = wrd::xyz(__ldg(s.tris + 3 * tri + 1)),
-             c = wrd::xyz(__ldg(s.tris + 3 * tri + 2));
+    const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), c = __ldg(s.tris + 3 * tri + 2);
     if (mat & wrd::LIGHT_BIT) return false;
     const f3 dd = mk(d.x, d.y, d.z);
     p = mk(o.x, o.y, o.z) + dd * h.x;
     wo = -dd;
-    n = guide_normal(wrd::normalize(wrd::cross(b - a, c - a)), wo);
+    n = guide_normal(wrd::surface_normal(a, b, c, h.y, h.z), wo);
     return true;
 }
 

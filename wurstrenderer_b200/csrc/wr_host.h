@@ -40,6 +40,8 @@ struct Mesh {
     std::string name;
     std::vector<float> positions;   // xyz per vertex
     std::vector<uint32_t> indices;  // 3 per triangle
+    std::vector<float> normals;     // phong meshes: the OBJ's `vn` per vertex, as read (float xyz)
+    bool phong = false;             // Phong tessellation patches instead of flat triangles
     int material = -1;              // surfaces: index into Scene::materials
     int light = -1;                 // emitters: index into Scene::lights
     uint32_t num_triangles() const { return uint32_t(indices.size() / 3); }

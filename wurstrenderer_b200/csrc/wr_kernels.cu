@@ -378,7 +378,7 @@ __device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c)
 //   SHADOW = true:  shadow -- any hit of every queued shadow ray; unoccluded contributions
 //                   are added to the FP64 film (and to the path's training records)
 
-template <int BLOCK, bool SHADOW>
+template <int BLOCK, bool SHADOW, bool PHONG>
 __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w, uint32_t *stack) {
     const uint32_t n = SHADOW ? min(w.ctr[CTR_SHADOW], w.shadow_capacity) : w.ctr[CTR_ACTIVE];
     uint32_t *fetch = w.ctr + (SHADOW ? CTR_SHADOW_FETCH : CTR_EXTEND_FETCH);
@@ -387,6 +387,7 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
     st.stride = BLOCK;
     st.sp = 0;
     RayPre r{};
+    PatchRay pr{};   // read only by the PHONG instantiation
     float t = 0.f, bu = 0.f, bv = 0.f;
     uint32_t tri = MISS, ray = 0, nv = 0, nt = 0;
     int node = kTraceDone, leaf = 0;
@@ -407,6 +408,7 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
                     if (SHADOW) { o = w.sq.o[ray]; d = w.sq.d[ray]; tmax = o.w; }
                     else { o = w.cur.o[ray]; d = w.cur.d[ray]; tmax = __int_as_float(0x7f800000); }
                     r = ray_setup(xyz(o), xyz(d));
+                    if (PHONG) pr = PatchRay{o.x, o.y, o.z, d.x, d.y, d.z};
                     t = tmax; tri = MISS; bu = 0.f; bv = 0.f;
                     node = 0; leaf = 0; st.sp = 0;
                     busy = true;
@@ -417,8 +419,8 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
         }
         if (!__any_sync(0xffffffffu, busy)) break;
         const int min_active = __any_sync(0xffffffffu, exhausted) ? 0 : w.fetch_min;
-        if (busy && traverse_steps<SHADOW>(s.nodes, s.tris, r, kRayEps, t, tri, bu, bv, node, leaf, st, nv, nt,
-                                           min_active)) {
+        if (busy && traverse_steps<SHADOW, PHONG>(s.nodes, s.tris, r, kRayEps, t, tri, bu, bv, node, leaf, st, nv,
+                                                  nt, min_active, s.patches, pr)) {
             busy = false;
             if (SHADOW) {
                 if (tri == MISS) {   // unoccluded
@@ -438,10 +440,10 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
     }
 }
 
-template <int BLOCK>
+template <int BLOCK, bool PHONG>
 __global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    trace_queue<BLOCK, false>(s, w, stack);
+    trace_queue<BLOCK, false, PHONG>(s, w, stack);
 }
 
 // lens point of a sample's camera vertex (ThinlensCamera::sampleWe0ByPdf, thinlens.h:121-136; the
@@ -553,8 +555,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
             // lightsplatting.h:85-104); emitter hits and misses end the subpath
             if (tri != MISS && !(__ldg(s.tri_mat + tri) & LIGHT_BIT)) {
                 const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
-                const f3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(cc);
-                const f3 ng = normalize(cross(p1 - p0, p2 - p0));
+                const f3 ng = surface_normal(a, b, cc, h.y, h.z);
                 const f3 pos = o + d * t;
                 const DevMaterial mm = s.materials[__ldg(s.tri_mat + tri)];
                 const Frame fr(ng);
@@ -604,8 +605,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
             }
         } else {
             const float4 a = __ldg(s.tris + 3 * tri), b = __ldg(s.tris + 3 * tri + 1), cc = __ldg(s.tris + 3 * tri + 2);
-            const f3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(cc);
-            const f3 ng = normalize(cross(p1 - p0, p2 - p0));
+            const f3 ng = surface_normal(a, b, cc, h.y, h.z);
             const f3 pos = o + d * t;
             const uint32_t mat = __ldg(s.tri_mat + tri);
             if (mat & LIGHT_BIT) {
@@ -886,10 +886,10 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
     }
 }
 
-template <int BLOCK>
+template <int BLOCK, bool PHONG>
 __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    trace_queue<BLOCK, true>(s, w, stack);
+    trace_queue<BLOCK, true, PHONG>(s, w, stack);
 }
 
 // queue bookkeeping between iterations (one thread); also drives the graph's while loop
@@ -934,6 +934,10 @@ __global__ void k_resolve(const double *film, double *out, uint32_t total_pix, c
 
 // ----------------------------------------------------------- ray batches ----
 // rays: n x 8 floats (ox, oy, oz, tnear, dx, dy, dz, tfar)
+// out: 3 float4 per ray -- (geomID, primID, t, leaf index), (u, v, 0, 0) with the triangle's
+// barycentrics (zero on a patch, whose texture coordinate the reference leaves at zero), and
+// (unit geometry normal, 0)
+template <bool PHONG>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_batch(DevScene s, const float4 *rays, uint32_t n, int any_hit,
                                                            float4 *out, uint32_t *visits) {
     __shared__ uint32_t stack[kSmemStack * kTraceBlock];
@@ -943,15 +947,25 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_batch(DevScene s, const f
         float t, bu = 0.f, bv = 0.f;
         uint32_t tri;
         bool hit;
-        if (any_hit) hit = traverse<true>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt);
-        else hit = traverse<false>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt);
+        if (any_hit)
+            hit = traverse<true, PHONG>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt,
+                                        s.patches);
+        else
+            hit = traverse<false, PHONG>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt,
+                                         s.patches);
         uint32_t gid = MISS, pid = MISS;
+        f3 ng = mk(0.f, 0.f, 0.f);
         if (hit) {
-            gid = __float_as_uint(__ldg(s.tris + 3 * tri + 1).w);
-            pid = __float_as_uint(__ldg(s.tris + 3 * tri + 2).w);
+            const float4 ta = __ldg(s.tris + 3 * tri), tb = __ldg(s.tris + 3 * tri + 1), tc = __ldg(s.tris + 3 * tri + 2);
+            gid = __float_as_uint(tb.w);
+            pid = __float_as_uint(tc.w);
+            ng = surface_normal(ta, tb, tc, bu, bv);
+            if (__float_as_uint(ta.w) & wrp::kPatchFlag) { bu = 0.f; bv = 0.f; }
         }
-        out[2 * i] = make_float4(__uint_as_float(gid), __uint_as_float(pid), hit ? t : __int_as_float(0x7f800000), 0.f);
-        out[2 * i + 1] = make_float4(bu, bv, __uint_as_float(tri), 0.f);
+        out[3 * i] = make_float4(__uint_as_float(gid), __uint_as_float(pid), hit ? t : __int_as_float(0x7f800000),
+                                 __uint_as_float(tri));
+        out[3 * i + 1] = make_float4(bu, bv, 0.f, 0.f);
+        out[3 * i + 2] = make_float4(ng.x, ng.y, ng.z, 0.f);
     }
     if (visits) {
         atomicAdd(visits, nv);
@@ -1065,9 +1079,15 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
     const WaveArgs w = make_args(b, parity, r);
     switch (which) {
         case KERNEL_EXTEND:
-            if (r.trace_block == 64) k_extend<64><<<r.grid_trace, 64, 0, st>>>(s, w);
-            else if (r.trace_block == 256) k_extend<256><<<r.grid_trace, 256, 0, st>>>(s, w);
-            else k_extend<128><<<r.grid_trace, 128, 0, st>>>(s, w);
+            if (s.patches) {
+                if (r.trace_block == 64) k_extend<64, true><<<r.grid_trace, 64, 0, st>>>(s, w);
+                else if (r.trace_block == 256) k_extend<256, true><<<r.grid_trace, 256, 0, st>>>(s, w);
+                else k_extend<128, true><<<r.grid_trace, 128, 0, st>>>(s, w);
+            } else {
+                if (r.trace_block == 64) k_extend<64, false><<<r.grid_trace, 64, 0, st>>>(s, w);
+                else if (r.trace_block == 256) k_extend<256, false><<<r.grid_trace, 256, 0, st>>>(s, w);
+                else k_extend<128, false><<<r.grid_trace, 128, 0, st>>>(s, w);
+            }
             break;
         case KERNEL_SHADE:
             if (w.lobes) k_shade<true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
@@ -1080,9 +1100,15 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
             break;
         case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
         case KERNEL_SHADOW:
-            if (r.trace_block == 64) k_shadow<64><<<r.grid_trace, 64, 0, st>>>(s, w);
-            else if (r.trace_block == 256) k_shadow<256><<<r.grid_trace, 256, 0, st>>>(s, w);
-            else k_shadow<128><<<r.grid_trace, 128, 0, st>>>(s, w);
+            if (s.patches) {
+                if (r.trace_block == 64) k_shadow<64, true><<<r.grid_trace, 64, 0, st>>>(s, w);
+                else if (r.trace_block == 256) k_shadow<256, true><<<r.grid_trace, 256, 0, st>>>(s, w);
+                else k_shadow<128, true><<<r.grid_trace, 128, 0, st>>>(s, w);
+            } else {
+                if (r.trace_block == 64) k_shadow<64, false><<<r.grid_trace, 64, 0, st>>>(s, w);
+                else if (r.trace_block == 256) k_shadow<256, false><<<r.grid_trace, 256, 0, st>>>(s, w);
+                else k_shadow<128, false><<<r.grid_trace, 128, 0, st>>>(s, w);
+            }
             break;
         case KERNEL_ADVANCE: k_advance<<<1, 1, 0, st>>>(w); break;
         default: break;
@@ -1108,7 +1134,8 @@ void launch_resolve(const double *film, double *out, const RenderLaunch &r, cuda
 
 void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,
                         int grid, cudaStream_t st) {
-    k_trace_batch<<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+    if (s.patches) k_trace_batch<true><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+    else k_trace_batch<false><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
 }
 
 void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t ntables, float *cdf, float *pdf,
@@ -1124,12 +1151,16 @@ void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n,
     k_scale_pdf<<<592, 256, 0, st>>>(weights, total, pdf, n);
 }
 
-int occupancy_blocks(int which, int trace_block) {
+int occupancy_blocks(int which, int trace_block, bool phong) {
     int nb = 0;
-    if (which == 0) {
-        if (trace_block == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<64>, 64, 0);
-        else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128>, 128, 0);
+    if (which == 0 && phong) {
+        if (trace_block == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<64, true>, 64, 0);
+        else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256, true>, 256, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128, true>, 128, 0);
+    } else if (which == 0) {
+        if (trace_block == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<64, false>, 64, 0);
+        else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256, false>, 256, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128, false>, 128, 0);
     } else {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false>, kShadeBlock, 0);
     }

@@ -270,14 +270,19 @@ struct ObjMeshRaw {
     std::string name;
     int mtl = 0;
     std::vector<uint32_t> gidx;   // global vertex indices, 3 per triangle
+    std::vector<int32_t> nidx;    // global `vn` indices per corner (-1: none)
 };
 
-void load_obj(const std::string &path, const std::map<std::string, double> &sigma, Scene &scene) {
+// `phong`: the mesh entry's "phong_tessellation" flag. Its surface meshes become Phong
+// tessellation patches (Simple2Parser::ParseScene, src/sceneio/simple2parser.h:37-55) with one
+// vertex per distinct (position, normal) pair, as Assimp's JoinIdenticalVertices leaves them;
+// its emitters stay triangle meshes (simple2parser.h:58).
+void load_obj(const std::string &path, const std::map<std::string, double> &sigma, bool phong, Scene &scene) {
     const std::string data = slurp(path);
     std::vector<MtlEntry> mats(1);
     mats[0].name = "DefaultMaterial";
     std::unordered_map<std::string, int> mat_idx{{"DefaultMaterial", 0}};
-    std::vector<float> verts;
+    std::vector<float> verts, norms;
     std::vector<ObjMeshRaw> meshes;
     int cur_mtl = 0;
     auto start_mesh = [&](const std::string &name) {
@@ -286,7 +291,7 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
         meshes.back().mtl = cur_mtl;
     };
     const char *p = data.data(), *end = p + data.size();
-    std::vector<long> poly;
+    std::vector<long> poly, npoly;
     while (p < end) {
         const char *le = static_cast<const char *>(memchr(p, '\n', size_t(end - p)));
         if (!le) le = end;
@@ -294,11 +299,15 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
         if (q + 1 < le && q[0] == 'v' && (q[1] == ' ' || q[1] == '\t')) {
             char *e2 = const_cast<char *>(q + 1);
             for (int k = 0; k < 3; ++k) verts.push_back(strtof(e2, &e2));
+        } else if (q + 2 < le && q[0] == 'v' && q[1] == 'n' && (q[2] == ' ' || q[2] == '\t')) {
+            char *e2 = const_cast<char *>(q + 2);
+            for (int k = 0; k < 3; ++k) norms.push_back(strtof(e2, &e2));
         } else if (q + 1 < le && q[0] == 'f' && (q[1] == ' ' || q[1] == '\t')) {
             if (meshes.empty()) start_mesh("defaultobject");
             poly.clear();
+            npoly.clear();
             const char *r = q + 1;
-            const long nv = long(verts.size() / 3);
+            const long nv = long(verts.size() / 3), nn = long(norms.size() / 3);
             while (true) {
                 r = skip_ws(r, le);
                 if (r >= le) break;
@@ -308,12 +317,28 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
                 long gi = v < 0 ? nv + v : v - 1;
                 if (gi < 0 || gi >= nv) throw Error(WR_ERR_PARSE, "obj: vertex index out of range in " + path);
                 poly.push_back(gi);
+                long ni = -1;   // v, v/vt, v//vn or v/vt/vn
+                if (e2 < le && *e2 == '/') {
+                    char *e3 = e2 + 1;
+                    if (e3 < le && *e3 != '/') strtol(e3, &e3, 10);
+                    if (e3 < le && *e3 == '/') {
+                        char *e4 = e3 + 1;
+                        const long n = strtol(e4, &e3, 10);
+                        if (e3 != e4) {
+                            ni = n < 0 ? nn + n : n - 1;
+                            if (ni < 0 || ni >= nn) throw Error(WR_ERR_PARSE, "obj: normal index out of range in " + path);
+                        }
+                    }
+                    e2 = e3;
+                }
+                npoly.push_back(ni);
                 r = token_end(e2, le);
             }
             for (size_t k = 1; k + 1 < poly.size(); ++k) {
-                meshes.back().gidx.push_back(uint32_t(poly[0]));
-                meshes.back().gidx.push_back(uint32_t(poly[k]));
-                meshes.back().gidx.push_back(uint32_t(poly[k + 1]));
+                for (size_t c : {size_t(0), k, k + 1}) {
+                    meshes.back().gidx.push_back(uint32_t(poly[c]));
+                    meshes.back().nidx.push_back(int32_t(npoly[c]));
+                }
             }
         } else if (q + 1 < le && (q[0] == 'o' || q[0] == 'g') && (q[1] == ' ' || q[1] == '\t')) {
             const char *n0 = skip_ws(q + 1, le);
@@ -379,16 +404,41 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
         Mesh m;
         m.name = om.name;
         m.indices.resize(om.gidx.size());
-        std::vector<uint32_t> used;
-        for (size_t k = 0; k < om.gidx.size(); ++k) {
-            const uint32_t g = om.gidx[k];
-            if (local[g] < 0) { local[g] = int32_t(used.size()); used.push_back(g); }
-            m.indices[k] = uint32_t(local[g]);
-        }
-        m.positions.resize(used.size() * 3);
-        for (size_t k = 0; k < used.size(); ++k) {
-            for (int c = 0; c < 3; ++c) m.positions[3 * k + c] = verts[3 * size_t(used[k]) + c];
-            local[used[k]] = -1;
+        if (phong && !emitter[om.mtl]) {
+            // one vertex per distinct (position, normal) pair
+            std::unordered_map<uint64_t, uint32_t> pair_idx;
+            for (size_t k = 0; k < om.gidx.size(); ++k) {
+                if (om.nidx[k] < 0)
+                    throw Error(WR_ERR_UNSUPPORTED, "phong_tessellation mesh '" + om.name + "' in " + path +
+                                                        " has a face corner without a vertex normal (vn)");
+                const uint64_t key = (uint64_t(om.gidx[k]) << 32) | uint32_t(om.nidx[k]);
+                auto it = pair_idx.find(key);
+                uint32_t li;
+                if (it == pair_idx.end()) {
+                    li = uint32_t(pair_idx.size());
+                    pair_idx.emplace(key, li);
+                    for (int c = 0; c < 3; ++c) {
+                        m.positions.push_back(verts[3 * size_t(om.gidx[k]) + c]);
+                        m.normals.push_back(norms[3 * size_t(om.nidx[k]) + c]);
+                    }
+                } else {
+                    li = it->second;
+                }
+                m.indices[k] = li;
+            }
+            m.phong = true;
+        } else {
+            std::vector<uint32_t> used;
+            for (size_t k = 0; k < om.gidx.size(); ++k) {
+                const uint32_t g = om.gidx[k];
+                if (local[g] < 0) { local[g] = int32_t(used.size()); used.push_back(g); }
+                m.indices[k] = uint32_t(local[g]);
+            }
+            m.positions.resize(used.size() * 3);
+            for (size_t k = 0; k < used.size(); ++k) {
+                for (int c = 0; c < 3; ++c) m.positions[3 * k + c] = verts[3 * size_t(used[k]) + c];
+                local[used[k]] = -1;
+            }
         }
         if (emitter[om.mtl]) {
             m.light = int(om.mtl);   // temporarily the material index; resolved below
@@ -427,15 +477,14 @@ Scene load_from_node(const JNode &root, const std::string &base_dir) {
     if (const JNode *meshes = root.find("meshes")) {
         if (meshes->kind != JNode::ARR) throw Error(WR_ERR_PARSE, "scene json: 'meshes' must be an array");
         for (const JNode &mj : meshes->items) {
-            if (mj.num("phong_tessellation", 0.0) != 0.0)
-                throw Error(WR_ERR_UNSUPPORTED, "phong_tessellation meshes are not supported");
+            const bool phong = mj.num("phong_tessellation", 0.0) != 0.0;
             std::map<std::string, double> sigma;
             if (const JNode *sj = mj.find("oren_nayar_sigma")) {
                 for (size_t i = 0; i < sj->keys.size(); ++i) sigma[sj->keys[i]] = sj->items[i].n;
             }
             if (mj.num("mitsuba_srgb", 0.0) != 0.0)
                 throw Error(WR_ERR_UNSUPPORTED, "mitsuba_srgb colour conversion is not supported");
-            load_obj(join_path(base_dir, mj.str("path", "")), sigma, s);
+            load_obj(join_path(base_dir, mj.str("path", "")), sigma, phong, s);
         }
     }
     if (const JNode *cj = root.find("camera")) {

@@ -15,9 +15,15 @@
 //   when an edge function is exactly zero. Hits are accepted on (tmin, tmax] as
 //   Embree's |den|*tnear < T <= |den|*tfar, with no back-face culling. The
 //   barycentrics returned are Embree's (u, v) = weights of v1 and v2.
+//
+// Scenes with Phong tessellation patches use the PHONG instantiation: a leaf primitive whose
+// record carries wrp::kPatchFlag is tested first against its own box, then with the FP64
+// patch test of wr_phong.cuh; an accepted patch hit stores its unit normal, octahedrally
+// encoded, in the two barycentric slots. Triangle-only scenes never compile that code in.
 #pragma once
 
 #include "wr_device.cuh"
+#include "wr_phong.cuh"
 
 namespace wrd {
 
@@ -99,6 +105,40 @@ __device__ __forceinline__ bool tri_test(const RayPre &r, float4 a, float4 b, fl
     return true;
 }
 
+// the float ray as the patch test takes it (PHONG instantiations only)
+struct PatchRay {
+    float ox, oy, oz, dx, dy, dz;
+};
+
+// leaf primitive i is a patch: its own box, then the FP64 test against (tmin, t]; on a hit
+// lowers t and stores the encoded normal in (bu, bv)
+__device__ __forceinline__ bool patch_leaf_test(const RayPre &r, const PatchRay &pr, const double *patches, uint32_t i,
+                                                float4 a, float4 b, float4 c, float tmin, float &t, float &bu,
+                                                float &bv) {
+    float lo[3], hi[3];
+    wrp::load_patch_box(patches, i, lo, hi);
+    if (box_entry(r, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], tmin, t) == __int_as_float(0x7f800000)) return false;
+    const wrp::Patch<wrp::Rd> P = wrp::load_patch(patches, i, a, b, c);
+    wrp::Rd tm = wrp::Rd(double(t));
+    wrp::V<wrp::Rd> n;
+    if (!wrp::patch_intersect(P, pr.ox, pr.oy, pr.oz, pr.dx, pr.dy, pr.dz, tmin, tm, n)) return false;
+    const float2 e = wrp::oct_encode(float(n.x.v), float(n.y.v), float(n.z.v));
+    t = float(tm.v);
+    bu = e.x;
+    bv = e.y;
+    return true;
+}
+
+// unit geometry normal of a hit on leaf primitive (a, b, c): the triangle's face normal,
+// or the patch normal the traversal stored (encoded) in the barycentric slots
+__device__ __forceinline__ f3 surface_normal(float4 a, float4 b, float4 c, float bu, float bv) {
+    if (__float_as_uint(a.w) & wrp::kPatchFlag) {
+        const float3 n = wrp::oct_decode(bu, bv);
+        return mk(n.x, n.y, n.z);
+    }
+    return normalize(cross(xyz(b) - xyz(a), xyz(c) - xyz(a)));
+}
+
 struct TraceStack {
     uint32_t *smem;   // kSmemStack x blockDim.x words, column = threadIdx.x
     int stride;
@@ -124,13 +164,14 @@ struct TraceStack {
 // descending inner nodes until every converged lane of the warp holds a leaf,
 // so that the triangle tests run with most lanes active. The warp vote only
 // steers scheduling; each lane's result does not depend on other lanes.
-template <bool ANY_HIT>
+template <bool ANY_HIT, bool PHONG = false>
 __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const float4 *__restrict__ tris, f3 o,
                                          f3 d, float tmin, float tmax, uint32_t *smem_stack, float &t, uint32_t &tri,
                                          float &bu, float &bv, uint32_t *node_visits = nullptr,
-                                         uint32_t *tri_tests = nullptr) {
+                                         uint32_t *tri_tests = nullptr, const double *patches = nullptr) {
     constexpr int kDone = 0x7fffffff;   // traversal finished (stack empty)
     const RayPre r = ray_setup(o, d);
+    const PatchRay pr{o.x, o.y, o.z, d.x, d.y, d.z};
     TraceStack st;
     st.smem = smem_stack + threadIdx.x;
     st.stride = blockDim.x;
@@ -178,6 +219,16 @@ __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const
                 const float4 b = __ldg(tris + 3 * i + 1);
                 const float4 c = __ldg(tris + 3 * i + 2);
                 ++nt;
+                if (PHONG && (__float_as_uint(a.w) & wrp::kPatchFlag)) {
+                    if (patch_leaf_test(r, pr, patches, i, a, b, c, tmin, t, bu, bv)) {
+                        tri = i;
+                        if (ANY_HIT) {
+                            if (node_visits) { *node_visits += nv; *tri_tests += nt; }
+                            return true;
+                        }
+                    }
+                    continue;
+                }
                 float th, uh, vh;
                 if (tri_test(r, a, b, c, tmin, t, th, uh, vh)) {
                     if (ANY_HIT) {
@@ -208,11 +259,12 @@ __device__ __forceinline__ bool traverse(const float4 *__restrict__ nodes, const
 // exhausted); the result is the same as `traverse`'s, only the schedule differs.
 constexpr int kTraceDone = 0x7fffffff;
 
-template <bool ANY_HIT>
+template <bool ANY_HIT, bool PHONG = false>
 __device__ __forceinline__ bool traverse_steps(const float4 *__restrict__ nodes, const float4 *__restrict__ tris,
                                                const RayPre &r, float tmin, float &t, uint32_t &tri, float &bu,
                                                float &bv, int &node, int &leaf, TraceStack &st, uint32_t &nv,
-                                               uint32_t &nt, int min_active) {
+                                               uint32_t &nt, int min_active, const double *patches = nullptr,
+                                               const PatchRay &pr = PatchRay{}) {
     while (node != kTraceDone) {
         while (node >= 0 && node != kTraceDone) {
             const float4 n0 = __ldg(nodes + 4 * node + 0);
@@ -251,6 +303,17 @@ __device__ __forceinline__ bool traverse_steps(const float4 *__restrict__ nodes,
                 const float4 b = __ldg(tris + 3 * i + 1);
                 const float4 c = __ldg(tris + 3 * i + 2);
                 ++nt;
+                if (PHONG && (__float_as_uint(a.w) & wrp::kPatchFlag)) {
+                    if (patch_leaf_test(r, pr, patches, i, a, b, c, tmin, t, bu, bv)) {
+                        tri = i;
+                        if (ANY_HIT) {
+                            node = kTraceDone;
+                            leaf = 0;
+                            return true;
+                        }
+                    }
+                    continue;
+                }
                 float th, uh, vh;
                 if (tri_test(r, a, b, c, tmin, t, th, uh, vh)) {
                     if (ANY_HIT) {

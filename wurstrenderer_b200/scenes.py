@@ -52,6 +52,7 @@ class Mesh:
     material: str
     positions: np.ndarray          # (V, 3) float32
     triangles: np.ndarray          # (T, 3) int, 0-based, local to this mesh
+    normals: np.ndarray | None = None   # (V, 3) float32 vertex normals, written as `vn`
 
 
 @dataclass
@@ -59,10 +60,11 @@ class SceneSpec:
     meshes: list = field(default_factory=list)
     materials: dict = field(default_factory=dict)
 
-    def add(self, name, material, positions, triangles):
+    def add(self, name, material, positions, triangles, normals=None):
         self.meshes.append(Mesh(name, material.name,
                                 np.asarray(positions, np.float32),
-                                np.asarray(triangles, np.int64)))
+                                np.asarray(triangles, np.int64),
+                                None if normals is None else np.asarray(normals, np.float32)))
         self.materials.setdefault(material.name, material)
 
     @property
@@ -190,14 +192,24 @@ def _fmt3(v):
 
 
 def write_obj(spec: SceneSpec, obj_path: str, mtl_name: str):
-    """Writes one OBJ (global 1-based vertex indices) and its MTL."""
+    """Writes one OBJ (global 1-based vertex indices) and its MTL. Meshes with normals get
+    one `vn` per vertex and `f v//vn` faces (normal index = vertex index)."""
     with open(obj_path, "w") as f:
         f.write("mtllib %s\n" % mtl_name)
         base = 1
+        nbase = 1
         for m in spec.meshes:
             f.write("o %s\nusemtl %s\n" % (m.name, m.material))
             np.savetxt(f, m.positions.astype(np.float32), fmt="v %.9g %.9g %.9g")
-            np.savetxt(f, m.triangles + base, fmt="f %d %d %d")
+            if m.normals is not None:
+                np.savetxt(f, m.normals.astype(np.float32), fmt="vn %.9g %.9g %.9g")
+                idx = m.triangles + base
+                nidx = m.triangles + nbase
+                np.savetxt(f, np.stack([idx[:, 0], nidx[:, 0], idx[:, 1], nidx[:, 1], idx[:, 2], nidx[:, 2]], 1),
+                           fmt="f %d//%d %d//%d %d//%d")
+                nbase += m.normals.shape[0]
+            else:
+                np.savetxt(f, m.triangles + base, fmt="f %d %d %d")
             base += m.positions.shape[0]
     mtl_path = os.path.join(os.path.dirname(obj_path), mtl_name)
     with open(mtl_path, "w") as f:
@@ -228,6 +240,41 @@ def write_scene(out_dir, name, spec, camera, renders, envmap=None, extra=None):
     with open(path, "w") as f:
         json.dump(scene, f, indent=1)
     return path
+
+
+def write_scene_entries(out_dir, name, entries, camera, renders, envmap=None):
+    """Writes a scene with several mesh entries: `entries` is a list of (suffix, spec, extra
+    mesh-entry keys); each spec goes to `<name>_<suffix>.obj/.mtl`. Returns the JSON path."""
+    os.makedirs(out_dir, exist_ok=True)
+    meshes = []
+    for suffix, spec, extra in entries:
+        base = "%s_%s" % (name, suffix)
+        write_obj(spec, os.path.join(out_dir, base + ".obj"), base + ".mtl")
+        entry = {"path": base + ".obj"}
+        sig = {m.name: float(m.sigma) for m in spec.materials.values() if m.sigma is not None}
+        if sig:
+            entry["oren_nayar_sigma"] = sig
+        entry.update(extra or {})
+        meshes.append(entry)
+    scene = {"comment": name, "camera": camera, "meshes": meshes, "render": renders}
+    if envmap is not None:
+        scene["envmap"] = envmap
+    path = os.path.join(out_dir, name + ".json")
+    with open(path, "w") as f:
+        json.dump(scene, f, indent=1)
+    return path
+
+
+def vertex_normals(positions, triangles):
+    """Area-weighted vertex normals (unit, float32) of an indexed triangle mesh."""
+    p = np.asarray(positions, np.float64)
+    t = np.asarray(triangles, np.int64)
+    fn = np.cross(p[t[:, 1]] - p[t[:, 0]], p[t[:, 2]] - p[t[:, 0]])
+    n = np.zeros_like(p)
+    for c in range(3):
+        np.add.at(n, t[:, c], fn)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    return n.astype(np.float32)
 
 
 def nee_render(output, spp, num_path_vertices):
@@ -277,6 +324,46 @@ def write_cornell(out_dir, name="cornell", resolution=(256, 256), spp=16,
     cam = dict(CORNELL_CAMERA, resolution=list(resolution))
     return write_scene(out_dir, name, spec, cam,
                        [nee_render(output or name + ".pfm", spp, num_path_vertices)])
+
+
+def phong_objects_spec(seed=1007, n_objects=5):
+    """Smooth low-poly objects for Phong tessellation: icospheres (1-2 subdivisions) and
+    radially perturbed blobs, each with area-weighted vertex normals; diffuse, glossy
+    and mixed materials."""
+    rng = np.random.default_rng(seed)
+    spec = SceneSpec()
+    centers = [(-0.5, 0.32, 0.25), (0.45, 0.3, 0.35), (0.0, 0.9, -0.4), (-0.45, 1.35, -0.2), (0.5, 1.0, -0.35)]
+    radii = [0.3, 0.28, 0.33, 0.25, 0.22]
+    for i in range(n_objects):
+        p, t = icosphere(centers[i], radii[i], 1 + (i % 2))
+        if i >= 3:   # a blob: radius varies smoothly with direction
+            d = (p - np.asarray(centers[i])) / radii[i]
+            r = radii[i] * (1.0 + 0.18 * d[:, 0] * d[:, 1] + 0.12 * d[:, 2] ** 2)
+            p = np.asarray(centers[i]) + d * r[:, None]
+        n = vertex_normals(p, t)
+        kind = i % 3
+        if kind == 0:
+            mat = Material("m_phong%d" % i, kd=tuple(rng.uniform(0.3, 0.8, 3)))
+        elif kind == 1:
+            mat = Material("m_phong%d" % i, ks=tuple(rng.uniform(0.5, 0.8, 3)), exponent=float(rng.uniform(20, 80)))
+        else:
+            mat = Material("m_phong%d" % i, kd=tuple(rng.uniform(0.2, 0.5, 3)), ks=(0.3, 0.3, 0.3), exponent=30.0)
+        spec.add("phong%d" % i, mat, p, t, normals=n)
+    return spec
+
+
+def write_phong_cornell(out_dir, name="phong_cornell", resolution=(128, 128), spp=16,
+                        num_path_vertices=8, integrator="nextevent_path_tracer"):
+    """Cornell walls and light as triangles (first entry) plus the smooth objects of
+    `phong_objects_spec` as a "phong_tessellation": true entry."""
+    walls = cornell_spec()
+    walls.meshes = [m for m in walls.meshes if m.name not in ("short_box", "tall_box")]
+    cam = dict(CORNELL_CAMERA, resolution=list(resolution))
+    render = nee_render(name + ".pfm", spp, num_path_vertices)
+    render["integrator"] = integrator
+    return write_scene_entries(out_dir, name, [("walls", walls, None),
+                                               ("objects", phong_objects_spec(), {"phong_tessellation": True})],
+                               cam, [render])
 
 
 def material_zoo_spec(seed=7):
