@@ -39,6 +39,11 @@ WORKLOAD_JOBS = ("jobs128: 128 jobs over the 36-triangle Cornell box, random cam
 METRIC = "Mpaths/s"
 
 
+WORKLOAD_PHONG = ("heightfield_phong: 1024x512, 16 spp, num_path_vertices 18; the heightfield workload's 522k-triangle "
+                  "floor and 4 lights as triangles, its 2000 spheres as 160,000 Phong tessellation patches "
+                  "(80-face icospheres with radial vertex normals, FP64 patch test)")
+
+
 def env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -56,6 +61,10 @@ def scene_path(rank, world, dist, workload="heightfield"):
     elif workload in ("door", "c5"):
         d, p = workload_dir(workload)
         writer = lambda: scenes.write_guided_workload(workload, d, spp=WORKLOAD_SPP[workload])
+    elif workload == "phong":
+        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_phong_v1")
+        p = os.path.join(d, "heightfield_phong.json")
+        writer = lambda: scenes.write_heightfield_phong(d)
     else:
         d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_heightfield_v1")
         p = os.path.join(d, "heightfield_spheres.json")
@@ -305,12 +314,13 @@ def main():
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven launches instead of one graph per render (profiling runs: ncu does not "
                          "profile kernels inside conditional graph nodes)")
-    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128", "door", "c5"],
+    ap.add_argument("--workload", default="heightfield", choices=["heightfield", "jobs128", "door", "c5", "phong"],
                     help="heightfield: the 1M-triangle single render (headline); jobs128: 128 batched jobs "
                          "over the Cornell box, one graph launch per step; door: one guided render (learned "
                          "proposal trained on its first 32 spp) of the 200k-triangle door-gap room at 256 spp; "
                          "c5: one plain render of the 10M-triangle full combination at 3840x2160, 1024 spp, "
-                         "with the guided-vs-plain study on it")
+                         "with the guided-vs-plain study on it; phong: the heightfield scene with its spheres "
+                         "as Phong tessellation patches, 16 spp")
     args = ap.parse_args()
 
     world = env_int("WORLD_SIZE", 1)
@@ -470,7 +480,8 @@ def main():
             "config": {"workload": {"heightfield": WORKLOAD, "jobs128": WORKLOAD_JOBS,
                                     "door": DOOR_WORKLOAD + ", 256 spp, guided (learned proposal trained on its "
                                                             "first 32 spp)",
-                                    "c5": C5_WORKLOAD + ", 1024 spp, plain NEE+MIS"}[args.workload],
+                                    "c5": C5_WORKLOAD + ", 1024 spp, plain NEE+MIS",
+                                    "phong": WORKLOAD_PHONG}[args.workload],
                        "parallelism": "replicas x%d, FP64 film reduce" % world,
                        "autotuned": tune, "autotune_probe_ms": tune_ms,
                        "l2": "256 MB buffer written between timed steps; path state > L2",

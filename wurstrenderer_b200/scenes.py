@@ -433,6 +433,27 @@ def write_heightfield_spheres(out_dir, name="heightfield_spheres", resolution=(1
     return write_scene(out_dir, name, spec, cam, [nee_render(name + ".pfm", spp, num_path_vertices)])
 
 
+def write_heightfield_phong(out_dir, name="heightfield_phong", resolution=(1024, 512), spp=16,
+                            num_path_vertices=18, seed=1002, n_spheres=2000):
+    """The heightfield workload with its spheres as Phong tessellation patches: the fBm floor
+    and the lights stay triangles (first mesh entry); the 2000 spheres are 80-face icospheres
+    with their exact (radial) vertex normals in a "phong_tessellation": true entry."""
+    spec = heightfield_spheres_spec(seed, sphere_subdiv=1, n_spheres=n_spheres)
+    base, smooth = SceneSpec(), SceneSpec()
+    for m in spec.meshes:
+        mat = spec.materials[m.material]
+        if m.name.startswith("sphere"):
+            c = m.positions.astype(np.float64).mean(axis=0)
+            n = m.positions.astype(np.float64) - c
+            n /= np.linalg.norm(n, axis=1, keepdims=True)
+            smooth.add(m.name, mat, m.positions, m.triangles, normals=n.astype(np.float32))
+        else:
+            base.add(m.name, mat, m.positions, m.triangles)
+    cam = dict(HEIGHTFIELD_CAMERA, resolution=list(resolution))
+    return write_scene_entries(out_dir, name, [("base", base, None), ("spheres", smooth, {"phong_tessellation": True})],
+                               cam, [nee_render(name + ".pfm", spp, num_path_vertices)])
+
+
 def batch_jobs(seed=1003, n_jobs=128, num_path_vertices=14):
     """Workload C3 job table: random cameras inside the Cornell box looking at a box centre."""
     rng = np.random.default_rng(seed)
