@@ -310,6 +310,8 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs only)")
     ap.add_argument("--quick", action="store_true", help="skip e2e, profile and CPU baseline (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="use the default wavefront settings")
+    ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8],
+                    help="2: binary BVH, 8: compressed 8-wide BVH, 0: the library default")
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time study")
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven launches instead of one graph per render (profiling runs: ncu does not "
@@ -345,7 +347,7 @@ def main():
     path = scene_path(rank, world, dist, args.workload)
 
     t0 = time.perf_counter()
-    scene = wr.Scene.from_file(path)
+    scene = wr.Scene.from_file(path, bvh_width=args.bvh_width)
     load_s = time.perf_counter() - t0
     info = scene.info
     W, H = info["width"], info["height"]
@@ -488,6 +490,7 @@ def main():
                        "queue_capacity": prof["queue_capacity"], "grid_trace": prof["grid_trace"],
                        "grid_shade": prof["grid_shade"], "scene_load_s": load_s,
                        "bvh_nodes": info["bvh_nodes"], "bvh_depth": info["bvh_depth"],
+                       "bvh_width": args.bvh_width or "library default",
                        "iterations_per_step": iters / args.steps, "wall_ms_per_step": wall_ms / args.steps},
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

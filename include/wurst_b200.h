@@ -119,10 +119,15 @@ typedef struct wr_scene_info {
 #define WR_BVH_HOST_SAH 0       /* binned SAH on the host, <= max_leaf triangles per leaf (default) */
 #define WR_BVH_DEVICE_LBVH 1    /* linear BVH built on the device (Morton codes, radix sort, Karras 2012) */
 
+#define WR_BVH_WIDTH_DEFAULT 2 /* bvh_width 0 selects this */
+
 typedef struct wr_scene_options {
     int bvh_builder;         /* WR_BVH_HOST_SAH or WR_BVH_DEVICE_LBVH */
-    int max_leaf;            /* host SAH: triangles per leaf, 1..16 (0 = 4) */
-    int reserved[6];
+    int max_leaf;            /* host SAH: triangles per leaf, 1..16 (0 = 4; 3 for the 8-wide tree) */
+    int bvh_width;           /* 2: binary BVH (64-byte nodes); 8: compressed 8-wide BVH (80-byte
+                                nodes, 8-bit quantised child boxes, <= 3 triangles per leaf);
+                                0: WR_BVH_WIDTH_DEFAULT */
+    int reserved[5];
 } wr_scene_options;
 
 /* Parses a simple2 scene JSON (Simple2Parser::Parse, src/sceneio/simple2parser.h:84-100),

@@ -69,6 +69,23 @@ def test_image_matches_reference(wr_lib, name):
     assert abs(img.mean() / ref_a.mean() - 1.0) < 0.01
 
 
+@pytest.mark.parametrize("name", ["hf", "phong"])
+def test_wide_bvh_image_matches_reference(wr_lib, name):
+    """Renders through the compressed 8-wide BVH pass the same image bar."""
+    path, meta = golden_scene(name)
+    ref_a = np.load("%s/%s_ref_hi_a.npy" % (GOLDEN, name)).astype(np.float64)
+    ref_b = np.load("%s/%s_ref_hi_b.npy" % (GOLDEN, name)).astype(np.float64)
+    spp = meta["hi_spp"] // K
+    with wr_lib.Scene.from_file(path, bvh_width=8) as sc:
+        runs = np.stack([sc.render(spp=spp, seed=2000 + i) for i in range(K)])
+    img = runs.mean(axis=0)
+    floor = relmse(ref_b, ref_a)
+    err = relmse(img, ref_a)
+    assert err <= 2.0 * floor + 1e-6, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
+    z = block_z(runs, ref_a)
+    assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
+
+
 def test_graph_and_plain_launches_agree(wr_lib):
     path, _ = golden_scene("zoo")
     with wr_lib.Scene.from_file(path) as sc:

@@ -44,6 +44,31 @@ def test_closest_hit_ids_match_reference(wr_lib, oracle_lib, name):
 
 
 @pytest.mark.parametrize("name", FIXTURES)
+def test_wide_bvh_hits_match_reference(wr_lib, oracle_lib, name):
+    """The compressed 8-wide BVH gives the same closest hits and occlusion answers as the binary
+    one (the tree changes which boxes are visited, never the accepted hit)."""
+    path, _ = golden_scene(name)
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name))
+    hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
+    with wr_lib.Scene.from_file(path, bvh_width=8) as sc:
+        g, p, t, uv = sc.trace_closest(rays)
+        occ = sc.trace_occluded(rays)
+    with wr_lib.Scene.from_file(path, bvh_width=2) as sb:
+        g2, p2, t2, uv2 = sb.trace_closest(rays)
+        occ2 = sb.trace_occluded(rays)
+    _, _, _, uv_ref = oracle_lib.OracleScene(path).trace_closest(rays)
+    t_ref = hits[:, 2].view(np.float32)
+    same = (g == hits[:, 0]) & (p == hits[:, 1])
+    bad = ~same & ~_tie_or_edge(t_ref, t, uv_ref)
+    assert bad.sum() == 0, "mismatching rays: %s" % np.nonzero(bad)[0][:10]
+    both = (g == g2) & (p == p2)
+    assert np.array_equal(t[both], t2[both])
+    # the two trees test tied candidates (a ray through a shared edge) in different orders
+    assert (~both & ~_tie_or_edge(t2, t, uv_ref)).sum() == 0
+    assert (occ != occ2).sum() <= max(1, int(0.002 * len(rays)))
+
+
+@pytest.mark.parametrize("name", FIXTURES)
 def test_occlusion_matches_oracle(wr_lib, oracle_lib, name):
     path, _ = golden_scene(name)
     rays = np.load("%s/%s_rays.npy" % (GOLDEN, name)).copy()

@@ -79,7 +79,8 @@ class SceneInfo(ctypes.Structure):
 
 
 class SceneOptions(ctypes.Structure):
-    _fields_ = [("bvh_builder", ctypes.c_int), ("max_leaf", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+    _fields_ = [("bvh_builder", ctypes.c_int), ("max_leaf", ctypes.c_int), ("bvh_width", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
 
 
 BVH_HOST_SAH = 0
@@ -159,12 +160,15 @@ class Scene:
         self._h = handle
 
     @classmethod
-    def from_file(cls, json_path: str, bvh_builder: int = BVH_HOST_SAH, max_leaf: int = 0) -> "Scene":
+    def from_file(cls, json_path: str, bvh_builder: int = BVH_HOST_SAH, max_leaf: int = 0,
+                  bvh_width: int = 0) -> "Scene":
+        """bvh_width: 2 binary BVH, 8 compressed 8-wide BVH, 0 the library default."""
         L = load_library()
         h = ctypes.c_void_p()
         opts = SceneOptions()
         opts.bvh_builder = int(bvh_builder)
         opts.max_leaf = int(max_leaf)
+        opts.bvh_width = int(bvh_width)
         _check(L.wr_scene_create_ex(os.fspath(json_path).encode(), ctypes.byref(opts), ctypes.byref(h)))
         return cls(h)
 

@@ -269,4 +269,178 @@ BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_lea
     return res;
 }
 
+// ------------------------------------------------------------------------
+// Compressed 8-wide BVH (after Ylitie, Karras and Laine, "Efficient incoherent ray traversal on
+// GPUs through compressed wide BVHs", HPG 2017), collapsed from the binary tree above.
+//
+// Node = 80 bytes = 5 x uint4 (words):
+//   0-2  p.xyz: origin of the child-box grid (the node box's lower corner), float
+//   3    e.x | e.y << 8 | e.z << 16 | imask << 24: grid scale 2^(e-127) per axis (biased
+//        float exponents); imask bit s: slot s holds an inner node
+//   4    first inner child (inner children are stored contiguously in slot order)
+//   5    first triangle (leaf triangles of all leaf slots are stored contiguously)
+//   6-7  meta byte per slot: leaf = count (1..3) << 5 | offset from word 5; else 0
+//   8-13 quantised lower bounds: 8 bytes x, 8 bytes y, 8 bytes z
+//   14-19 quantised upper bounds: 8 bytes x, 8 bytes y, 8 bytes z
+// Child box along x: [p.x + lo_q * 2^(e.x-127), p.x + hi_q * 2^(e.x-127)], rounded outward; empty
+// slots carry lo_q = 255 > hi_q = 0 and are never entered.
+// Slot s holds the child that a ray of direction octant s (bit k: negative component k) should
+// visit first: children are assigned greedily by the least dot(child centre - node centre,
+// octant direction). A ray of octant o then visits its hit inner children in order of slot ^ o.
+namespace {
+
+struct WChild {
+    Aabb box;
+    int32_t code;   // binary inner node (>= 0) or leaf code (bit 31 set)
+};
+
+Aabb binary_child_box(const float *o, int slot) {
+    Aabb b;
+    const float *xy = o + (slot == 0 ? 0 : 4);
+    b.lo[0] = xy[0]; b.hi[0] = xy[1]; b.lo[1] = xy[2]; b.hi[1] = xy[3];
+    b.lo[2] = o[8 + 2 * slot]; b.hi[2] = o[9 + 2 * slot];
+    return b;
+}
+
+}  // namespace
+
+WideBvh build_wide8(const BvhBuildResult &bin) {
+    WideBvh w;
+    const size_t nbin = bin.nodes.size() / 16;
+    if (nbin == 0) return w;
+    struct Work { int bnode; uint32_t wnode; int depth; };
+    std::vector<Work> work{{0, 0u, 1}};
+    w.nodes.assign(20, 0u);
+    auto children_of = [&](int b, std::vector<WChild> &out) {
+        const float *o = &bin.nodes[size_t(b) * 16];
+        int32_t code[2];
+        memcpy(&code[0], &o[12], 4);
+        memcpy(&code[1], &o[13], 4);
+        for (int s = 0; s < 2; ++s) {
+            const Aabb bx = binary_child_box(o, s);
+            if (!(bx.lo[0] <= bx.hi[0]) || bx.lo[0] == INFINITY) continue;   // empty slot
+            out.push_back(WChild{bx, code[s]});
+        }
+    };
+    while (!work.empty()) {
+        const Work it = work.back();
+        work.pop_back();
+        w.depth = std::max(w.depth, it.depth);
+        std::vector<WChild> ch;
+        children_of(it.bnode, ch);
+        // open the inner child of largest area until 8 children
+        while (ch.size() < 8) {
+            int best = -1;
+            double best_area = -1.0;
+            for (size_t i = 0; i < ch.size(); ++i)
+                if (ch[i].code >= 0 && ch[i].box.half_area() > best_area) {
+                    best = int(i);
+                    best_area = ch[i].box.half_area();
+                }
+            if (best < 0) break;
+            std::vector<WChild> sub;
+            children_of(ch[size_t(best)].code, sub);
+            if (ch.size() - 1 + sub.size() > 8) break;
+            ch.erase(ch.begin() + best);
+            ch.insert(ch.end(), sub.begin(), sub.end());
+        }
+        Aabb nb;
+        for (const WChild &c : ch) nb.grow(c.box);
+        // slot assignment by octant
+        int slot_of[8], child_in[8];
+        for (int i = 0; i < 8; ++i) { slot_of[i] = -1; child_in[i] = -1; }
+        {
+            double cost[8][8];
+            for (size_t i = 0; i < ch.size(); ++i) {
+                double v[3];
+                for (int k = 0; k < 3; ++k)
+                    v[k] = 0.5 * (double(ch[i].box.lo[k]) + ch[i].box.hi[k]) - 0.5 * (double(nb.lo[k]) + nb.hi[k]);
+                for (int s = 0; s < 8; ++s)
+                    cost[i][s] = ((s & 1) ? -v[0] : v[0]) + ((s & 2) ? -v[1] : v[1]) + ((s & 4) ? -v[2] : v[2]);
+            }
+            for (size_t n = 0; n < ch.size(); ++n) {
+                double bc = INFINITY;
+                int bi = -1, bs = -1;
+                for (size_t i = 0; i < ch.size(); ++i) {
+                    if (slot_of[i] >= 0) continue;
+                    for (int s = 0; s < 8; ++s)
+                        if (child_in[s] < 0 && cost[i][s] < bc) { bc = cost[i][s]; bi = int(i); bs = s; }
+                }
+                if (bi < 0) {   // NaN costs: any free slot
+                    for (size_t i = 0; i < ch.size() && bi < 0; ++i)
+                        if (slot_of[i] < 0) bi = int(i);
+                    for (int s = 0; s < 8 && bs < 0; ++s)
+                        if (child_in[s] < 0) bs = s;
+                }
+                slot_of[bi] = bs;
+                child_in[bs] = bi;
+            }
+        }
+        uint32_t *o = &w.nodes[size_t(it.wnode) * 20];
+        // grid: origin at the node's lower corner, per-axis power-of-two scale with 255 steps
+        int e[3];
+        for (int k = 0; k < 3; ++k) {
+            const double ext = double(nb.hi[k]) - double(nb.lo[k]);
+            int ex = -126;
+            if (ext > 0.0) {
+                frexp(ext / 255.0, &ex);   // ext / 255 < 2^ex
+                ex = std::max(ex, -126);
+            }
+            e[k] = ex + 127;
+            if (e[k] > 254) throw Error(WR_ERR_UNSUPPORTED, "scene extent too large for the compressed BVH");
+            memcpy(&o[k], &nb.lo[k], 4);
+        }
+        uint32_t imask = 0, n_inner = 0;
+        for (int s = 0; s < 8; ++s)
+            if (child_in[s] >= 0 && ch[size_t(child_in[s])].code >= 0) { imask |= 1u << s; ++n_inner; }
+        o[3] = uint32_t(e[0]) | uint32_t(e[1]) << 8 | uint32_t(e[2]) << 16 | imask << 24;
+        const uint32_t base_child = uint32_t(w.nodes.size() / 20);
+        const uint32_t base_tri = uint32_t(w.order.size());
+        o[4] = base_child;
+        o[5] = base_tri;
+        uint8_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0}, qlo[3][8], qhi[3][8];
+        for (int s = 0; s < 8; ++s)
+            for (int k = 0; k < 3; ++k) { qlo[k][s] = 255; qhi[k][s] = 0; }
+        uint32_t next_inner = 0;
+        std::vector<Work> pushes;
+        for (int s = 0; s < 8; ++s) {
+            if (child_in[s] < 0) continue;
+            const WChild &c = ch[size_t(child_in[s])];
+            for (int k = 0; k < 3; ++k) {
+                const double scale = std::ldexp(1.0, e[k] - 127);
+                const double p = double(nb.lo[k]);
+                double ql = std::floor((double(c.box.lo[k]) - p) / scale);
+                double qh = std::ceil((double(c.box.hi[k]) - p) / scale);
+                ql = std::min(std::max(ql, 0.0), 255.0);
+                qh = std::min(std::max(qh, 0.0), 255.0);
+                while (ql > 0.0 && p + ql * scale > double(c.box.lo[k])) ql -= 1.0;
+                while (qh < 255.0 && p + qh * scale < double(c.box.hi[k])) qh += 1.0;
+                qlo[k][s] = uint8_t(ql);
+                qhi[k][s] = uint8_t(qh);
+            }
+            if (c.code >= 0) {
+                pushes.push_back(Work{c.code, base_child + next_inner, it.depth + 1});
+                ++next_inner;
+            } else {
+                const uint32_t code = uint32_t(c.code);
+                const uint32_t first = code & 0x07ffffffu, count = ((code >> 27) & 0xfu) + 1u;
+                if (count > 3) throw Error(WR_ERR_UNSUPPORTED, "compressed BVH leaves hold at most 3 triangles");
+                const uint32_t off = uint32_t(w.order.size()) - base_tri;
+                for (uint32_t t = first; t < first + count; ++t) w.order.push_back(bin.tri_order[t]);
+                meta[s] = uint8_t(count << 5 | off);
+            }
+        }
+        uint32_t *on = &w.nodes[size_t(it.wnode) * 20];   // (o may be stale after the resize below)
+        memcpy(&on[6], meta, 8);
+        for (int k = 0; k < 3; ++k) {
+            memcpy(&on[8 + 2 * k], qlo[k], 8);
+            memcpy(&on[14 + 2 * k], qhi[k], 8);
+        }
+        w.nodes.resize(w.nodes.size() + size_t(n_inner) * 20, 0u);
+        for (auto pw = pushes.rbegin(); pw != pushes.rend(); ++pw) work.push_back(*pw);
+    }
+    if (w.nodes.size() / 20 >= (1u << 24)) throw Error(WR_ERR_UNSUPPORTED, "more than 2^24 compressed BVH nodes");
+    return w;
+}
+
 }  // namespace wr

@@ -78,7 +78,7 @@ struct wr_scene {
     cudaStream_t stream = nullptr;
     int device = 0;
     // scene data
-    DevBuf nodes, tris, patches, tri_mat, materials, lights, light_tris, light_tri_cdf, light_tri_pdf, light_cdf, light_pdf;
+    DevBuf nodes, wnodes, tris, patches, tri_mat, materials, lights, light_tris, light_tri_cdf, light_tri_pdf, light_cdf, light_pdf;
     uint32_t num_patches = 0;
     DevBuf env_texels, env_pixel_pdf, env_row_cdf, env_row_pdf, env_col_cdf, env_col_pdf;
     wrd::DevScene dev{};
@@ -238,15 +238,26 @@ void build_device_scene(wr_scene &s) {
         }
     }
     const std::vector<float> &build_in = npatch ? bvh_verts : verts;
+    const bool wide = s.opts.bvh_width == 8;
     wr::BvhBuildResult bvh;
     const auto tb = std::chrono::steady_clock::now();
     if (s.opts.bvh_builder == WR_BVH_DEVICE_LBVH) {
         bvh = wr::build_bvh_lbvh(build_in, st, &s.bvh_ms);
     } else {
-        bvh = wr::build_bvh_sah(build_in, s.opts.max_leaf > 0 ? s.opts.max_leaf : 4, 0);
+        // the compressed 8-wide tree encodes at most 3 triangles per leaf
+        const int ml = s.opts.max_leaf > 0 ? s.opts.max_leaf : (wide ? 3 : 4);
+        bvh = wr::build_bvh_sah(build_in, wide ? std::min(ml, 3) : ml, 0);
         s.bvh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
     }
-    s.bvh_nodes = int(bvh.nodes.size() / 16);
+    wr::WideBvh wbvh;
+    if (wide) {
+        const auto tw = std::chrono::steady_clock::now();
+        wbvh = wr::build_wide8(bvh);
+        s.bvh_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
+        bvh.tri_order = wbvh.order;   // leaf order of the wide tree
+        bvh.depth = wbvh.depth;
+    }
+    s.bvh_nodes = wide ? int(wbvh.nodes.size() / 20) : int(bvh.nodes.size() / 16);
     s.bvh_depth = bvh.depth;
     s.sah_cost = bvh.sah_cost;
     if (bvh.depth > wrd::kMaxStack) throw Error(WR_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
@@ -269,7 +280,8 @@ void build_device_scene(wr_scene &s) {
             memcpy(pd + 9, &box_out[6 * size_t(g)], 24);
         }
     }
-    upload(s.nodes, bvh.nodes, st);
+    if (wide) upload(s.wnodes, wbvh.nodes, st);
+    else upload(s.nodes, bvh.nodes, st);
     upload(s.tris, trisf, st);
     upload(s.tri_mat, leaf_mat, st);
     s.num_patches = npatch;
@@ -365,7 +377,8 @@ void build_device_scene(wr_scene &s) {
     upload(s.light_tris, ltris, st);
 
     wrd::DevScene &d = s.dev;
-    d.nodes = s.nodes.as<float4>();
+    d.nodes = wide ? nullptr : s.nodes.as<float4>();
+    d.wnodes = wide ? s.wnodes.as<uint4>() : nullptr;
     d.tris = s.tris.as<float4>();
     d.patches = npatch ? s.patches.as<double>() : nullptr;
     d.tri_mat = s.tri_mat.as<uint32_t>();
@@ -601,7 +614,7 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     r.iter_limit = uint32_t(std::min<unsigned long long>((waves + 2) * (unsigned long long)(max_nverts + 2) + 64,
                                                          0xffffffffull));
     r.trace_block = (desc.trace_block == 64 || desc.trace_block == 256) ? desc.trace_block : 128;
-    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block, s.dev.patches != nullptr));
+    r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block, s.dev.patches != nullptr, s.dev.wnodes != nullptr));
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * std::max(1, wrk::occupancy_blocks(1));
 
     const int profile = desc.profile;
@@ -1077,6 +1090,9 @@ std::unique_ptr<wr_scene> create(wr::Scene &&host, const wr_scene_options *opts 
     if (opts) s->opts = *opts;
     if (s->opts.bvh_builder != WR_BVH_HOST_SAH && s->opts.bvh_builder != WR_BVH_DEVICE_LBVH)
         throw Error(WR_ERR_INVALID_ARGUMENT, "unknown bvh_builder");
+    if (s->opts.bvh_width == 0) s->opts.bvh_width = WR_BVH_WIDTH_DEFAULT;
+    if (s->opts.bvh_width != 2 && s->opts.bvh_width != 8)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "bvh_width must be 2 or 8");
     s->host = std::move(host);
     build_device_scene(*s);
     return s;
@@ -1307,7 +1323,7 @@ int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_rende
         }
         // 3) persistent-CTA count of the traversal and shading kernels
         const int blk = (cur.trace_block == 64 || cur.trace_block == 256) ? cur.trace_block : 128;
-        const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk, s->dev.patches != nullptr));
+        const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk, s->dev.patches != nullptr, s->dev.wnodes != nullptr));
         const int occ_s = sms * std::max(1, wrk::occupancy_blocks(1));
         for (double f : {0.5, 1.0}) {
             wr_render_desc d = cur;

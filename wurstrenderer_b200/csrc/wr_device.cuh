@@ -92,7 +92,8 @@ constexpr int INTEGRATOR_PRIMITIVE = 1;  // primitive_path_tracer (src/renderer/
 constexpr int INTEGRATOR_LIGHT = 2;      // light_splatting (src/renderer/lightsplatting.h)
 
 struct DevScene {
-    const float4 *nodes;
+    const float4 *nodes;            // binary BVH (4 x float4 per node)
+    const uint4 *wnodes;            // compressed 8-wide BVH (5 x uint4 per node), nullptr when binary
     const float4 *tris;             // leaf order: p0, p1, p2 (.w: index | patch flag, mesh, primitive)
     const double *patches;          // Phong tessellation patches (wrp::kPatchDoubles per leaf primitive),
                                     // nullptr when the scene has none

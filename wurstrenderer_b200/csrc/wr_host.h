@@ -103,4 +103,13 @@ struct BvhBuildResult {
 };
 BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_leaf, int threads);
 
+// Compressed 8-wide BVH collapsed from a binary one whose leaves hold at most 3 triangles
+// (layout in wr_bvh.cpp); `order` is the new leaf order -> global triangle index.
+struct WideBvh {
+    std::vector<uint32_t> nodes;     // 20 words (80 bytes) per node
+    std::vector<uint32_t> order;
+    int depth = 0;
+};
+WideBvh build_wide8(const BvhBuildResult &binary);
+
 }  // namespace wr

@@ -378,7 +378,7 @@ __device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c)
 //   SHADOW = true:  shadow -- any hit of every queued shadow ray; unoccluded contributions
 //                   are added to the FP64 film (and to the path's training records)
 
-template <int BLOCK, bool SHADOW, bool PHONG>
+template <int BLOCK, bool SHADOW, bool PHONG, bool WIDE>
 __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w, uint32_t *stack) {
     const uint32_t n = SHADOW ? min(w.ctr[CTR_SHADOW], w.shadow_capacity) : w.ctr[CTR_ACTIVE];
     uint32_t *fetch = w.ctr + (SHADOW ? CTR_SHADOW_FETCH : CTR_EXTEND_FETCH);
@@ -391,6 +391,8 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
     float t = 0.f, bu = 0.f, bv = 0.f;
     uint32_t tri = MISS, ray = 0, nv = 0, nt = 0;
     int node = kTraceDone, leaf = 0;
+    WideState ws{-1, 0u, 0u, 0u};   // WIDE: compressed 8-wide traversal state
+    uint32_t oct = 0;
     bool busy = false, exhausted = false;
     const uint32_t lane = lane_id();
     while (true) {
@@ -409,6 +411,10 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
                     else { o = w.cur.o[ray]; d = w.cur.d[ray]; tmax = __int_as_float(0x7f800000); }
                     r = ray_setup(xyz(o), xyz(d));
                     if (PHONG) pr = PatchRay{o.x, o.y, o.z, d.x, d.y, d.z};
+                    if (WIDE) {
+                        ws = WideState{0, 0u, 0u, 0u};
+                        oct = ray_octant(xyz(d));
+                    }
                     t = tmax; tri = MISS; bu = 0.f; bv = 0.f;
                     node = 0; leaf = 0; st.sp = 0;
                     busy = true;
@@ -419,8 +425,16 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
         }
         if (!__any_sync(0xffffffffu, busy)) break;
         const int min_active = __any_sync(0xffffffffu, exhausted) ? 0 : w.fetch_min;
-        if (busy && traverse_steps<SHADOW, PHONG>(s.nodes, s.tris, r, kRayEps, t, tri, bu, bv, node, leaf, st, nv,
-                                                  nt, min_active, s.patches, pr)) {
+        bool finished = false;
+        if (busy) {
+            if (WIDE)
+                finished = traverse_steps_w8<SHADOW, PHONG>(s.wnodes, s.tris, r, oct, kRayEps, t, tri, bu, bv, ws, st,
+                                                             nv, nt, min_active, s.patches, pr);
+            else
+                finished = traverse_steps<SHADOW, PHONG>(s.nodes, s.tris, r, kRayEps, t, tri, bu, bv, node, leaf, st,
+                                                          nv, nt, min_active, s.patches, pr);
+        }
+        if (finished) {
             busy = false;
             if (SHADOW) {
                 if (tri == MISS) {   // unoccluded
@@ -440,10 +454,10 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
     }
 }
 
-template <int BLOCK, bool PHONG>
+template <int BLOCK, bool PHONG, bool WIDE>
 __global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    trace_queue<BLOCK, false, PHONG>(s, w, stack);
+    trace_queue<BLOCK, false, PHONG, WIDE>(s, w, stack);
 }
 
 // lens point of a sample's camera vertex (ThinlensCamera::sampleWe0ByPdf, thinlens.h:121-136; the
@@ -886,10 +900,10 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
     }
 }
 
-template <int BLOCK, bool PHONG>
+template <int BLOCK, bool PHONG, bool WIDE>
 __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    trace_queue<BLOCK, true, PHONG>(s, w, stack);
+    trace_queue<BLOCK, true, PHONG, WIDE>(s, w, stack);
 }
 
 // queue bookkeeping between iterations (one thread); also drives the graph's while loop
@@ -937,7 +951,7 @@ __global__ void k_resolve(const double *film, double *out, uint32_t total_pix, c
 // out: 3 float4 per ray -- (geomID, primID, t, leaf index), (u, v, 0, 0) with the triangle's
 // barycentrics (zero on a patch, whose texture coordinate the reference leaves at zero), and
 // (unit geometry normal, 0)
-template <bool PHONG>
+template <bool PHONG, bool WIDE>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_batch(DevScene s, const float4 *rays, uint32_t n, int any_hit,
                                                            float4 *out, uint32_t *visits) {
     __shared__ uint32_t stack[kSmemStack * kTraceBlock];
@@ -947,7 +961,13 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_batch(DevScene s, const f
         float t, bu = 0.f, bv = 0.f;
         uint32_t tri;
         bool hit;
-        if (any_hit)
+        if (WIDE && any_hit)
+            hit = traverse_w8<true, PHONG>(s.wnodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv,
+                                           &nt, s.patches);
+        else if (WIDE)
+            hit = traverse_w8<false, PHONG>(s.wnodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv,
+                                            &nt, s.patches);
+        else if (any_hit)
             hit = traverse<true, PHONG>(s.nodes, s.tris, xyz(a), xyz(b), a.w, b.w, stack, t, tri, bu, bv, &nv, &nt,
                                         s.patches);
         else
@@ -1074,21 +1094,33 @@ static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &
     return w;
 }
 
+// the traversal kernel instantiation for the scene: block size x (Phong patches) x (BVH width)
+template <int BLOCK, bool SHADOW, bool PHONG, bool WIDE>
+void launch_trace_4(const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
+    if (SHADOW) k_shadow<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w);
+    else k_extend<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w);
+}
+
+template <int BLOCK, bool SHADOW>
+void launch_trace_3(const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
+    if (s.patches && s.wnodes) launch_trace_4<BLOCK, SHADOW, true, true>(s, w, r, st);
+    else if (s.patches) launch_trace_4<BLOCK, SHADOW, true, false>(s, w, r, st);
+    else if (s.wnodes) launch_trace_4<BLOCK, SHADOW, false, true>(s, w, r, st);
+    else launch_trace_4<BLOCK, SHADOW, false, false>(s, w, r, st);
+}
+
+template <bool SHADOW>
+void launch_trace(const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
+    if (r.trace_block == 64) launch_trace_3<64, SHADOW>(s, w, r, st);
+    else if (r.trace_block == 256) launch_trace_3<256, SHADOW>(s, w, r, st);
+    else launch_trace_3<128, SHADOW>(s, w, r, st);
+}
+
 void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
                    cudaStream_t st) {
     const WaveArgs w = make_args(b, parity, r);
     switch (which) {
-        case KERNEL_EXTEND:
-            if (s.patches) {
-                if (r.trace_block == 64) k_extend<64, true><<<r.grid_trace, 64, 0, st>>>(s, w);
-                else if (r.trace_block == 256) k_extend<256, true><<<r.grid_trace, 256, 0, st>>>(s, w);
-                else k_extend<128, true><<<r.grid_trace, 128, 0, st>>>(s, w);
-            } else {
-                if (r.trace_block == 64) k_extend<64, false><<<r.grid_trace, 64, 0, st>>>(s, w);
-                else if (r.trace_block == 256) k_extend<256, false><<<r.grid_trace, 256, 0, st>>>(s, w);
-                else k_extend<128, false><<<r.grid_trace, 128, 0, st>>>(s, w);
-            }
-            break;
+        case KERNEL_EXTEND: launch_trace<false>(s, w, r, st); break;
         case KERNEL_SHADE:
             if (w.lobes) k_shade<true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
             else k_shade<false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
@@ -1099,17 +1131,7 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
                                            b.lobes, b.capacity, r.guide_sms, st);
             break;
         case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
-        case KERNEL_SHADOW:
-            if (s.patches) {
-                if (r.trace_block == 64) k_shadow<64, true><<<r.grid_trace, 64, 0, st>>>(s, w);
-                else if (r.trace_block == 256) k_shadow<256, true><<<r.grid_trace, 256, 0, st>>>(s, w);
-                else k_shadow<128, true><<<r.grid_trace, 128, 0, st>>>(s, w);
-            } else {
-                if (r.trace_block == 64) k_shadow<64, false><<<r.grid_trace, 64, 0, st>>>(s, w);
-                else if (r.trace_block == 256) k_shadow<256, false><<<r.grid_trace, 256, 0, st>>>(s, w);
-                else k_shadow<128, false><<<r.grid_trace, 128, 0, st>>>(s, w);
-            }
-            break;
+        case KERNEL_SHADOW: launch_trace<true>(s, w, r, st); break;
         case KERNEL_ADVANCE: k_advance<<<1, 1, 0, st>>>(w); break;
         default: break;
     }
@@ -1134,8 +1156,10 @@ void launch_resolve(const double *film, double *out, const RenderLaunch &r, cuda
 
 void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,
                         int grid, cudaStream_t st) {
-    if (s.patches) k_trace_batch<true><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
-    else k_trace_batch<false><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+    if (s.patches && s.wnodes) k_trace_batch<true, true><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+    else if (s.patches) k_trace_batch<true, false><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+    else if (s.wnodes) k_trace_batch<false, true><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
+    else k_trace_batch<false, false><<<grid, kTraceBlock, 0, st>>>(s, rays, n, any_hit, out, visits);
 }
 
 void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t ntables, float *cdf, float *pdf,
@@ -1151,16 +1175,25 @@ void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n,
     k_scale_pdf<<<592, 256, 0, st>>>(weights, total, pdf, n);
 }
 
-int occupancy_blocks(int which, int trace_block, bool phong) {
+template <int BLOCK, bool PHONG, bool WIDE> int extend_occupancy() {
     int nb = 0;
-    if (which == 0 && phong) {
-        if (trace_block == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<64, true>, 64, 0);
-        else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256, true>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128, true>, 128, 0);
-    } else if (which == 0) {
-        if (trace_block == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<64, false>, 64, 0);
-        else if (trace_block == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<256, false>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<128, false>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<BLOCK, PHONG, WIDE>, BLOCK, 0);
+    return nb;
+}
+
+template <int BLOCK> int extend_occupancy_3(bool phong, bool wide) {
+    if (phong && wide) return extend_occupancy<BLOCK, true, true>();
+    if (phong) return extend_occupancy<BLOCK, true, false>();
+    if (wide) return extend_occupancy<BLOCK, false, true>();
+    return extend_occupancy<BLOCK, false, false>();
+}
+
+int occupancy_blocks(int which, int trace_block, bool phong, bool wide) {
+    int nb = 0;
+    if (which == 0) {
+        if (trace_block == 64) nb = extend_occupancy_3<64>(phong, wide);
+        else if (trace_block == 256) nb = extend_occupancy_3<256>(phong, wide);
+        else nb = extend_occupancy_3<128>(phong, wide);
     } else {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false>, kShadeBlock, 0);
     }

@@ -59,8 +59,8 @@ void launch_cdf_build(const double *weights, const uint32_t *offsets, uint32_t n
                       double *sums, cudaStream_t st);
 void launch_env_weights(const float4 *texels, int w, int h, double *out, cudaStream_t st);
 void launch_scale_pdf(const double *weights, double total, float *pdf, size_t n, cudaStream_t st);
-// resident blocks per SM of the extend (which 0; the Phong-patch variant with `phong`) or
-// shade (which 1) kernel
-int occupancy_blocks(int which, int trace_block = 128, bool phong = false);
+// resident blocks per SM of the extend (which 0; the variant for Phong patches and / or the
+// compressed 8-wide BVH) or shade (which 1) kernel
+int occupancy_blocks(int which, int trace_block = 128, bool phong = false, bool wide = false);
 
 }  // namespace wrk

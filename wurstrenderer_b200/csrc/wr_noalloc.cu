@@ -167,7 +167,7 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
     r.iter_limit = uint32_t((waves + 2) * (unsigned long long)(nverts + 2) + 64);
     r.trace_block = (desc.trace_block == 64 || desc.trace_block == 256) ? desc.trace_block : 128;
     r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace
-                                       : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block, v.dev.patches != nullptr));
+                                       : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block, v.dev.patches != nullptr, v.dev.wnodes != nullptr));
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * (wrk::occupancy_blocks(1) > 0 ? wrk::occupancy_blocks(1) : 1);
     r.has_cond = 0;
     r.prof = nullptr;

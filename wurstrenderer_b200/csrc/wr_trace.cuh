@@ -336,4 +336,162 @@ __device__ __forceinline__ bool traverse_steps(const float4 *__restrict__ nodes,
     return true;
 }
 
+// ------------------------------------------------------------------------
+// Traversal of the compressed 8-wide BVH (layout in wr_bvh.cpp: 80-byte nodes, child boxes
+// quantised to 8 bits on a per-node power-of-two grid, octant-ordered slots).
+//
+// Per node: the 8 child boxes are decoded in ray space, t = q * (scale / d) + (p - o) / d (one
+// FMA per plane), and slab-tested against (tmin, t]; the triangles of the hit leaf slots are
+// tested at once; the hit inner slots form a group visited in order slot ^ octant. The current
+// group is (node << 8 | remaining hit positions) with that node's first-child index and inner
+// mask in registers; a group with hits left is pushed when its first child is entered, and
+// re-read from its node when popped. Resumable like traverse_steps (state: next node, group,
+// stack), leaving after any node once fewer than `min_active` lanes of the warp are busy.
+struct WideState {
+    int node;            // next node to intersect, -1 when none
+    uint32_t grp;        // current group: node << 8 | hit positions left
+    uint32_t gbase;      // first inner child of the group's node
+    uint32_t gimask;     // inner slots of the group's node
+};
+
+// quantised byte k of an 8-byte lane (two words) as an exact float: the byte is placed in the
+// mantissa of 2^23 by one byte permute, and 2^23 is subtracted (exact for integers < 2^23)
+__device__ __forceinline__ float wq_byte(uint32_t lo, uint32_t hi, int k) {
+    return __uint_as_float(__byte_perm(k < 4 ? lo : hi, 0x4B000000u, 0x7540u | uint32_t(k & 3))) - 8388608.0f;
+}
+
+template <bool ANY_HIT, bool PHONG = false>
+__device__ __forceinline__ bool traverse_steps_w8(const uint4 *__restrict__ wnodes, const float4 *__restrict__ tris,
+                                                  const RayPre &r, uint32_t oct, float tmin, float &t, uint32_t &tri,
+                                                  float &bu, float &bv, WideState &ws, TraceStack &st, uint32_t &nv,
+                                                  uint32_t &nt, int min_active, const double *patches = nullptr,
+                                                  const PatchRay &pr = PatchRay{}) {
+    const bool negx = r.ix < 0.f, negy = r.iy < 0.f, negz = r.iz < 0.f;
+    while (true) {
+        if (ws.node >= 0) {
+            const uint4 n0 = __ldg(wnodes + 5 * ws.node + 0);
+            const uint4 n1 = __ldg(wnodes + 5 * ws.node + 1);
+            const uint4 n2 = __ldg(wnodes + 5 * ws.node + 2);
+            const uint4 n3 = __ldg(wnodes + 5 * ws.node + 3);
+            const uint4 n4 = __ldg(wnodes + 5 * ws.node + 4);
+            ++nv;
+            const float sx = __uint_as_float((n0.w & 0xffu) << 23) * r.ix;
+            const float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * r.iy;
+            const float sz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * r.iz;
+            const float ox = fmaf(__uint_as_float(n0.x), r.ix, -r.oix);
+            const float oy = fmaf(__uint_as_float(n0.y), r.iy, -r.oiy);
+            const float oz = fmaf(__uint_as_float(n0.z), r.iz, -r.oiz);
+            const uint32_t imask = n0.w >> 24;
+            // near / far quantised planes per axis (lo words: 8 bytes x, y, z; hi words likewise)
+            const uint32_t xnl = negx ? n3.z : n2.x, xnh = negx ? n3.w : n2.y;
+            const uint32_t xfl = negx ? n2.x : n3.z, xfh = negx ? n2.y : n3.w;
+            const uint32_t ynl = negy ? n4.x : n2.z, ynh = negy ? n4.y : n2.w;
+            const uint32_t yfl = negy ? n2.z : n4.x, yfh = negy ? n2.w : n4.y;
+            const uint32_t znl = negz ? n4.z : n3.x, znh = negz ? n4.w : n3.y;
+            const uint32_t zfl = negz ? n3.x : n4.z, zfh = negz ? n3.y : n4.w;
+            uint32_t hits = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float txn = fmaf(wq_byte(xnl, xnh, k), sx, ox), txf = fmaf(wq_byte(xfl, xfh, k), sx, ox);
+                const float tyn = fmaf(wq_byte(ynl, ynh, k), sy, oy), tyf = fmaf(wq_byte(yfl, yfh, k), sy, oy);
+                const float tzn = fmaf(wq_byte(znl, znh, k), sz, oz), tzf = fmaf(wq_byte(zfl, zfh, k), sz, oz);
+                const float tn = fmaxf(fmaxf(txn, tyn), fmaxf(tzn, tmin));
+                const float tf = fminf(fminf(txf, tyf), fminf(tzf, t));
+                if (tn <= tf * 1.0000005f) hits |= 1u << k;
+            }
+            // triangles of the hit leaf slots
+            uint32_t tmask = 0, inner = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (!(hits & (1u << k))) continue;
+                if (imask & (1u << k)) {
+                    inner |= 1u << (uint32_t(k) ^ oct);
+                } else {
+                    const uint32_t m = ((k < 4 ? n1.z : n1.w) >> (8 * (k & 3))) & 0xffu;
+                    tmask |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+                }
+            }
+            const uint32_t base_tri = n1.y;
+            while (tmask) {
+                const uint32_t i = base_tri + uint32_t(__ffs(tmask) - 1);
+                tmask &= tmask - 1u;
+                const float4 a = __ldg(tris + 3 * i + 0);
+                const float4 b = __ldg(tris + 3 * i + 1);
+                const float4 c = __ldg(tris + 3 * i + 2);
+                ++nt;
+                if (PHONG && (__float_as_uint(a.w) & wrp::kPatchFlag)) {
+                    if (patch_leaf_test(r, pr, patches, i, a, b, c, tmin, t, bu, bv)) {
+                        tri = i;
+                        if (ANY_HIT) {
+                            ws.node = -1;
+                            ws.grp = 0;
+                            st.sp = 0;
+                            return true;
+                        }
+                    }
+                    continue;
+                }
+                float th, uh, vh;
+                if (tri_test(r, a, b, c, tmin, t, th, uh, vh)) {
+                    if (ANY_HIT) {
+                        t = th; tri = i; bu = uh; bv = vh;
+                        ws.node = -1;
+                        ws.grp = 0;
+                        st.sp = 0;
+                        return true;
+                    }
+                    if (th < t || tri == MISS) { t = th; tri = i; bu = uh; bv = vh; }
+                }
+            }
+            if (inner) {
+                if (ws.grp & 0xffu) st.push(int(ws.grp));
+                ws.grp = uint32_t(ws.node) << 8 | inner;
+                ws.gbase = n1.x;
+                ws.gimask = imask;
+            }
+            ws.node = -1;
+        }
+        // next child: the lowest hit position of the current group, else a popped group
+        if (!(ws.grp & 0xffu)) {
+            if (!st.sp) return true;
+            ws.grp = uint32_t(st.pop());
+            const uint32_t pn = ws.grp >> 8;
+            const uint32_t *pw = reinterpret_cast<const uint32_t *>(wnodes + 5 * pn);
+            ws.gbase = __ldg(pw + 4);
+            ws.gimask = __ldg(pw + 3) >> 24;
+        }
+        const uint32_t pos = uint32_t(__ffs(ws.grp & 0xffu) - 1);
+        ws.grp &= ~(1u << pos);
+        const uint32_t slot = pos ^ oct;
+        ws.node = int(ws.gbase + __popc(ws.gimask & ((1u << slot) - 1u)));
+        if (__popc(__activemask()) < min_active) return false;
+    }
+}
+
+__device__ __forceinline__ uint32_t ray_octant(f3 d) {
+    return (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+}
+
+// one whole query on the compressed 8-wide BVH (the k_trace_batch path)
+template <bool ANY_HIT, bool PHONG = false>
+__device__ __forceinline__ bool traverse_w8(const uint4 *__restrict__ wnodes, const float4 *__restrict__ tris, f3 o,
+                                            f3 d, float tmin, float tmax, uint32_t *smem_stack, float &t,
+                                            uint32_t &tri, float &bu, float &bv, uint32_t *node_visits = nullptr,
+                                            uint32_t *tri_tests = nullptr, const double *patches = nullptr) {
+    const RayPre r = ray_setup(o, d);
+    const PatchRay pr{o.x, o.y, o.z, d.x, d.y, d.z};
+    TraceStack st;
+    st.smem = smem_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.sp = 0;
+    WideState ws{0, 0u, 0u, 0u};
+    tri = MISS;
+    t = tmax;
+    uint32_t nv = 0, nt = 0;
+    traverse_steps_w8<ANY_HIT, PHONG>(wnodes, tris, r, ray_octant(d), tmin, t, tri, bu, bv, ws, st, nv, nt, 0,
+                                      patches, pr);
+    if (node_visits) { *node_visits += nv; *tri_tests += nt; }
+    return tri != MISS;
+}
+
 }  // namespace wrd
