@@ -267,6 +267,12 @@ int wr_trace_stats(wr_scene *scene, const float *rays, int n, int any_hit, unsig
 /* PFM output in the reference's layout (FimageIo::SavePfmColor, src/common/floatimage.h:435-462). */
 int wr_write_pfm(const char *path, const double *rgb, int width, int height);
 
+/* Float image input as the scene loader reads environment maps (FimageIo::Load,
+ * src/common/floatimage.h:379-404): .pfm, .hdr (Radiance RGBE) or .exr (one-part scanline
+ * OpenEXR, HALF / FLOAT channels, uncompressed / RLE / ZIPS / ZIP). Writes the size; with rgb
+ * non-NULL also width * height * 3 floats, row 0 = top (call once with NULL to size the buffer). */
+int wr_read_image(const char *path, int *width, int *height, float *rgb);
+
 /* Whole simple2 flow of the reference CLI (src/main.cpp:5-15,
  * src/sceneio/simple2parser.h:102-223): load the scene, render every
  * "nextevent_path_tracer" entry of "render" and write its "output" PFM next

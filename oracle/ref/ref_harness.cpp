@@ -19,6 +19,7 @@
 //            [--crop x0 y0 x1 y1] [--serial] [--threads T] [--raw out.f64] [--camera '<json>']
 //   wurst_ref trace <scene.json> <rays.f32> <hits.bin>
 //   wurst_ref trace2 <scene.json> <rays.f32> <hits.bin>   (any geometry type; 8 words per ray)
+//   wurst_ref imgload <image.pfm|.hdr|.exr> <out.bin>     (the reference's FimageIo::Load)
 // `render` without --crop/--serial calls PathNeeRenderer::render() itself
 // (all hardware threads). --serial/--crop run the same per-tile loop as
 // render() (pathnextevent.h:152-191) over the selected tiles on --threads
@@ -385,6 +386,26 @@ int cmd_trace2(int argc, char **argv) {
     return 0;
 }
 
+// The reference's own image input (FimageIo::Load, src/common/floatimage.h:379-404: PFM, HDR via
+// stb_image, EXR via tinyexr): writes width, height (int32) and W*H*3 floats, row 0 = top.
+int cmd_imgload(int argc, char **argv) {
+    (void)argc;
+    Fimage<Spectrum> img = FimageIo::Load(filesystem::path(argv[2]));
+    const int W = img.mSize[0], H = img.mSize[1];
+    std::vector<float> out(size_t(W) * H * 3);
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < 3; ++c) out[3 * (size_t(y) * W + x) + c] = float(img.at(x, y)[c]);
+    FILE *f = fopen(argv[3], "wb");
+    if (!f) throw std::runtime_error("cannot write " + std::string(argv[3]));
+    const int32_t wh[2] = {W, H};
+    fwrite(wh, 4, 2, f);
+    fwrite(out.data(), 4, out.size(), f);
+    fclose(f);
+    printf("{\"width\": %d, \"height\": %d}\n", W, H);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -392,6 +413,7 @@ int main(int argc, char **argv) {
         if (argc >= 4 && std::string(argv[1]) == "render") return cmd_render(argc, argv);
         if (argc >= 5 && std::string(argv[1]) == "trace") return cmd_trace(argc, argv);
         if (argc >= 5 && std::string(argv[1]) == "trace2") return cmd_trace2(argc, argv);
+        if (argc >= 4 && std::string(argv[1]) == "imgload") return cmd_imgload(argc, argv);
         fprintf(stderr, "usage: wurst_ref render <scene.json> <out.pfm> [options] | trace <scene.json> <rays> <hits>\n");
         return 2;
     } catch (const std::exception &e) {

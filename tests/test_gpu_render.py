@@ -86,6 +86,36 @@ def test_wide_bvh_image_matches_reference(wr_lib, name):
     assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
 
 
+def test_exr_and_hdr_envmaps_render_like_pfm(wr_lib, tmp_path):
+    """The env fixture with its sky stored losslessly as OpenEXR (FLOAT, ZIP) renders as with the
+    PFM; stored as Radiance HDR it renders as the PFM of the HDR's decoded values."""
+    import json
+    import shutil
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from image_writers import write_exr, write_hdr
+    path, _ = golden_scene("env")
+    d = os.path.dirname(path)
+    for f in os.listdir(d):
+        shutil.copy(os.path.join(d, f), tmp_path / f)
+    scene = json.load(open(path))
+    env = wr_lib.read_image(os.path.join(d, scene["envmap"]))
+    write_exr(str(tmp_path / "sky.exr"), {c: env[..., k] for k, c in enumerate("RGB")}, "zip", "float")
+    write_hdr(str(tmp_path / "sky.hdr"), env, rle=True)
+    wr_lib.write_pfm(str(tmp_path / "sky_hdr.pfm"), wr_lib.read_image(str(tmp_path / "sky.hdr")))
+    images = {}
+    for name in ("sky.exr", "sky.hdr", "sky_hdr.pfm", scene["envmap"]):
+        scene_v = dict(scene, envmap=name)
+        p = tmp_path / ("scene_" + name.replace(".", "_") + ".json")
+        p.write_text(json.dumps(scene_v))
+        with wr_lib.Scene.from_file(str(p)) as sc:
+            images[name] = sc.render(spp=16, seed=7)
+    # same random streams and the same environment; only the FP64 atomic summation order may differ
+    assert np.allclose(images["sky.exr"], images[scene["envmap"]], rtol=1e-9, atol=1e-12)
+    assert np.allclose(images["sky.hdr"], images["sky_hdr.pfm"], rtol=1e-9, atol=1e-12)
+    assert np.isfinite(images["sky.hdr"]).all()
+
+
 def test_graph_and_plain_launches_agree(wr_lib):
     path, _ = golden_scene("zoo")
     with wr_lib.Scene.from_file(path) as sc:

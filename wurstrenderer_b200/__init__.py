@@ -90,7 +90,7 @@ BVH_DEVICE_LBVH = 1
 # every function the C ABI exports (include/wurst_b200.h)
 EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
-           "wr_trace_closest", "wr_trace_hits", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_run_simple2",
+           "wr_trace_closest", "wr_trace_hits", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_read_image", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
            "wr_render_batch_device", "wr_autotune", "wr_guide_reset", "wr_guide_get_params", "wr_guide_set_params",
            "wr_guide_box", "wr_guide_eval", "wr_guide_gradient", "wr_guide_train"]
@@ -130,6 +130,7 @@ def load_library(path: str = LIB_PATH):
     L.wr_trace_occluded.argtypes = [vp, fp, ip, fp]
     L.wr_trace_stats.argtypes = [vp, fp, ip, ip, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
     L.wr_write_pfm.argtypes = [cp, fp, ip, ip]
+    L.wr_read_image.argtypes = [cp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), fp]
     L.wr_run_simple2.argtypes = [cp]
     L.wr_run_jsimple2.argtypes = [cp]
     L.wr_set_device.argtypes = [ip]
@@ -421,6 +422,17 @@ def write_pfm(path: str, image: np.ndarray) -> None:
     """PFM in the reference's layout (rows bottom-to-top, little-endian float RGB)."""
     img = np.ascontiguousarray(image, np.float64)
     _check(load_library().wr_write_pfm(os.fspath(path).encode(), _ptr(img), img.shape[1], img.shape[0]))
+
+
+def read_image(path: str) -> np.ndarray:
+    """Reads a .pfm / .hdr / .exr image as the scene loader reads environment maps:
+    (H, W, 3) float32, row 0 = top (FimageIo::Load, src/common/floatimage.h:379-404)."""
+    L = load_library()
+    w, h = ctypes.c_int(0), ctypes.c_int(0)
+    _check(L.wr_read_image(os.fspath(path).encode(), ctypes.byref(w), ctypes.byref(h), None))
+    out = np.empty((h.value, w.value, 3), np.float32)
+    _check(L.wr_read_image(os.fspath(path).encode(), ctypes.byref(w), ctypes.byref(h), _ptr(out)))
+    return out
 
 
 def read_pfm(path: str) -> np.ndarray:

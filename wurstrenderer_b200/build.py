@@ -27,7 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall,-Wno-
           "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 CU_FLAGS = ARCH + COMMON + ["--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES = ["wr_scene_io.cpp", "wr_bvh.cpp", "wr_capi.cpp", "wr_kernels.cu", "wr_noalloc.cu", "wr_lbvh.cu", "wr_guide.cu"]
+SOURCES = ["wr_scene_io.cpp", "wr_image_io.cpp", "wr_bvh.cpp", "wr_capi.cpp", "wr_kernels.cu", "wr_noalloc.cu", "wr_lbvh.cu", "wr_guide.cu"]
 
 
 def _newest_header():
@@ -58,7 +58,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 flags = ARCH + COMMON + ["-x", "c++"]
             _run([NVCC] + flags + ["-c", path, "-o", obj], verbose)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fPIC", "-lpthread"], verbose)
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fPIC", "-lpthread", "-lz"], verbose)
     cli_src = os.path.join(CSRC, "wr_cli.cpp")
     if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB), os.path.getmtime(cli_src)):
         _run([NVCC] + ARCH + ["-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-x", "c++", cli_src, "-o", CLI,

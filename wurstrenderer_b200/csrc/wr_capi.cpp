@@ -1568,6 +1568,20 @@ int wr_write_pfm(const char *path, const double *rgb, int width, int height) {
     }
 }
 
+int wr_read_image(const char *path, int *width, int *height, float *rgb) {
+    if (!path || !width || !height) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        int w = 0, h = 0;
+        const std::vector<float> img = wr::read_image(path, &w, &h);
+        *width = w;
+        *height = h;
+        if (rgb) memcpy(rgb, img.data(), img.size() * sizeof(float));
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
 int wr_run_simple2(const char *path) {
     wr_scene *s = nullptr;
     int rc = wr_scene_create(path, &s);

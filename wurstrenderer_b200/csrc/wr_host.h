@@ -93,6 +93,8 @@ Scene load_simple2_text(const std::string &json_text, const std::string &base_di
 Camera parse_camera_json(const std::string &camera_json);
 void write_pfm(const std::string &path, const double *rgb, int width, int height);
 std::vector<float> read_pfm(const std::string &path, int *width, int *height);
+// .pfm / .hdr / .exr by extension (FimageIo::LoadAny, src/common/floatimage.h:379-396); RGB, row 0 = top
+std::vector<float> read_image(const std::string &path, int *width, int *height);
 
 // BVH (wr_bvh.cpp): binary BVH over all triangles, device node layout
 struct BvhBuildResult {

@@ -468,7 +468,7 @@ Scene load_from_node(const JNode &root, const std::string &base_dir) {
     const std::string envmap = root.str("envmap", "");
     if (!envmap.empty()) {
         int w = 0, h = 0;
-        s.env.rgb = read_pfm(join_path(base_dir, envmap), &w, &h);
+        s.env.rgb = read_image(join_path(base_dir, envmap), &w, &h);
         if (w != 2 * h) throw Error(WR_ERR_INVALID_ARGUMENT, "envmap has wrong size");
         s.env.width = w;
         s.env.height = h;
