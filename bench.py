@@ -440,9 +440,19 @@ def main():
     value = paths_per_rank * world * args.steps / (max_ms / 1e3) / 1e6
 
     if args.quick:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "ms_per_step": max_ms / args.steps, "spp": spp, "quick": True}
+        if args.steps == 1 and args.warmup == 0 and batch_jobs is None:
+            # the timed render once more, with its per-kernel launch and ray counts (profiling runs: an
+            # ncu capture limited to the first extend launches sees only the timed render's)
+            scene.render_device(film.data_ptr(), spp=spp, seed=rank_seed(7919 * (rank + 1), rank),
+                                queue_capacity=qc, profile=2, guiding=1 if args.workload == "door" else 0,
+                                **knobs)
+            pst = scene.stats
+            line["extend_launches"] = dict(zip(wr.KERNELS, pst["kernel_count"]))["extend"]
+            line["extend_rays"] = dict(zip(wr.KERNELS, pst["kernel_items"]))["extend"]
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-                              "ms_per_step": max_ms / args.steps, "spp": spp, "quick": True}), flush=True)
+            print(json.dumps(line), flush=True)
         scene.close()
         if world > 1:
             dist.destroy_process_group()
