@@ -177,7 +177,7 @@ def relmse(x, ref, eps=1e-2):
     return float(np.mean((x - ref) ** 2 / (ref ** 2 + eps)))
 
 
-@pytest.mark.parametrize("name", ["cornell", "zoo", "env", "hf"])
+@pytest.mark.parametrize("name", ["cornell", "zoo", "env", "hf", "phong"])
 def test_guided_render_matches_reference(wr_lib, name):
     """Guided renders (fresh network trained on the first 32 spp of every run) are the
     same estimator with another sampling density: within the reference's noise floor."""
