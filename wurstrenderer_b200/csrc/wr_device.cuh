@@ -30,7 +30,7 @@ constexpr float kRayEps = 1e-4f;              // Ray<Vec>::Epsilon (src/common/m
 
 constexpr int kTraceBlock = 128;   // threads per block of the traversal kernels
 constexpr int kShadeBlock = 256;   // threads per block of shade / raygen
-constexpr int kSmemStack = 32;     // traversal stack entries kept in shared memory per ray
+constexpr int kSmemStack = 8;      // traversal stack entries kept in shared memory per ray (the rest in local memory)
 constexpr int kMaxStack = 64;      // total traversal stack entries (the BVH builder stays below)
 
 // device counters of the wavefront loop (uint32 each)
