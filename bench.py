@@ -534,7 +534,7 @@ def main():
     if world == 1 and not args.no_guiding and args.workload in ("heightfield", "c5"):
         study = "c5" if args.workload == "c5" else "door"
         line["equal_time_relmse"] = guided_vs_plain(wr, study, plain_spp=1024 if study == "c5" else 256,
-                                                    seeds=1 if study == "c5" else 2)
+                                                    seeds=1 if study == "c5" else 3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()
