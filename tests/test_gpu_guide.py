@@ -180,7 +180,10 @@ def relmse(x, ref, eps=1e-2):
 @pytest.mark.parametrize("name", ["cornell", "zoo", "env", "hf", "phong"])
 def test_guided_render_matches_reference(wr_lib, name):
     """Guided renders (fresh network trained on the first 32 spp of every run) are the
-    same estimator with another sampling density: within the reference's noise floor."""
+    same estimator with another sampling density: within the reference's noise floor. The block
+    z-scores divide by the GPU's and the reference's own variance (the latter from its two
+    independent halves): the guided estimator is less noisy than the reference, so taking the
+    two variances equal would understate the spread of the difference."""
     from test_gpu_render import block_z
     path, meta = golden_scene(name)
     ref_a = np.load(os.path.join(GOLDEN, name + "_ref_hi_a.npy")).astype(np.float64)
@@ -199,7 +202,7 @@ def test_guided_render_matches_reference(wr_lib, name):
     floor = relmse(ref_b, ref_a)
     err = relmse(img, ref_a)
     assert err <= 2.0 * floor + 1e-6, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
-    z = block_z(runs, ref_a)
+    z = block_z(runs, 0.5 * (ref_a + ref_b), ref_pair=(ref_a, ref_b))
     assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
     assert abs(img.mean() / ref_a.mean() - 1.0) < 0.01
 

@@ -17,7 +17,9 @@
 
 namespace wrd {
 
-constexpr float kGuideAlpha = 0.5f;   // probability of sampling the guide instead of the BSDF
+// probability of sampling the guide instead of the BSDF (0.65 measured best of 0.5 / 0.65 / 0.75 /
+// 0.85 in equal-time error on the door-gap room)
+constexpr float kGuideAlpha = 0.65f;
 
 __device__ __forceinline__ float guide_weight_sum(const wrg::PackedLobes &L) {
     float w[8];
