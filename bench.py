@@ -380,7 +380,8 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
     tune = {}
     tune_ms = None
-    if not args.no_autotune:
+    if not args.no_autotune and args.workload != "jobs128":
+        # (the autotuner probes renders of the scene's own camera, which do not represent a batch)
         tune, tune_ms = scene.autotune(probe_spp=16)
         tune = {k: v for k, v in tune.items() if k != "use_graph"}
     if args.queue_capacity:

@@ -1285,6 +1285,9 @@ int wr_render_batch_device(wr_scene *s, const wr_job *jobs, int n, const wr_rend
 
 int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms) {
     if (!s || !best) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
+    // a setting replaces the current one only when its probe is 2 % faster: smaller differences are
+    // within the run-to-run spread of a probe render
+    constexpr double kTuneMargin = 0.98;
     try {
         wr_render_desc cur{};
         if (base) cur = *base;
@@ -1312,14 +1315,14 @@ int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_rende
             d.trace_block = blk;
             d.grid_trace = 0;
             const double t = trial(d);
-            if (t < bt) { bt = t; cur = d; }
+            if (t < bt * kTuneMargin) { bt = t; cur = d; }
         }
         // 2) wavefront capacity
         for (int cap : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
             wr_render_desc d = cur;
             d.queue_capacity = cap;
             const double t = trial(d);
-            if (t < bt) { bt = t; cur = d; }
+            if (t < bt * kTuneMargin) { bt = t; cur = d; }
         }
         // 3) persistent-CTA count of the traversal and shading kernels
         const int blk = (cur.trace_block == 64 || cur.trace_block == 256) ? cur.trace_block : 128;
@@ -1329,20 +1332,20 @@ int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_rende
             wr_render_desc d = cur;
             d.grid_trace = std::max(sms, int(occ_t * f));
             const double t = trial(d);
-            if (t < bt) { bt = t; cur = d; }
+            if (t < bt * kTuneMargin) { bt = t; cur = d; }
         }
         for (double f : {0.5, 1.0}) {
             wr_render_desc d = cur;
             d.grid_shade = std::max(sms, int(occ_s * f));
             const double t = trial(d);
-            if (t < bt) { bt = t; cur = d; }
+            if (t < bt * kTuneMargin) { bt = t; cur = d; }
         }
         // 4) dynamic ray fetching threshold
         for (int th : {12, 16, 24, 28}) {
             wr_render_desc d = cur;
             d.fetch_threshold = th;
             const double t = trial(d);
-            if (t < bt) { bt = t; cur = d; }
+            if (t < bt * kTuneMargin) { bt = t; cur = d; }
         }
         *best = cur;
         if (base) { best->num_spp = base->num_spp; best->profile = base->profile; }
