@@ -753,7 +753,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
 // GUIDED: the learned proposal is on (w.lobes); a separate instantiation keeps the plain
 // shade kernel's register count (and occupancy) unchanged
 template <bool GUIDED>
-__global__ void __launch_bounds__(kShadeBlock, GUIDED ? 2 : 1) k_shade(DevScene s, WaveArgs w) {
+__global__ void __launch_bounds__(kShadeBlock, GUIDED ? 2 : 3) k_shade(DevScene s, WaveArgs w) {
     const uint32_t n = w.ctr[CTR_ACTIVE];
     if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 1, (unsigned long long)n);
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
