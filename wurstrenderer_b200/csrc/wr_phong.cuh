@@ -77,7 +77,6 @@ __host__ __device__ __forceinline__ Rd acos_(Rd a) { return Rd(acos(a.v)); }
 __host__ __device__ __forceinline__ Rd cos_(Rd a) { return Rd(cos(a.v)); }
 __host__ __device__ __forceinline__ Rd abs_(Rd a) { return Rd(fabs(a.v)); }
 __host__ __device__ __forceinline__ Rd copysign_(Rd a, Rd b) { return Rd(copysign(a.v, b.v)); }
-__host__ __device__ __forceinline__ double val(Rd a) { return a.v; }
 #endif
 
 WRP_HD double sqrt_(double a) { return sqrt(a); }
@@ -86,7 +85,6 @@ WRP_HD double acos_(double a) { return acos(a); }
 WRP_HD double cos_(double a) { return cos(a); }
 WRP_HD double abs_(double a) { return fabs(a); }
 WRP_HD double copysign_(double a, double b) { return copysign(a, b); }
-WRP_HD double val(double a) { return a; }
 
 template <class T> struct V {
     T x, y, z;
