@@ -80,18 +80,52 @@ def scene_path(rank, world, dist, workload="heightfield"):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region.
+
+    Read-only NVML queries every 10 ms on the device this rank renders on (matched by UUID, so
+    CUDA_VISIBLE_DEVICES remapping does not matter); where NVML is not usable, nvidia-smi every
+    200 ms on the local-rank index."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    PERIOD_S = 0.01
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, cuda_device=None):
         self.rows = []
         self.proc = None
         self.gpu = gpu_index
+        self.nvml = None
+        self.stop_evt = threading.Event()
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(cuda_device if cuda_device is not None else 0).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+            self.nvml = (pynvml, h, bits, float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)))
+        except Exception:
+            self.nvml = None
+
+    def _poll_nvml(self):
+        pynvml, h, bits, _ = self.nvml
+        while not self.stop_evt.is_set():
+            try:
+                sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((sm, [n for n, b in zip(self.NAMES, bits) if r & b]))
+            except Exception:
+                pass
+            self.stop_evt.wait(self.PERIOD_S)
 
     def start(self):
+        if self.nvml is not None:
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.t.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.gpu)],
@@ -106,6 +140,13 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_evt.set()
+            self.t.join(timeout=2)
+            sm = sorted(r[0] for r in self.rows)
+            reasons = sorted({n for r in self.rows for n in r[1]})
+            return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": self.nvml[3], "reasons": reasons,
+                    "samples": len(sm), "sm_mhz_min": sm[0] if sm else None, "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -115,7 +156,7 @@ class ClockSampler:
             self.proc.kill()
         self.t.join(timeout=2)
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = self.NAMES
         for r in self.rows:
             if len(r) < 9:
                 continue
@@ -129,7 +170,7 @@ class ClockSampler:
                     reasons.add(n)
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peaks():
@@ -419,7 +460,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
 
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(local_rank, torch.cuda.current_device())
     clocks.start()
     dev_ms, launches, iters = 0.0, 0, 0
     wall0 = time.perf_counter()
