@@ -14,7 +14,8 @@ with one NCCL reduce per step. Rank 0 prints one JSON line.
 
 `value` is device time (CUDA events on the renderer's stream, summed over the K
 steps, max over ranks); `e2e` is the same metric through the public C ABI call
-with host output (wr_render: film copied device->host inside the timed region).
+with host output (wr_render: film copied device->host into pinned host memory inside the timed
+region).
 The CPU baseline runs the oracle (the reference's own renderer code compiled
 here, or its FP64 restatement) on the box's host cores on a bounded sample of
 the same workload (full frame at reduced spp; per-path work is unchanged).
@@ -501,7 +502,7 @@ def main():
         return
 
     # end to end through the public C ABI with host output (device->host copy of the film inside)
-    host = np.empty((H, W, 3), np.float64)
+    host = torch.empty((H, W, 3), dtype=torch.float64, pin_memory=True).numpy()   # pinned host film
     e2e_ms = 0.0
     for i in range(args.steps):
         torch.cuda.synchronize()
@@ -540,6 +541,7 @@ def main():
         traffic = tr["dram_bytes_per_ray"] * rays / launches_e
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
+                "dram_gbs": None if traffic is None else traffic / (avg_ms / 1e3) / 1e9,
                 "alg_bytes_per_launch": alg_bytes / launches_e, "avg_launch_ms": avg_ms,
                 "rays_per_launch": rays / launches_e, "node_visits_per_ray": nv / max(1, rays),
                 "tri_tests_per_ray": nt / max(1, rays),
