@@ -120,14 +120,21 @@ typedef struct wr_scene_info {
 #define WR_BVH_DEVICE_LBVH 1    /* linear BVH built on the device (Morton codes, radix sort, Karras 2012) */
 
 #define WR_BVH_WIDTH_DEFAULT 2 /* bvh_width 0 selects this */
+#define WR_MAX_LEAF_DEFAULT 2  /* max_leaf 0 selects this (binary and 8-wide trees) */
+#define WR_SAH_PATCH_COST_DEFAULT 16 /* sah_patch_cost_milli 0 selects this many triangle tests */
 
 typedef struct wr_scene_options {
     int bvh_builder;         /* WR_BVH_HOST_SAH or WR_BVH_DEVICE_LBVH */
-    int max_leaf;            /* host SAH: triangles per leaf, 1..16 (0 = 4; 3 for the 8-wide tree) */
+    int max_leaf;            /* host SAH: triangles per leaf, 1..16 (0 = WR_MAX_LEAF_DEFAULT; at
+                                most 3 for the 8-wide tree) */
     int bvh_width;           /* 2: binary BVH (64-byte nodes); 8: compressed 8-wide BVH (80-byte
                                 nodes, 8-bit quantised child boxes, <= 3 triangles per leaf);
                                 0: WR_BVH_WIDTH_DEFAULT */
-    int reserved[5];
+    int sah_trav_cost_milli; /* host SAH: cost of one traversal step relative to one triangle
+                                test, in thousandths, 1..100000 (0 = 1000) */
+    int sah_patch_cost_milli;/* host SAH: cost of one Phong patch test relative to one triangle
+                                test, in thousandths, 1..1000000 (0 = WR_SAH_PATCH_COST_DEFAULT) */
+    int reserved[3];
 } wr_scene_options;
 
 /* Parses a simple2 scene JSON (Simple2Parser::Parse, src/sceneio/simple2parser.h:84-100),

@@ -138,3 +138,39 @@ def test_patch_hits_and_normals_match_reference(wr_lib, oracle_lib, name):
     assert np.abs(np.linalg.norm(nrm[m], axis=1) - 1.0).max() < 1e-5
     occ_ref = hng[:, 4] > 0.5
     assert (occ.astype(bool) != occ_ref).sum() <= max(1, int(0.001 * len(rays)))
+
+
+@pytest.mark.parametrize("name", ["hf", "phong"])
+@pytest.mark.parametrize("opts", [dict(max_leaf=1), dict(max_leaf=8, sah_trav_cost=3.0),
+                                  dict(sah_patch_cost=1.0), dict(sah_patch_cost=200.0, bvh_width=8)],
+                         ids=["leaf1", "leaf8_ct3", "patch1", "patch200_w8"])
+def test_tree_shape_options_keep_the_hits(wr_lib, oracle_lib, name, opts):
+    """Leaf size and the SAH's traversal / patch-test costs change the tree, never the accepted
+    hit: the same closest hits as the reference (ties and edges excused) and the same hits as
+    the default tree."""
+    path, _ = golden_scene(name)
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name))
+    hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
+    with wr_lib.Scene.from_file(path, **opts) as sc:
+        g, p, t, _ = sc.trace_closest(rays)
+        occ = sc.trace_occluded(rays)
+    with wr_lib.Scene.from_file(path) as sd:
+        g2, p2, t2, _ = sd.trace_closest(rays)
+        occ2 = sd.trace_occluded(rays)
+    _, _, _, uv_ref = oracle_lib.OracleScene(path).trace_closest(rays)
+    t_ref = hits[:, 2].view(np.float32)
+    same = (g == hits[:, 0]) & (p == hits[:, 1])
+    assert (~same & ~_tie_or_edge(t_ref, t, uv_ref)).sum() == 0
+    both = (g == g2) & (p == p2)
+    assert np.array_equal(t[both], t2[both])
+    assert (~both & ~_tie_or_edge(t2, t, uv_ref)).sum() == 0
+    assert (occ != occ2).sum() <= max(1, int(0.002 * len(rays)))
+
+
+def test_tree_shape_option_errors(wr_lib):
+    path, _ = golden_scene("cornell")
+    for bad in (dict(sah_trav_cost=-1.0), dict(sah_trav_cost=101.0), dict(sah_patch_cost=-2.0),
+                dict(sah_patch_cost=1001.0), dict(bvh_width=4)):
+        with pytest.raises(wr_lib.WurstError) as e:
+            wr_lib.Scene.from_file(path, **bad)
+        assert e.value.status == 1     # WR_ERR_INVALID_ARGUMENT

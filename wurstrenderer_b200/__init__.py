@@ -80,7 +80,8 @@ class SceneInfo(ctypes.Structure):
 
 class SceneOptions(ctypes.Structure):
     _fields_ = [("bvh_builder", ctypes.c_int), ("max_leaf", ctypes.c_int), ("bvh_width", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("sah_trav_cost_milli", ctypes.c_int), ("sah_patch_cost_milli", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
 
 
 BVH_HOST_SAH = 0
@@ -162,14 +163,18 @@ class Scene:
 
     @classmethod
     def from_file(cls, json_path: str, bvh_builder: int = BVH_HOST_SAH, max_leaf: int = 0,
-                  bvh_width: int = 0) -> "Scene":
-        """bvh_width: 2 binary BVH, 8 compressed 8-wide BVH, 0 the library default."""
+                  bvh_width: int = 0, sah_trav_cost: float = 0.0, sah_patch_cost: float = 0.0) -> "Scene":
+        """bvh_width: 2 binary BVH, 8 compressed 8-wide BVH, 0 the library default.
+        sah_trav_cost / sah_patch_cost: host SAH cost of a traversal step / of a Phong patch test,
+        relative to a triangle test (0: the library defaults, 1 and 16)."""
         L = load_library()
         h = ctypes.c_void_p()
         opts = SceneOptions()
         opts.bvh_builder = int(bvh_builder)
         opts.max_leaf = int(max_leaf)
         opts.bvh_width = int(bvh_width)
+        opts.sah_trav_cost_milli = int(round(float(sah_trav_cost) * 1000))
+        opts.sah_patch_cost_milli = int(round(float(sah_patch_cost) * 1000))
         _check(L.wr_scene_create_ex(os.fspath(json_path).encode(), ctypes.byref(opts), ctypes.byref(h)))
         return cls(h)
 

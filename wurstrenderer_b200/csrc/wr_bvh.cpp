@@ -62,9 +62,12 @@ struct Builder {
     std::vector<TmpNode> nodes;
     std::atomic<int> next_node{0};
     int max_leaf;
+    double trav_cost;                  // SAH cost of a traversal step, relative to a triangle test
+    const std::vector<float> *prim_cost;   // SAH cost of each primitive's test (null: 1 each)
     int par_depth;
 
-    Builder(const std::vector<float> &verts, int ml, int threads) : v(verts), max_leaf(ml) {
+    Builder(const std::vector<float> &verts, int ml, int threads, double ct, const std::vector<float> *pc)
+        : v(verts), max_leaf(ml), trav_cost(ct), prim_cost(pc) {
         const size_t n = v.size() / 9;
         tbox.resize(n);
         cen.resize(3 * n);
@@ -103,6 +106,7 @@ struct Builder {
         }
         nd.box = box;
         if (count <= 1) { nd.start = start; nd.count = count; return; }
+        auto weight = [&](uint32_t t) { return prim_cost ? double((*prim_cost)[t]) : 1.0; };
 
         // binned SAH over the three axes
         int best_axis = -1, best_split = -1;
@@ -113,37 +117,45 @@ struct Builder {
             const float scale = kBins / ext;
             Aabb bins[kBins];
             uint32_t cnt[kBins] = {0};
+            double wsum[kBins] = {0.0};
             for (uint32_t i = start; i < start + count; ++i) {
                 const uint32_t t = idx[i];
                 int b = int((cen[3 * size_t(t) + ax] - cb.lo[ax]) * scale);
                 b = std::min(std::max(b, 0), kBins - 1);
                 cnt[b]++;
+                wsum[b] += weight(t);
                 bins[b].grow(tbox[t]);
             }
-            double right_area[kBins];
+            double right_area[kBins], right_w[kBins];
             uint32_t right_cnt[kBins];
             Aabb acc;
             uint32_t c = 0;
+            double w = 0.0;
             for (int b = kBins - 1; b > 0; --b) {
                 acc.grow(bins[b]);
                 c += cnt[b];
+                w += wsum[b];
                 right_area[b] = acc.half_area();
                 right_cnt[b] = c;
+                right_w[b] = w;
             }
             acc = Aabb();
             c = 0;
+            w = 0.0;
             for (int b = 0; b < kBins - 1; ++b) {
                 acc.grow(bins[b]);
                 c += cnt[b];
+                w += wsum[b];
                 if (c == 0 || right_cnt[b + 1] == 0) continue;
-                const double cost = acc.half_area() * c + right_area[b + 1] * right_cnt[b + 1];
+                const double cost = acc.half_area() * w + right_area[b + 1] * right_w[b + 1];
                 if (cost < best_cost) { best_cost = cost; best_axis = ax; best_split = b; }
             }
         }
         const double parent_area = box.half_area();
-        // SAH with traversal cost 1 and triangle cost 1 (relative to the parent's area)
-        const double split_cost = 1.0 + (parent_area > 0 ? best_cost / parent_area : double(count));
-        const double leaf_cost = double(count);
+        // SAH with traversal cost trav_cost and each primitive's test cost (relative to the parent's area)
+        double leaf_cost = 0.0;
+        for (uint32_t i = start; i < start + count; ++i) leaf_cost += weight(idx[i]);
+        const double split_cost = trav_cost + (parent_area > 0 ? best_cost / parent_area : leaf_cost);
         if (count <= uint32_t(max_leaf) && (best_axis < 0 || leaf_cost <= split_cost)) {
             nd.start = start; nd.count = count; return;
         }
@@ -199,13 +211,15 @@ void put_child_box(float *out, int slot, const Aabb &b, bool empty) {
 
 }  // namespace
 
-BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_leaf, int threads) {
+BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_leaf, int threads, double trav_cost,
+                             const std::vector<float> *prim_cost) {
     BvhBuildResult res;
     const uint32_t n = uint32_t(tri_vertices.size() / 9);
     if (threads <= 0) threads = std::max(1u, std::thread::hardware_concurrency());
     max_leaf = std::max(1, std::min(max_leaf, int(kMaxLeafHard)));
     if (n >= (1u << 27)) throw Error(WR_ERR_UNSUPPORTED, "more than 2^27 triangles");
-    Builder b(tri_vertices, max_leaf, threads);
+    if (prim_cost && prim_cost->size() != n) throw Error(WR_ERR_INVALID_ARGUMENT, "prim_cost size");
+    Builder b(tri_vertices, max_leaf, threads, trav_cost, prim_cost);
     const int root = b.alloc();
     if (n > 0) b.build(root, 0, n, 0);
     else b.nodes[root].count = 0;

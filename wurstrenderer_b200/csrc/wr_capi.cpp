@@ -245,8 +245,18 @@ void build_device_scene(wr_scene &s) {
         bvh = wr::build_bvh_lbvh(build_in, st, &s.bvh_ms);
     } else {
         // the compressed 8-wide tree encodes at most 3 triangles per leaf
-        const int ml = s.opts.max_leaf > 0 ? s.opts.max_leaf : (wide ? 3 : 4);
-        bvh = wr::build_bvh_sah(build_in, wide ? std::min(ml, 3) : ml, 0);
+        const int ml = s.opts.max_leaf > 0 ? s.opts.max_leaf : WR_MAX_LEAF_DEFAULT;
+        const double ct = s.opts.sah_trav_cost_milli > 0 ? s.opts.sah_trav_cost_milli * 1e-3 : 1.0;
+        // a Phong patch test (FP64 cubic and quadratics) costs many triangle tests: weighting
+        // patches in the SAH keeps them in small leaves of their own
+        std::vector<float> prim_cost;
+        if (npatch) {
+            const double cp = s.opts.sah_patch_cost_milli > 0 ? s.opts.sah_patch_cost_milli * 1e-3
+                                                              : double(WR_SAH_PATCH_COST_DEFAULT);
+            prim_cost.resize(ntri);
+            for (uint32_t g = 0; g < ntri; ++g) prim_cost[g] = is_patch[g] ? float(cp) : 1.f;
+        }
+        bvh = wr::build_bvh_sah(build_in, wide ? std::min(ml, 3) : ml, 0, ct, npatch ? &prim_cost : nullptr);
         s.bvh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
     }
     wr::WideBvh wbvh;
@@ -1093,6 +1103,10 @@ std::unique_ptr<wr_scene> create(wr::Scene &&host, const wr_scene_options *opts 
     if (s->opts.bvh_width == 0) s->opts.bvh_width = WR_BVH_WIDTH_DEFAULT;
     if (s->opts.bvh_width != 2 && s->opts.bvh_width != 8)
         throw Error(WR_ERR_INVALID_ARGUMENT, "bvh_width must be 2 or 8");
+    if (s->opts.sah_trav_cost_milli < 0 || s->opts.sah_trav_cost_milli > 100000)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "sah_trav_cost_milli must be in 0..100000");
+    if (s->opts.sah_patch_cost_milli < 0 || s->opts.sah_patch_cost_milli > 1000000)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "sah_patch_cost_milli must be in 0..1000000");
     s->host = std::move(host);
     build_device_scene(*s);
     return s;
@@ -1185,7 +1199,7 @@ int wr_scene_inspect(const char *path, wr_scene_info *info) {
         for (const wr::Mesh &m : h.meshes)
             for (uint32_t i : m.indices)
                 for (int k = 0; k < 3; ++k) verts.push_back(m.positions[3 * size_t(i) + k]);
-        wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, 4, 0);
+        wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, WR_MAX_LEAF_DEFAULT, 0);
         memset(info, 0, sizeof(*info));
         info->width = h.has_camera ? h.camera.width : 0;
         info->height = h.has_camera ? h.camera.height : 0;

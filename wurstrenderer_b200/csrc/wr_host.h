@@ -103,7 +103,10 @@ struct BvhBuildResult {
     int depth = 0;
     double sah_cost = 0.0;
 };
-BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_leaf, int threads);
+// Binned-SAH BVH over triangles (9 floats each). trav_cost: SAH cost of a traversal step;
+// prim_cost: SAH cost of each primitive's test (null: 1 each), both relative to one triangle test.
+BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_leaf, int threads,
+                             double trav_cost = 1.0, const std::vector<float> *prim_cost = nullptr);
 
 // Compressed 8-wide BVH collapsed from a binary one whose leaves hold at most 3 triangles
 // (layout in wr_bvh.cpp); `order` is the new leaf order -> global triangle index.
