@@ -356,9 +356,11 @@ __device__ __forceinline__ void push_shadow(const WaveArgs &w, bool pred, f3 o, 
     uint32_t n;
     const uint32_t idx = warp_append(w.ctr + CTR_SHADOW, pred, n);
     if (pred && idx < w.shadow_capacity) {
-        w.sq.o[idx] = make_float4(o.x, o.y, o.z, tmax);
-        w.sq.d[idx] = make_float4(d.x, d.y, d.z, __uint_as_float(slot));
-        w.sq.c[idx] = make_float4(c.x, c.y, c.z, __uint_as_float(rec));
+        // streaming stores (evict-first in L2): the queues pass through L2 once per bounce and
+        // should not push the BVH out of it
+        __stcs(&w.sq.o[idx], make_float4(o.x, o.y, o.z, tmax));
+        __stcs(&w.sq.d[idx], make_float4(d.x, d.y, d.z, __uint_as_float(slot)));
+        __stcs(&w.sq.c[idx], make_float4(c.x, c.y, c.z, __uint_as_float(rec)));
     }
 }
 
@@ -407,7 +409,7 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
                 if (ray < n) {
                     float4 o, d;
                     float tmax;
-                    if (SHADOW) { o = w.sq.o[ray]; d = w.sq.d[ray]; tmax = o.w; }
+                    if (SHADOW) { o = __ldcs(&w.sq.o[ray]); d = __ldcs(&w.sq.d[ray]); tmax = o.w; }
                     else { o = w.cur.o[ray]; d = w.cur.d[ray]; tmax = __int_as_float(0x7f800000); }
                     r = ray_setup(xyz(o), xyz(d));
                     if (PHONG) pr = PatchRay{o.x, o.y, o.z, d.x, d.y, d.z};
@@ -438,8 +440,8 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
             busy = false;
             if (SHADOW) {
                 if (tri == MISS) {   // unoccluded
-                    const float4 c = w.sq.c[ray];
-                    film_add(w, __float_as_uint(w.sq.d[ray].w), mk(c.x, c.y, c.z));
+                    const float4 c = __ldcs(&w.sq.c[ray]);
+                    film_add(w, __float_as_uint(__ldcs(&w.sq.d[ray]).w), mk(c.x, c.y, c.z));
                     if (w.records) record_contribution(w.records, __float_as_uint(c.w), mk(c.x, c.y, c.z));
                 }
             } else {
@@ -551,12 +553,13 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
     bool want_rec = false;              // a record is created for this vertex
     f3 rec_pos = mk(0, 0, 0), rec_n = mk(0, 1, 0), rec_wo = mk(0, 1, 0), rec_thr = mk(0, 0, 0);
     if (valid) {
-        const float4 o4 = w.cur.o[i], d4 = w.cur.d[i], t4 = w.cur.thr[i];
-        meta = w.cur.meta[i];
-        if (w.records) rec = w.cur.rec[i];
+        // last reads of this bounce's path state (streaming: evict-first in L2)
+        const float4 o4 = __ldcs(&w.cur.o[i]), d4 = __ldcs(&w.cur.d[i]), t4 = __ldcs(&w.cur.thr[i]);
+        meta = __ldcs(&w.cur.meta[i]);
+        if (w.records) rec = __ldcs(&w.cur.rec[i]);
         const uint32_t depth = meta & 0xffu, job = meta >> 8;
         const DevJob &J = job_at(w, job);
-        const float4 h = w.hit[i];
+        const float4 h = __ldcs(&w.hit[i]);
         const f3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
         const float prevPdfW = o4.w;
         pixel = __float_as_uint(d4.w);   // global film pixel
@@ -742,11 +745,11 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
     uint32_t cnt;
     const uint32_t j = warp_append(w.ctr + CTR_NEXT, alive, cnt);
     if (alive) {
-        w.nxt.o[j] = make_float4(no.x, no.y, no.z, npdf);
-        w.nxt.d[j] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel));
-        w.nxt.thr[j] = make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample));
-        w.nxt.meta[j] = meta + 1u;
-        if (w.records) w.nxt.rec[j] = nrec;
+        __stcs(&w.nxt.o[j], make_float4(no.x, no.y, no.z, npdf));
+        __stcs(&w.nxt.d[j], make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel)));
+        __stcs(&w.nxt.thr[j], make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample)));
+        __stcs(&w.nxt.meta[j], meta + 1u);
+        if (w.records) __stcs(&w.nxt.rec[j], nrec);
     }
 }
 
@@ -859,11 +862,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
                     d = -l.pos;
                     thr = l.contrib * (kPi * R * R);
                 }
-                w.nxt.o[j] = make_float4(o.x, o.y, o.z, 0.f);
-                w.nxt.d[j] = make_float4(d.x, d.y, d.z, __uint_as_float(J.pix_offset + lpix));
-                w.nxt.thr[j] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(sample));
-                w.nxt.meta[j] = job << 8;
-                if (w.records) w.nxt.rec[j] = wrg::kNoRecord;
+                __stcs(&w.nxt.o[j], make_float4(o.x, o.y, o.z, 0.f));
+                __stcs(&w.nxt.d[j], make_float4(d.x, d.y, d.z, __uint_as_float(J.pix_offset + lpix)));
+                __stcs(&w.nxt.thr[j], make_float4(thr.x, thr.y, thr.z, __uint_as_float(sample)));
+                __stcs(&w.nxt.meta[j], job << 8);
+                if (w.records) __stcs(&w.nxt.rec[j], wrg::kNoRecord);
             } else {
                 // strategy C: connect the light vertex to the camera (pathnextevent.h:75-99)
                 CamLink cl;
@@ -889,11 +892,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
                 const float ct = dir.z;
                 const float pdfW = cam.per_film / (ct * ct * ct) / float(J.npix);
                 const f3 dw = normalize(cfx * dir.x + cfy * dir.y + cfz * dir.z);
-                w.nxt.o[j] = make_float4(c0.x, c0.y, c0.z, pdfW);
-                w.nxt.d[j] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(J.pix_offset + lpix));
-                w.nxt.thr[j] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sample));
-                w.nxt.meta[j] = job << 8;
-                if (w.records) w.nxt.rec[j] = wrg::kNoRecord;
+                __stcs(&w.nxt.o[j], make_float4(c0.x, c0.y, c0.z, pdfW));
+                __stcs(&w.nxt.d[j], make_float4(dw.x, dw.y, dw.z, __uint_as_float(J.pix_offset + lpix)));
+                __stcs(&w.nxt.thr[j], make_float4(1.f, 1.f, 1.f, __uint_as_float(sample)));
+                __stcs(&w.nxt.meta[j], job << 8);
+                if (w.records) __stcs(&w.nxt.rec[j], wrg::kNoRecord);
             }
         }
         push_shadow(w, shadow, so, sd, stmax, slot, sc);
