@@ -540,7 +540,9 @@ def main():
     if tr:
         traffic = tr["dram_bytes_per_ray"] * rays / launches_e
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
+                "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_extend (closest-hit traversal), timed alone in a profiled render; the timed renders "
+                          "run the same traversal fused with the previous iteration's shadow rays (k_trace_pair)",
                 "dram_gbs": None if traffic is None else traffic / (avg_ms / 1e3) / 1e9,
                 "alg_bytes_per_launch": alg_bytes / launches_e, "avg_launch_ms": avg_ms,
                 "rays_per_launch": rays / launches_e, "node_visits_per_ray": nv / max(1, rays),

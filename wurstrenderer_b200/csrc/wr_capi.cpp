@@ -683,7 +683,8 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     } else if (desc.use_graph) {
         // the whole render as one graph: clears, first wavefront, a while-loop node whose body is two
         // bounce iterations (the bookkeeping kernel clears the condition when the wavefront drains
-        // or the iteration bound is reached), and the resolve
+        // or the iteration bound is reached), the last shadow rays and the resolve; each iteration
+        // traces its extend rays and the previous iteration's shadow rays in one launch
         cudaGraph_t g = nullptr, gp = nullptr, gs = nullptr;
         cudaGraphExec_t ex = nullptr;
         auto cleanup = [&]() {
@@ -702,7 +703,7 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
             }
             WR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             clear();
-            if (trace) wrk::launch_prime(s.dev, b, r, st);
+            if (trace) wrk::launch_prime_fused(s.dev, b, r, st);
             WR_CUDA(cudaStreamEndCapture(st, &gp));
             cudaGraphNode_t np, nw, ns;
             WR_CUDA(cudaGraphAddChildGraphNode(&np, g, nullptr, 0, gp));
@@ -716,12 +717,13 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
                 WR_CUDA(cudaGraphAddNode(&nw, g, &np, 1, &cp));
                 cudaGraph_t body = cp.conditional.phGraph_out[0];
                 WR_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-                wrk::launch_iteration(s.dev, b, r, 0, st);
-                wrk::launch_iteration(s.dev, b, r, 1, st);
+                wrk::launch_iteration_fused(s.dev, b, r, 0, st);
+                wrk::launch_iteration_fused(s.dev, b, r, 1, st);
                 WR_CUDA(cudaStreamEndCapture(st, &body));
                 last = nw;
             }
             WR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            if (trace) wrk::launch_shadow_flush(s.dev, b, r, st);
             wrk::launch_resolve(b.film, dst, r, st);
             WR_CUDA(cudaStreamEndCapture(st, &gs));
             WR_CUDA(cudaGraphAddChildGraphNode(&ns, g, &last, 1, gs));
@@ -748,18 +750,18 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
         clear();
         WR_CUDA(cudaEventRecord(s.ev0, st));
         if (trace) {
-            wrk::launch_prime(s.dev, b, r, st);
+            wrk::launch_prime_fused(s.dev, b, r, st);
             WR_CUDA(cudaGetLastError());
-            launches += 3;
             while (true) {
-                wrk::launch_iteration(s.dev, b, r, 0, st);
-                wrk::launch_iteration(s.dev, b, r, 1, st);
+                wrk::launch_iteration_fused(s.dev, b, r, 0, st);
+                wrk::launch_iteration_fused(s.dev, b, r, 1, st);
                 WR_CUDA(cudaGetLastError());
-                launches += 10;
                 WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
                 WR_CUDA(cudaStreamSynchronize(st));
                 if (s.pinned[wrd::CTR_DONE]) break;
             }
+            wrk::launch_shadow_flush(s.dev, b, r, st);
+            WR_CUDA(cudaGetLastError());
         }
         wrk::launch_resolve(b.film, dst, r, st);
         WR_CUDA(cudaGetLastError());
@@ -786,9 +788,13 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     s.stats.render_ms = ms;
     s.stats.paths = total;
     s.stats.iterations = trace ? s.pinned[wrd::CTR_ITER] : 0;
-    // kernels per render: prime 3 + 5 (6 with guiding) per iteration + resolve (a graph launch runs the
-    // same kernels)
-    s.stats.kernel_launches = trace ? 3ull + (po.guide ? 6ull : 5ull) * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
+    // kernels per render (a graph launch runs the same kernels). Profiled: prime 3 + 5 (6 with
+    // guiding) per iteration + resolve; fused schedule: prime 2 + 4 (5) per iteration + the last
+    // shadow rays + resolve
+    if (profile)
+        s.stats.kernel_launches = trace ? 3ull + (po.guide ? 6ull : 5ull) * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
+    else
+        s.stats.kernel_launches = trace ? 2ull + (po.guide ? 5ull : 4ull) * s.pinned[wrd::CTR_ITER] + 2ull : 1ull;
     s.stats.max_shadow_queue = s.pinned[wrd::CTR_SHADOW_MAX];
     s.stats.queue_capacity = capacity;
     s.stats.grid_trace = r.grid_trace;

@@ -45,7 +45,8 @@ enum Counter {
     CTR_TIMEOUT = 7,     // the iteration bound was reached before the wavefront drained
     CTR_EXTEND_FETCH = 8,   // next ray of the current extend launch (dynamic fetching)
     CTR_SHADOW_FETCH = 9,   // next shadow ray of the current shadow launch
-    CTR_COUNT = 10
+    CTR_SHADOW_PENDING = 10,   // shadow rays of the previous iteration, traced by the next fused launch
+    CTR_COUNT = 11
 };
 
 struct DevMaterial {

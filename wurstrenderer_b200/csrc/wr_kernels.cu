@@ -380,9 +380,12 @@ __device__ __forceinline__ void film_add(const WaveArgs &w, uint32_t slot, f3 c)
 //   SHADOW = true:  shadow -- any hit of every queued shadow ray; unoccluded contributions
 //                   are added to the FP64 film (and to the path's training records)
 
+//   count_ctr: the counter holding the queue length (CTR_ACTIVE; CTR_SHADOW, or
+//              CTR_SHADOW_PENDING for the previous iteration's queue)
+
 template <int BLOCK, bool SHADOW, bool PHONG, bool WIDE>
-__device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w, uint32_t *stack) {
-    const uint32_t n = SHADOW ? min(w.ctr[CTR_SHADOW], w.shadow_capacity) : w.ctr[CTR_ACTIVE];
+__device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w, uint32_t *stack, int count_ctr) {
+    const uint32_t n = SHADOW ? min(w.ctr[count_ctr], w.shadow_capacity) : w.ctr[count_ctr];
     uint32_t *fetch = w.ctr + (SHADOW ? CTR_SHADOW_FETCH : CTR_EXTEND_FETCH);
     TraceStack st;
     st.smem = stack + threadIdx.x;
@@ -459,7 +462,7 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
 template <int BLOCK, bool PHONG, bool WIDE>
 __global__ void __launch_bounds__(BLOCK) k_extend(DevScene s, WaveArgs w) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    trace_queue<BLOCK, false, PHONG, WIDE>(s, w, stack);
+    trace_queue<BLOCK, false, PHONG, WIDE>(s, w, stack, CTR_ACTIVE);
 }
 
 // lens point of a sample's camera vertex (ThinlensCamera::sampleWe0ByPdf, thinlens.h:121-136; the
@@ -904,9 +907,34 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
 }
 
 template <int BLOCK, bool PHONG, bool WIDE>
-__global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w) {
+__global__ void __launch_bounds__(BLOCK) k_shadow(DevScene s, WaveArgs w, int count_ctr) {
     __shared__ uint32_t stack[kSmemStack * BLOCK];
-    trace_queue<BLOCK, true, PHONG, WIDE>(s, w, stack);
+    trace_queue<BLOCK, true, PHONG, WIDE>(s, w, stack, count_ctr);
+}
+
+// Extend of this iteration and the shadow rays of the previous one in one persistent launch:
+// a warp that finds the extend queue exhausted and its lanes finished moves on to the shadow
+// queue, so the shadow rays fill the extend launch's tail instead of waiting for it. The two
+// queues are independent: extend reads this wavefront's rays and writes hit records; the
+// shadow rays were queued by the previous shade / raygen and only add to the film (the next
+// shade appends to the shadow queue only after this launch).
+template <int BLOCK, bool PHONG, bool WIDE>
+__device__ __forceinline__ void trace_pair(const DevScene &s, const WaveArgs &w) {
+    __shared__ uint32_t stack[kSmemStack * BLOCK];
+    trace_queue<BLOCK, false, PHONG, WIDE>(s, w, stack, CTR_ACTIVE);
+    trace_queue<BLOCK, true, PHONG, WIDE>(s, w, stack, CTR_SHADOW_PENDING);
+}
+
+template <int BLOCK, bool WIDE>
+__global__ void __launch_bounds__(BLOCK) k_trace_pair(DevScene s, WaveArgs w) {
+    trace_pair<BLOCK, false, WIDE>(s, w);
+}
+
+// With Phong patches both FP64 patch tests in one kernel would take 190 registers (2 blocks of
+// 128 per SM); the bound keeps the 384 resident threads per SM of the separate kernels.
+template <int BLOCK, bool WIDE>
+__global__ void __launch_bounds__(BLOCK, (384 / BLOCK > 0 ? 384 / BLOCK : 1)) k_trace_pair_phong(DevScene s, WaveArgs w) {
+    trace_pair<BLOCK, true, WIDE>(s, w);
 }
 
 // queue bookkeeping between iterations (one thread); also drives the graph's while loop
@@ -916,6 +944,7 @@ __global__ void k_advance(WaveArgs w) {
     const uint32_t n_new = new_samples(w, filled, issued);
     if (w.ctr[CTR_SHADOW] > w.ctr[CTR_SHADOW_MAX]) w.ctr[CTR_SHADOW_MAX] = w.ctr[CTR_SHADOW];
     if (w.ctr[CTR_SHADOW] > w.shadow_capacity) w.ctr[CTR_OVERFLOW] = 1;
+    w.ctr[CTR_SHADOW_PENDING] = w.ctr[CTR_SHADOW];   // for a fused launch that traces them next
     w.ctr[CTR_ACTIVE] = filled + n_new;
     w.ctr[CTR_NEXT] = 0;
     w.ctr[CTR_SHADOW] = 0;
@@ -1098,32 +1127,42 @@ static WaveArgs make_args(const WaveBuffers &b, int parity, const RenderLaunch &
 }
 
 // the traversal kernel instantiation for the scene: block size x (Phong patches) x (BVH width)
-template <int BLOCK, bool SHADOW, bool PHONG, bool WIDE>
-void launch_trace_4(const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
-    if (SHADOW) k_shadow<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w);
-    else k_extend<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w);
+enum TraceLaunch { TRACE_EXTEND, TRACE_SHADOW, TRACE_SHADOW_PENDING, TRACE_PAIR };
+
+template <int BLOCK, bool PHONG, bool WIDE>
+void launch_trace_4(TraceLaunch what, const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
+    switch (what) {
+        case TRACE_EXTEND: k_extend<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w); break;
+        case TRACE_SHADOW: k_shadow<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w, CTR_SHADOW); break;
+        case TRACE_SHADOW_PENDING:
+            k_shadow<BLOCK, PHONG, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w, CTR_SHADOW_PENDING);
+            break;
+        case TRACE_PAIR:
+            if (PHONG) k_trace_pair_phong<BLOCK, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w);
+            else k_trace_pair<BLOCK, WIDE><<<r.grid_trace, BLOCK, 0, st>>>(s, w);
+            break;
+    }
 }
 
-template <int BLOCK, bool SHADOW>
-void launch_trace_3(const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
-    if (s.patches && s.wnodes) launch_trace_4<BLOCK, SHADOW, true, true>(s, w, r, st);
-    else if (s.patches) launch_trace_4<BLOCK, SHADOW, true, false>(s, w, r, st);
-    else if (s.wnodes) launch_trace_4<BLOCK, SHADOW, false, true>(s, w, r, st);
-    else launch_trace_4<BLOCK, SHADOW, false, false>(s, w, r, st);
+template <int BLOCK>
+void launch_trace_3(TraceLaunch what, const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
+    if (s.patches && s.wnodes) launch_trace_4<BLOCK, true, true>(what, s, w, r, st);
+    else if (s.patches) launch_trace_4<BLOCK, true, false>(what, s, w, r, st);
+    else if (s.wnodes) launch_trace_4<BLOCK, false, true>(what, s, w, r, st);
+    else launch_trace_4<BLOCK, false, false>(what, s, w, r, st);
 }
 
-template <bool SHADOW>
-void launch_trace(const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
-    if (r.trace_block == 64) launch_trace_3<64, SHADOW>(s, w, r, st);
-    else if (r.trace_block == 256) launch_trace_3<256, SHADOW>(s, w, r, st);
-    else launch_trace_3<128, SHADOW>(s, w, r, st);
+void launch_trace(TraceLaunch what, const DevScene &s, const WaveArgs &w, const RenderLaunch &r, cudaStream_t st) {
+    if (r.trace_block == 64) launch_trace_3<64>(what, s, w, r, st);
+    else if (r.trace_block == 256) launch_trace_3<256>(what, s, w, r, st);
+    else launch_trace_3<128>(what, s, w, r, st);
 }
 
 void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
                    cudaStream_t st) {
     const WaveArgs w = make_args(b, parity, r);
     switch (which) {
-        case KERNEL_EXTEND: launch_trace<false>(s, w, r, st); break;
+        case KERNEL_EXTEND: launch_trace(TRACE_EXTEND, s, w, r, st); break;
         case KERNEL_SHADE:
             if (w.lobes) k_shade<true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
             else k_shade<false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
@@ -1134,7 +1173,7 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
                                            b.lobes, b.capacity, r.guide_sms, st);
             break;
         case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
-        case KERNEL_SHADOW: launch_trace<true>(s, w, r, st); break;
+        case KERNEL_SHADOW: launch_trace(TRACE_SHADOW, s, w, r, st); break;
         case KERNEL_ADVANCE: k_advance<<<1, 1, 0, st>>>(w); break;
         default: break;
     }
@@ -1143,6 +1182,29 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
 void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity, cudaStream_t st) {
     for (int k : {KERNEL_EXTEND, KERNEL_GUIDE, KERNEL_SHADE, KERNEL_RAYGEN, KERNEL_SHADOW, KERNEL_ADVANCE})
         if (k != KERNEL_GUIDE || r.guide) launch_kernel(k, s, b, r, parity, st);
+}
+
+// Fused schedule: each iteration's extend shares one launch with the previous iteration's
+// shadow rays (k_trace_pair); the first wavefront's shadow rays go with the first extend, and
+// the last iteration's are traced by launch_shadow_flush after the loop. Same rays, same
+// film contributions as the separate schedule; only the FP64 atomic order differs.
+void launch_prime_fused(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st) {
+    RenderLaunch r0 = r;
+    r0.has_cond = 0;
+    for (int k : {KERNEL_RAYGEN, KERNEL_ADVANCE}) launch_kernel(k, s, b, r0, 1, st);
+}
+
+void launch_iteration_fused(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
+                            cudaStream_t st) {
+    launch_trace(TRACE_PAIR, s, make_args(b, parity, r), r, st);
+    for (int k : {KERNEL_GUIDE, KERNEL_SHADE, KERNEL_RAYGEN, KERNEL_ADVANCE})
+        if (k != KERNEL_GUIDE || r.guide) launch_kernel(k, s, b, r, parity, st);
+}
+
+void launch_shadow_flush(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st) {
+    RenderLaunch r0 = r;
+    r0.has_cond = 0;
+    launch_trace(TRACE_SHADOW_PENDING, s, make_args(b, 0, r0), r0, st);
 }
 
 void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st) {

@@ -52,6 +52,12 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
                    cudaStream_t st);
 void launch_prime(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st);
 void launch_iteration(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity, cudaStream_t st);
+// fused schedule: extend + the previous iteration's shadow rays in one launch, then a flush of
+// the last iteration's shadow rays after the loop
+void launch_prime_fused(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st);
+void launch_iteration_fused(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
+                            cudaStream_t st);
+void launch_shadow_flush(const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, cudaStream_t st);
 void launch_resolve(const double *film, double *out, const RenderLaunch &r, cudaStream_t st);
 void launch_trace_batch(const DevScene &s, const float4 *rays, uint32_t n, int any_hit, float4 *out, uint32_t *visits,
                         int grid, cudaStream_t st);
