@@ -183,13 +183,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def extend_traffic_per_ray():
-    """DRAM bytes per extend ray from the committed ncu capture summary, when present."""
+def traffic_per_ray():
+    """DRAM bytes per traced ray of the traversal kernels from the committed ncu capture summary
+    (keys "k_extend" and "k_trace_pair"), when present."""
     p = os.path.join(ROOT, "profiles", "extend_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
-    return None
+    return {}
 
 
 def cpu_model():
@@ -494,6 +495,7 @@ def main():
             pst = scene.stats
             line["extend_launches"] = dict(zip(wr.KERNELS, pst["kernel_count"]))["extend"]
             line["extend_rays"] = dict(zip(wr.KERNELS, pst["kernel_items"]))["extend"]
+            line["shadow_rays"] = dict(zip(wr.KERNELS, pst["kernel_items"]))["shadow"]
         if rank == 0:
             print(json.dumps(line), flush=True)
         scene.close()
@@ -535,18 +537,46 @@ def main():
     avg_ms = k_ms["extend"] / launches_e
     achieved = (alg_bytes / launches_e) / (avg_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    tr = extend_traffic_per_ray()
-    traffic = None
-    if tr:
-        traffic = tr["dram_bytes_per_ray"] * rays / launches_e
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "k_extend (closest-hit traversal), timed alone in a profiled render; the timed renders "
-                          "run the same traversal fused with the previous iteration's shadow rays (k_trace_pair)",
-                "dram_gbs": None if traffic is None else traffic / (avg_ms / 1e3) / 1e9,
-                "alg_bytes_per_launch": alg_bytes / launches_e, "avg_launch_ms": avg_ms,
-                "rays_per_launch": rays / launches_e, "node_visits_per_ray": nv / max(1, rays),
-                "tri_tests_per_ray": nt / max(1, rays),
+    tr = traffic_per_ray()
+    traffic = tr["k_extend"]["dram_bytes_per_ray"] * rays / launches_e if "k_extend" in tr else None
+    extend_alone = {"kernel": "k_extend (closest hit only, separate-kernel schedule)", "achieved": achieved,
+                    "frac": achieved / peak, "traffic": traffic,
+                    "dram_gbs": None if traffic is None else traffic / (avg_ms / 1e3) / 1e9,
+                    "alg_bytes_per_launch": alg_bytes / launches_e, "avg_launch_ms": avg_ms,
+                    "rays_per_launch": rays / launches_e, "node_visits_per_ray": nv / max(1, rays),
+                    "tri_tests_per_ray": nt / max(1, rays)}
+
+    # the same render with the fused schedule the timed renders use: per-launch device time of
+    # k_trace_pair (this iteration's extend rays + the previous iteration's shadow rays)
+    if batch_jobs is not None:
+        scene.render_batch(batch_jobs, queue_capacity=qc, profile=3, **knobs)
+    else:
+        scene.render_device(film.data_ptr(), spp=spp, seed=99, queue_capacity=qc, profile=3,
+                            guiding=1 if args.workload == "door" else 0, **knobs)
+    p3 = scene.stats
+    k3_ms = dict(zip(kn, p3["kernel_ms"]))
+    k3_cnt = dict(zip(kn, p3["kernel_count"]))
+    k3_items = dict(zip(kn, p3["kernel_items"]))
+    rays_e, rays_s = k3_items["extend"], k3_items["shadow"]
+    # shadow ray: 32 B in + 4 B visibility out; same node / triangle terms
+    alg_pair = (48 * rays_e + 36 * rays_s + 64 * (p3["extend_node_visits"] + p3["shadow_node_visits"]) +
+                48 * (p3["extend_tri_tests"] + p3["shadow_tri_tests"]))
+    launches_p = max(1, k3_cnt["extend"] + k3_cnt["shadow"])      # pair launches + the final shadow launch
+    pair_ms = (k3_ms["extend"] + k3_ms["shadow"]) / launches_p
+    achieved_p = (alg_pair / launches_p) / (pair_ms / 1e3) / 1e9
+    traffic_p = (tr["k_trace_pair"]["dram_bytes_per_ray"] * (rays_e + rays_s) / launches_p
+                 if "k_trace_pair" in tr else None)
+    roofline = {"bound": "hbm", "achieved": achieved_p, "peak": peak, "unit": "GB/s", "frac": achieved_p / peak,
+                "traffic": traffic_p, "peak_kind": peak_kind,
+                "kernel": "k_trace_pair (closest hit of this iteration's rays + any hit of the previous "
+                          "iteration's shadow rays, one persistent launch; the timed renders' traversal kernel)",
+                "dram_gbs": None if traffic_p is None else traffic_p / (pair_ms / 1e3) / 1e9,
+                "alg_bytes_per_launch": alg_pair / launches_p, "avg_launch_ms": pair_ms,
+                "extend_rays_per_launch": rays_e / launches_p, "shadow_rays_per_launch": rays_s / launches_p,
+                "node_visits_per_ray": (p3["extend_node_visits"] + p3["shadow_node_visits"]) / max(1, rays_e + rays_s),
+                "tri_tests_per_ray": (p3["extend_tri_tests"] + p3["shadow_tri_tests"]) / max(1, rays_e + rays_s),
+                "traversal_share_fused": (k3_ms["extend"] + k3_ms["shadow"]) / max(1e-9, sum(k3_ms.values())),
+                "k_extend_alone": extend_alone,
                 "kernel_share": {k: k_ms[k] / max(1e-9, sum(k_ms.values())) for k in kn}}
 
     if batch_jobs is None:

@@ -46,8 +46,12 @@ typedef struct wr_render_desc {
     int grid_shade;          /* persistent blocks of shade / raygen; 0 = occupancy-derived */
     int use_graph;           /* 1: the whole render is one CUDA-graph launch (while-loop node over the
                                 bounce iterations); 0: host-driven launches */
-    int profile;             /* 0: off; 1: per-kernel CUDA-event timing (plain launches);
-                                2: timing + traversal counters (node visits, triangle tests) */
+    int profile;             /* 0: off; 1: per-kernel CUDA-event timing (plain launches, extend and
+                                shadow rays in separate kernels); 2: timing + traversal counters
+                                (node visits, triangle tests); 3: as 2 with the fused schedule of
+                                unprofiled renders (WR_K_EXTEND times the kernel that traces each
+                                iteration's extend rays with the previous iteration's shadow rays,
+                                WR_K_SHADOW the last iteration's shadow rays) */
     int trace_block;         /* threads per block of the traversal kernels: 64, 128 or 256; 0 = 128 */
     int integrator;          /* 0: the render entry's "integrator" (default nextevent_path_tracer);
                                 1: nextevent_path_tracer; 2: primitive_path_tracer; 3: light_splatting */

@@ -659,11 +659,28 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
             WR_CUDA(cudaEventSynchronize(s.kev[1]));
             float ms = 0.f;
             WR_CUDA(cudaEventElapsedTime(&ms, s.kev[0], s.kev[1]));
-            s.stats.kernel_ms[which] += ms;
-            s.stats.kernel_count[which] += 1;
+            // profile 3 (fused schedule): the pair kernel is booked as extend, the flush as shadow
+            const int slot = which == wrk::KERNEL_TRACE_PAIR ? WR_K_EXTEND
+                           : which == wrk::KERNEL_SHADOW_FLUSH ? WR_K_SHADOW : which;
+            s.stats.kernel_ms[slot] += ms;
+            s.stats.kernel_count[slot] += 1;
             launches += 1;
         };
-        if (trace) {
+        if (trace && profile >= 3) {
+            timed(wrk::KERNEL_RAYGEN, 1);
+            timed(wrk::KERNEL_ADVANCE, 1);
+            int parity = 0;
+            while (true) {
+                for (int k : {wrk::KERNEL_TRACE_PAIR, wrk::KERNEL_GUIDE, wrk::KERNEL_SHADE, wrk::KERNEL_RAYGEN,
+                              wrk::KERNEL_ADVANCE})
+                    if (k != wrk::KERNEL_GUIDE || po.guide) timed(k, parity);
+                parity ^= 1;
+                WR_CUDA(cudaMemcpyAsync(s.pinned, b.ctr, wrd::CTR_COUNT * 4, cudaMemcpyDeviceToHost, st));
+                WR_CUDA(cudaStreamSynchronize(st));
+                if (s.pinned[wrd::CTR_DONE]) break;
+            }
+            timed(wrk::KERNEL_SHADOW_FLUSH, 0);
+        } else if (trace) {
             timed(wrk::KERNEL_RAYGEN, 1);
             timed(wrk::KERNEL_SHADOW, 1);
             timed(wrk::KERNEL_ADVANCE, 1);
@@ -791,7 +808,7 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     // kernels per render (a graph launch runs the same kernels). Profiled: prime 3 + 5 (6 with
     // guiding) per iteration + resolve; fused schedule: prime 2 + 4 (5) per iteration + the last
     // shadow rays + resolve
-    if (profile)
+    if (profile == 1 || profile == 2)
         s.stats.kernel_launches = trace ? 3ull + (po.guide ? 6ull : 5ull) * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
     else
         s.stats.kernel_launches = trace ? 2ull + (po.guide ? 5ull : 4ull) * s.pinned[wrd::CTR_ITER] + 2ull : 1ull;

@@ -452,9 +452,12 @@ __device__ __forceinline__ void trace_queue(const DevScene &s, const WaveArgs &w
             }
         }
     }
-    if (w.prof) {
-        atomicAdd(w.prof + (SHADOW ? 8 : 6), (unsigned long long)nv);
-        atomicAdd(w.prof + (SHADOW ? 9 : 7), (unsigned long long)nt);
+    if (w.prof) {   // the whole warp leaves the loop together: one atomic per warp and counter
+        const uint32_t wnv = __reduce_add_sync(0xffffffffu, nv), wnt = __reduce_add_sync(0xffffffffu, nt);
+        if (lane == 0) {
+            atomicAdd(w.prof + (SHADOW ? 8 : 6), (unsigned long long)wnv);
+            atomicAdd(w.prof + (SHADOW ? 9 : 7), (unsigned long long)wnt);
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + (SHADOW ? 3 : 0), (unsigned long long)n);
     }
 }
@@ -1174,6 +1177,8 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
             break;
         case KERNEL_RAYGEN: k_raygen<<<r.grid_shade, kShadeBlock, 0, st>>>(s, w); break;
         case KERNEL_SHADOW: launch_trace(TRACE_SHADOW, s, w, r, st); break;
+        case KERNEL_TRACE_PAIR: launch_trace(TRACE_PAIR, s, w, r, st); break;
+        case KERNEL_SHADOW_FLUSH: launch_trace(TRACE_SHADOW_PENDING, s, w, r, st); break;
         case KERNEL_ADVANCE: k_advance<<<1, 1, 0, st>>>(w); break;
         default: break;
     }

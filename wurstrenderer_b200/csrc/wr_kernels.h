@@ -46,7 +46,9 @@ struct RenderLaunch {
 };
 
 enum KernelId { KERNEL_EXTEND = 0, KERNEL_SHADE = 1, KERNEL_RAYGEN = 2, KERNEL_SHADOW = 3, KERNEL_ADVANCE = 4,
-                KERNEL_RESOLVE = 5, KERNEL_GUIDE = 6 };
+                KERNEL_RESOLVE = 5, KERNEL_GUIDE = 6,
+                // fused schedule: extend + the previous iteration's shadow rays; the last shadow rays
+                KERNEL_TRACE_PAIR = 8, KERNEL_SHADOW_FLUSH = 9 };
 
 void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const RenderLaunch &r, int parity,
                    cudaStream_t st);
