@@ -178,3 +178,29 @@ def test_light_splatting_under_sky_flux(wr_lib):
         img = np.mean([sc.render(spp=512, seed=500 + i) for i in range(8)], axis=0)
     assert np.isfinite(img).all()
     assert abs(img.mean() / ref.mean() - 1.0) < 0.04, (img.mean(), ref.mean())
+
+
+def test_profiled_schedules_agree(wr_lib):
+    """The separate-kernel schedule (profile 1 / 2) and the fused one (unprofiled renders and
+    profile 3: each iteration's extend rays traced with the previous iteration's shadow rays) add
+    the same contributions; only the FP64 atomic order may differ."""
+    path, _ = golden_scene("zoo")
+    with wr_lib.Scene.from_file(path) as sc:
+        a = sc.render(spp=32, seed=5)
+        fused = sc.stats
+        b = sc.render(spp=32, seed=5, profile=2)
+        sep = sc.stats
+        c = sc.render(spp=32, seed=5, profile=3)
+        p3 = sc.stats
+    assert np.allclose(a, b, rtol=1e-9, atol=1e-12)
+    assert np.allclose(a, c, rtol=1e-9, atol=1e-12)
+    k = wr_lib.KERNELS
+    n2, n3 = dict(zip(k, sep["kernel_count"])), dict(zip(k, p3["kernel_count"]))
+    i2, i3 = dict(zip(k, sep["kernel_items"])), dict(zip(k, p3["kernel_items"]))
+    # "iterations" counts the bookkeeping launches, the first wavefront's included
+    assert n3["extend"] == p3["iterations"] - 1 and n3["shadow"] == 1      # pair launches + the last shadow rays
+    assert n2["extend"] == sep["iterations"] - 1 and n2["shadow"] == sep["iterations"]
+    assert i3["extend"] == i2["extend"] and i3["shadow"] == i2["shadow"]   # the same rays either way
+    assert p3["shadow_node_visits"] == sep["shadow_node_visits"] and p3["extend_tri_tests"] == sep["extend_tri_tests"]
+    assert fused["kernel_launches"] == 2 + 4 * (fused["iterations"] - 1) + 2
+    assert sep["kernel_launches"] == 3 + 5 * (sep["iterations"] - 1) + 1

@@ -805,13 +805,15 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     s.stats.render_ms = ms;
     s.stats.paths = total;
     s.stats.iterations = trace ? s.pinned[wrd::CTR_ITER] : 0;
-    // kernels per render (a graph launch runs the same kernels). Profiled: prime 3 + 5 (6 with
-    // guiding) per iteration + resolve; fused schedule: prime 2 + 4 (5) per iteration + the last
-    // shadow rays + resolve
+    // kernels per render (a graph launch runs the same kernels). CTR_ITER counts the bookkeeping
+    // launches, the first wavefront's included. Separate kernels (profile 1 / 2): prime 3 + 5 (6
+    // with guiding) per further iteration + resolve; fused schedule: prime 2 + 4 (5) per further
+    // iteration + the last shadow rays + resolve
+    const unsigned long long iters = s.pinned[wrd::CTR_ITER] > 0 ? s.pinned[wrd::CTR_ITER] - 1ull : 0ull;
     if (profile == 1 || profile == 2)
-        s.stats.kernel_launches = trace ? 3ull + (po.guide ? 6ull : 5ull) * s.pinned[wrd::CTR_ITER] + 1ull : 1ull;
+        s.stats.kernel_launches = trace ? 3ull + (po.guide ? 6ull : 5ull) * iters + 1ull : 1ull;
     else
-        s.stats.kernel_launches = trace ? 2ull + (po.guide ? 5ull : 4ull) * s.pinned[wrd::CTR_ITER] + 2ull : 1ull;
+        s.stats.kernel_launches = trace ? 2ull + (po.guide ? 5ull : 4ull) * iters + 2ull : 1ull;
     s.stats.max_shadow_queue = s.pinned[wrd::CTR_SHADOW_MAX];
     s.stats.queue_capacity = capacity;
     s.stats.grid_trace = r.grid_trace;
