@@ -201,6 +201,9 @@ def test_profiled_schedules_agree(wr_lib):
     assert n3["extend"] == p3["iterations"] - 1 and n3["shadow"] == 1      # pair launches + the last shadow rays
     assert n2["extend"] == sep["iterations"] - 1 and n2["shadow"] == sep["iterations"]
     assert i3["extend"] == i2["extend"] and i3["shadow"] == i2["shadow"]   # the same rays either way
-    assert p3["shadow_node_visits"] == sep["shadow_node_visits"] and p3["extend_tri_tests"] == sep["extend_tri_tests"]
+    # node visits and triangle tests depend slightly on which rays share a warp (a lane holding a
+    # postponed leaf keeps descending until the warp's other lanes hold one too), not the hits
+    for key in ("extend_node_visits", "extend_tri_tests", "shadow_node_visits", "shadow_tri_tests"):
+        assert abs(p3[key] / sep[key] - 1.0) < 0.01, key
     assert fused["kernel_launches"] == 2 + 4 * (fused["iterations"] - 1) + 2
     assert sep["kernel_launches"] == 3 + 5 * (sep["iterations"] - 1) + 1
