@@ -156,9 +156,14 @@ int wr_scene_create_from_json(const char *json_text, const char *base_dir, wr_sc
 void wr_scene_destroy(wr_scene *scene);
 
 /* Host-only validation of a scene (no GPU needed): parses the JSON and its
- * meshes and builds the BVH exactly as wr_scene_create does, fills `info`
- * (build_ms covers parse + BVH only) and uploads nothing. */
+ * meshes and builds the host SAH BVH as wr_scene_create does, fills `info`
+ * (build_ms covers parse + BVH only) and uploads nothing. Phong tessellation
+ * surfaces enter as their triangles (wr_scene_create bounds each patch). */
 int wr_scene_inspect(const char *scene_json_path, wr_scene_info *info);
+
+/* Same with build options (opts may be NULL: defaults; the host SAH builder only,
+ * WR_ERR_UNSUPPORTED for WR_BVH_DEVICE_LBVH). */
+int wr_scene_inspect_ex(const char *scene_json_path, const wr_scene_options *opts, wr_scene_info *info);
 
 int wr_scene_get_info(const wr_scene *scene, wr_scene_info *info);
 

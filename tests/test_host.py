@@ -4,6 +4,7 @@ Covers: the C ABI library loads and exports every function include/wurst_b200.h
 declares; scene loading (simple2 JSON, OBJ/MTL, PFM) and the BVH build agree
 with the oracle's reading of the same files; error statuses; the CLI flags.
 """
+import ctypes
 import os
 import re
 import subprocess
@@ -152,3 +153,29 @@ def test_heightfield_workload_size(wr_lib, tmp_path):
     assert info["num_lights"] == 4
     assert (info["width"], info["height"], info["num_spp"], info["num_path_vertices"]) == (1024, 512, 64, 18)
     assert info["bvh_depth"] <= 64
+
+
+def test_inspect_build_options(wr_lib):
+    """Leaf size, SAH traversal cost and BVH width through the host-only inspect: one triangle per
+    leaf gives n - 1 inner nodes; a dearer traversal step gives fewer nodes; the 8-wide tree is
+    shallower; bad options fail with WR_ERR_INVALID_ARGUMENT, the device LBVH with UNSUPPORTED."""
+    path, _ = golden_scene("hf")
+    base = wr_lib.inspect_scene(path)
+    n = base["num_triangles"]
+    assert wr_lib.inspect_scene(path, max_leaf=1)["bvh_nodes"] == n - 1
+    leaf4 = wr_lib.inspect_scene(path, max_leaf=4)
+    assert leaf4["bvh_nodes"] <= base["bvh_nodes"] < n - 1          # default: 2 per leaf
+    dear = wr_lib.inspect_scene(path, max_leaf=8, sah_trav_cost=4.0)
+    assert dear["bvh_nodes"] < leaf4["bvh_nodes"]
+    wide = wr_lib.inspect_scene(path, bvh_width=8)
+    assert wide["bvh_depth"] < base["bvh_depth"] and wide["bvh_nodes"] < base["bvh_nodes"]
+    for bad in (dict(max_leaf=17), dict(max_leaf=-1), dict(bvh_width=4), dict(sah_trav_cost=-1.0),
+                dict(sah_trav_cost=200.0)):
+        with pytest.raises(wr_lib.WurstError) as e:
+            wr_lib.inspect_scene(path, **bad)
+        assert e.value.status == 1, bad
+    L = wr_lib.load_library()
+    opts = wr_lib.SceneOptions()
+    opts.bvh_builder = wr_lib.BVH_DEVICE_LBVH
+    info = wr_lib.SceneInfo()
+    assert L.wr_scene_inspect_ex(path.encode(), ctypes.byref(opts), ctypes.byref(info)) == 4   # WR_ERR_UNSUPPORTED

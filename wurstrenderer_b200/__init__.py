@@ -89,7 +89,7 @@ BVH_DEVICE_LBVH = 1
 
 
 # every function the C ABI exports (include/wurst_b200.h)
-EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_get_info",
+EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json", "wr_scene_destroy", "wr_scene_inspect", "wr_scene_inspect_ex", "wr_scene_get_info",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_hits", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_read_image", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH):
     L.wr_scene_destroy.restype = None
     L.wr_scene_get_info.argtypes = [vp, ctypes.POINTER(SceneInfo)]
     L.wr_scene_inspect.argtypes = [cp, ctypes.POINTER(SceneInfo)]
+    L.wr_scene_inspect_ex.argtypes = [cp, ctypes.POINTER(SceneOptions), ctypes.POINTER(SceneInfo)]
     L.wr_scene_set_camera_json.argtypes = [vp, cp]
     L.wr_render.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
     L.wr_render_device.argtypes = [vp, ctypes.POINTER(RenderDesc), fp]
@@ -404,10 +405,16 @@ def set_device(device: int) -> None:
     _check(load_library().wr_set_device(int(device)))
 
 
-def inspect_scene(json_path: str) -> dict:
-    """Host-only scene validation (parse + BVH build, no GPU): returns the scene info."""
+def inspect_scene(json_path: str, max_leaf: int = 0, bvh_width: int = 0, sah_trav_cost: float = 0.0) -> dict:
+    """Host-only scene validation (parse + host SAH BVH build, no GPU): returns the scene info.
+    The build options mean what they mean for Scene.from_file."""
     inf = SceneInfo()
-    _check(load_library().wr_scene_inspect(os.fspath(json_path).encode(), ctypes.byref(inf)))
+    opts = SceneOptions()
+    opts.bvh_builder = BVH_HOST_SAH
+    opts.max_leaf = int(max_leaf)
+    opts.bvh_width = int(bvh_width)
+    opts.sah_trav_cost_milli = int(round(float(sah_trav_cost) * 1000))
+    _check(load_library().wr_scene_inspect_ex(os.fspath(json_path).encode(), ctypes.byref(opts), ctypes.byref(inf)))
     return {k: getattr(inf, k) for k, _ in SceneInfo._fields_}
 
 

@@ -1120,18 +1120,25 @@ void trace_batch(wr_scene &s, const float *rays, int n, int any_hit, std::vector
     if (nt) *nt = vis[1];
 }
 
+// build options checked, bvh_width 0 replaced by the default
+wr_scene_options checked_options(const wr_scene_options *opts) {
+    wr_scene_options o{};
+    if (opts) o = *opts;
+    if (o.bvh_builder != WR_BVH_HOST_SAH && o.bvh_builder != WR_BVH_DEVICE_LBVH)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "unknown bvh_builder");
+    if (o.bvh_width == 0) o.bvh_width = WR_BVH_WIDTH_DEFAULT;
+    if (o.bvh_width != 2 && o.bvh_width != 8) throw Error(WR_ERR_INVALID_ARGUMENT, "bvh_width must be 2 or 8");
+    if (o.max_leaf < 0 || o.max_leaf > 16) throw Error(WR_ERR_INVALID_ARGUMENT, "max_leaf must be in 0..16");
+    if (o.sah_trav_cost_milli < 0 || o.sah_trav_cost_milli > 100000)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "sah_trav_cost_milli must be in 0..100000");
+    if (o.sah_patch_cost_milli < 0 || o.sah_patch_cost_milli > 1000000)
+        throw Error(WR_ERR_INVALID_ARGUMENT, "sah_patch_cost_milli must be in 0..1000000");
+    return o;
+}
+
 std::unique_ptr<wr_scene> create(wr::Scene &&host, const wr_scene_options *opts = nullptr) {
     std::unique_ptr<wr_scene> s(new wr_scene());
-    if (opts) s->opts = *opts;
-    if (s->opts.bvh_builder != WR_BVH_HOST_SAH && s->opts.bvh_builder != WR_BVH_DEVICE_LBVH)
-        throw Error(WR_ERR_INVALID_ARGUMENT, "unknown bvh_builder");
-    if (s->opts.bvh_width == 0) s->opts.bvh_width = WR_BVH_WIDTH_DEFAULT;
-    if (s->opts.bvh_width != 2 && s->opts.bvh_width != 8)
-        throw Error(WR_ERR_INVALID_ARGUMENT, "bvh_width must be 2 or 8");
-    if (s->opts.sah_trav_cost_milli < 0 || s->opts.sah_trav_cost_milli > 100000)
-        throw Error(WR_ERR_INVALID_ARGUMENT, "sah_trav_cost_milli must be in 0..100000");
-    if (s->opts.sah_patch_cost_milli < 0 || s->opts.sah_patch_cost_milli > 1000000)
-        throw Error(WR_ERR_INVALID_ARGUMENT, "sah_patch_cost_milli must be in 0..1000000");
+    s->opts = checked_options(opts);
     s->host = std::move(host);
     build_device_scene(*s);
     return s;
@@ -1214,9 +1221,14 @@ int wr_scene_create_from_json(const char *json_text, const char *base_dir, wr_sc
 
 void wr_scene_destroy(wr_scene *s) { delete s; }
 
-int wr_scene_inspect(const char *path, wr_scene_info *info) {
+int wr_scene_inspect(const char *path, wr_scene_info *info) { return wr_scene_inspect_ex(path, nullptr, info); }
+
+int wr_scene_inspect_ex(const char *path, const wr_scene_options *opts, wr_scene_info *info) {
     if (!path || !info) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
     try {
+        const wr_scene_options o = checked_options(opts);
+        if (o.bvh_builder != WR_BVH_HOST_SAH)
+            throw Error(WR_ERR_UNSUPPORTED, "inspect builds the host SAH tree only (the LBVH is built on the device)");
         const auto t0 = std::chrono::steady_clock::now();
         wr::Scene h = wr::load_simple2_file(path);
         std::vector<float> verts;
@@ -1224,7 +1236,16 @@ int wr_scene_inspect(const char *path, wr_scene_info *info) {
         for (const wr::Mesh &m : h.meshes)
             for (uint32_t i : m.indices)
                 for (int k = 0; k < 3; ++k) verts.push_back(m.positions[3 * size_t(i) + k]);
-        wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, WR_MAX_LEAF_DEFAULT, 0);
+        const bool wide = o.bvh_width == 8;
+        const int ml = o.max_leaf > 0 ? o.max_leaf : WR_MAX_LEAF_DEFAULT;
+        const double ct = o.sah_trav_cost_milli > 0 ? o.sah_trav_cost_milli * 1e-3 : 1.0;
+        wr::BvhBuildResult bvh = wr::build_bvh_sah(verts, wide ? std::min(ml, 3) : ml, 0, ct);
+        int nodes = int(bvh.nodes.size() / 16);
+        if (wide) {
+            const wr::WideBvh wb = wr::build_wide8(bvh);
+            nodes = int(wb.nodes.size() / 20);
+            bvh.depth = wb.depth;
+        }
         memset(info, 0, sizeof(*info));
         info->width = h.has_camera ? h.camera.width : 0;
         info->height = h.has_camera ? h.camera.height : 0;
@@ -1234,7 +1255,7 @@ int wr_scene_inspect(const char *path, wr_scene_info *info) {
         info->num_meshes = int(h.meshes.size());
         info->num_lights = int(h.lights.size());
         info->has_envmap = h.has_env ? 1 : 0;
-        info->bvh_nodes = int(bvh.nodes.size() / 16);
+        info->bvh_nodes = nodes;
         info->bvh_depth = bvh.depth;
         info->bvh_sah_cost = bvh.sah_cost;
         info->num_renders = int(h.renders.size());
