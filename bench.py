@@ -571,6 +571,9 @@ def main():
                 "kernel": "k_trace_pair (closest hit of this iteration's rays + any hit of the previous "
                           "iteration's shadow rays, one persistent launch; the timed renders' traversal kernel)",
                 "dram_gbs": None if traffic_p is None else traffic_p / (pair_ms / 1e3) / 1e9,
+                # measured DRAM bytes over the same time: the HBM share actually used (the
+                # algorithmic bytes are mostly L1 / L2 hits, so `frac` can exceed 1)
+                "dram_frac": None if traffic_p is None else traffic_p / (pair_ms / 1e3) / 1e9 / peak,
                 "alg_bytes_per_launch": alg_pair / launches_p, "avg_launch_ms": pair_ms,
                 "extend_rays_per_launch": rays_e / launches_p, "shadow_rays_per_launch": rays_s / launches_p,
                 "node_visits_per_ray": (p3["extend_node_visits"] + p3["shadow_node_visits"]) / max(1, rays_e + rays_s),
