@@ -14,7 +14,8 @@
 // carries a box at +infinity so that it is never entered. Nodes are stored in
 // depth-first order (left child right after its parent) so that a traversal
 // descending to the near child mostly touches adjacent cache lines.
-// Top levels are built in parallel with std::thread.
+// Top levels are built in parallel with std::thread, and the bounds and bins of long ranges are
+// gathered by several threads.
 
 #include <algorithm>
 #include <atomic>
@@ -53,35 +54,79 @@ struct TmpNode {
 constexpr int kBins = 32;
 constexpr uint32_t kMaxLeafHard = 16;   // 4-bit count field
 constexpr int kDepthBudget = 60;         // traversal stack holds 64 entries
+constexpr uint32_t kParallelRange = 1u << 18;   // ranges at least this long are binned by several threads
+constexpr uint32_t kChunk = 1u << 16;           // primitives per thread at least
+constexpr uint32_t kSpawnRange = 1u << 13;      // subtrees at least this large may get a thread
+
+// SAH bins of one range for all three axes. Merging two bin sets gives exactly the bins of the
+// union (box min / max; counts; weights that are small integers in the scenes built here), so the
+// tree does not depend on how a range was split between threads.
+struct BinSet {
+    Aabb box[3][kBins];
+    uint32_t cnt[3][kBins] = {};
+    double w[3][kBins] = {};
+    void merge(const BinSet &o) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < kBins; ++b) {
+                box[a][b].grow(o.box[a][b]);
+                cnt[a][b] += o.cnt[a][b];
+                w[a][b] += o.w[a][b];
+            }
+    }
+};
+
+// splits [start, start + count) into up to `threads` chunks run in parallel; f(a, b, chunk)
+template <class F>
+int for_chunks(uint32_t start, uint32_t count, int threads, F &&f) {
+    const int parts = count >= kParallelRange ? int(std::min<uint32_t>(uint32_t(std::max(threads, 1)), count / kChunk)) : 1;
+    if (parts <= 1) {
+        f(start, start + count, 0);
+        return 1;
+    }
+    const uint32_t step = (count + uint32_t(parts) - 1) / uint32_t(parts);
+    std::vector<std::future<void>> fut;
+    for (int p = 1; p < parts; ++p) {
+        const uint32_t a = start + std::min(count, uint32_t(p) * step), b = start + std::min(count, uint32_t(p + 1) * step);
+        fut.push_back(std::async(std::launch::async, [&f, a, b, p] { f(a, b, p); }));
+    }
+    f(start, start + std::min(count, step), 0);
+    for (auto &x : fut) x.get();
+    return parts;
+}
+
+// one primitive's build record; the records are partitioned in place, so every pass over a
+// node's range reads contiguous memory
+struct Prim {
+    Aabb box;
+    float c[3];      // centroid of the box
+    uint32_t id;     // input order
+    float w;         // SAH cost of its test
+};
 
 struct Builder {
     const std::vector<float> &v;       // 9 floats per triangle
-    std::vector<Aabb> tbox;
-    std::vector<float> cen;            // 3 per triangle
-    std::vector<uint32_t> idx;
+    std::vector<Prim> prims;
     std::vector<TmpNode> nodes;
-    std::atomic<int> next_node{0};
     int max_leaf;
     double trav_cost;                  // SAH cost of a traversal step, relative to a triangle test
     const std::vector<float> *prim_cost;   // SAH cost of each primitive's test (null: 1 each)
-    int par_depth;
+    int nthreads;
+    std::atomic<int> spawned{0};       // subtree threads running besides the caller's
 
     Builder(const std::vector<float> &verts, int ml, int threads, double ct, const std::vector<float> *pc)
-        : v(verts), max_leaf(ml), trav_cost(ct), prim_cost(pc) {
+        : v(verts), max_leaf(ml), trav_cost(ct), prim_cost(pc), nthreads(threads) {
         const size_t n = v.size() / 9;
-        tbox.resize(n);
-        cen.resize(3 * n);
-        idx.resize(n);
+        prims.resize(n);
         nodes.resize(std::max<size_t>(2 * n + 1, 3));
-        par_depth = 0;
-        while ((1 << par_depth) < threads * 2) ++par_depth;
         auto prep = [&](size_t a, size_t b) {
             for (size_t i = a; i < b; ++i) {
+                Prim &q = prims[i];
                 Aabb bb;
                 for (int c = 0; c < 3; ++c) bb.grow(&v[9 * i + 3 * c]);
-                tbox[i] = bb;
-                for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5f * (bb.lo[k] + bb.hi[k]);
-                idx[i] = uint32_t(i);
+                q.box = bb;
+                for (int k = 0; k < 3; ++k) q.c[k] = 0.5f * (bb.lo[k] + bb.hi[k]);
+                q.id = uint32_t(i);
+                q.w = prim_cost ? (*prim_cost)[i] : 1.f;
             }
         };
         std::vector<std::thread> th;
@@ -93,38 +138,76 @@ struct Builder {
         for (auto &x : th) x.join();
     }
 
-    int alloc() { return next_node.fetch_add(1); }
+    // Node slots without a shared counter: a subtree over c primitives has at most 2c - 1 nodes,
+    // so the node of a range owns the 2c - 1 slots from its own index; its left child takes the
+    // next slot (and 2 nl - 1 slots), its right child the slots after those.
 
-    // builds the subtree over idx[start, start+count) into node `ni`
+    // builds the subtree over prims[start, start+count) into node `ni`
     void build(int ni, uint32_t start, uint32_t count, int depth) {
         TmpNode &nd = nodes[ni];
-        Aabb box, cb;
-        for (uint32_t i = start; i < start + count; ++i) {
-            const uint32_t t = idx[i];
-            box.grow(tbox[t]);
-            cb.grow(&cen[3 * size_t(t)]);
+        Aabb box, cb;   // node box and centroid box
+        auto bound = [&](uint32_t a, uint32_t b, Aabb &bb, Aabb &cc) {
+            for (uint32_t i = a; i < b; ++i) {
+                bb.grow(prims[i].box);
+                cc.grow(prims[i].c);
+            }
+        };
+        if (count < kParallelRange) {
+            bound(start, start + count, box, cb);
+        } else {
+            std::vector<Aabb> pb(size_t(std::min(nthreads, 64))), pc(pb.size());
+            const int parts = for_chunks(start, count, int(pb.size()), [&](uint32_t a, uint32_t b, int p) {
+                bound(a, b, pb[size_t(p)], pc[size_t(p)]);
+            });
+            for (int p = 0; p < parts; ++p) { box.grow(pb[size_t(p)]); cb.grow(pc[size_t(p)]); }
         }
         nd.box = box;
         if (count <= 1) { nd.start = start; nd.count = count; return; }
-        auto weight = [&](uint32_t t) { return prim_cost ? double((*prim_cost)[t]) : 1.0; };
 
-        // binned SAH over the three axes
-        int best_axis = -1, best_split = -1;
-        double best_cost = INFINITY;
+        // binned SAH over the three axes: one pass over the primitives fills the bins of all three
+        float scale[3];
+        bool axis_ok[3];
         for (int ax = 0; ax < 3; ++ax) {
             const float ext = cb.hi[ax] - cb.lo[ax];
-            if (!(ext > 0.f)) continue;
-            const float scale = kBins / ext;
-            Aabb bins[kBins];
-            uint32_t cnt[kBins] = {0};
-            double wsum[kBins] = {0.0};
-            for (uint32_t i = start; i < start + count; ++i) {
-                const uint32_t t = idx[i];
-                int b = int((cen[3 * size_t(t) + ax] - cb.lo[ax]) * scale);
-                b = std::min(std::max(b, 0), kBins - 1);
-                cnt[b]++;
-                wsum[b] += weight(t);
-                bins[b].grow(tbox[t]);
+            axis_ok[ax] = ext > 0.f;
+            scale[ax] = axis_ok[ax] ? kBins / ext : 0.f;
+        }
+        auto fill = [&](uint32_t a, uint32_t b, BinSet &bs) {
+            for (uint32_t i = a; i < b; ++i) {
+                const Prim &q = prims[i];
+                const Aabb &tb = q.box;
+                const double wt = double(q.w);
+                for (int ax = 0; ax < 3; ++ax) {
+                    if (!axis_ok[ax]) continue;
+                    int bi = int((q.c[ax] - cb.lo[ax]) * scale[ax]);
+                    bi = std::min(std::max(bi, 0), kBins - 1);
+                    bs.box[ax][bi].grow(tb);
+                    bs.cnt[ax][bi]++;
+                    bs.w[ax][bi] += wt;
+                }
+            }
+        };
+        BinSet bins;
+        if (count < kParallelRange) {
+            fill(start, start + count, bins);
+        } else {
+            std::vector<BinSet> part(size_t(std::min(nthreads, 64)));
+            const int parts = for_chunks(start, count, int(part.size()), [&](uint32_t a, uint32_t b, int p) {
+                fill(a, b, part[size_t(p)]);
+            });
+            for (int p = 0; p < parts; ++p) bins.merge(part[size_t(p)]);
+        }
+        int best_axis = -1, best_split = -1;
+        double best_cost = INFINITY;
+        double total_w = -1.0;   // summed primitive costs (from the bins of any binned axis)
+        for (int ax = 0; ax < 3; ++ax) {
+            if (!axis_ok[ax]) continue;
+            const Aabb *binb = bins.box[ax];
+            const uint32_t *cnt = bins.cnt[ax];
+            const double *wsum = bins.w[ax];
+            if (total_w < 0.0) {
+                total_w = 0.0;
+                for (int b = 0; b < kBins; ++b) total_w += wsum[b];
             }
             double right_area[kBins], right_w[kBins];
             uint32_t right_cnt[kBins];
@@ -132,7 +215,7 @@ struct Builder {
             uint32_t c = 0;
             double w = 0.0;
             for (int b = kBins - 1; b > 0; --b) {
-                acc.grow(bins[b]);
+                acc.grow(binb[b]);
                 c += cnt[b];
                 w += wsum[b];
                 right_area[b] = acc.half_area();
@@ -143,7 +226,7 @@ struct Builder {
             c = 0;
             w = 0.0;
             for (int b = 0; b < kBins - 1; ++b) {
-                acc.grow(bins[b]);
+                acc.grow(binb[b]);
                 c += cnt[b];
                 w += wsum[b];
                 if (c == 0 || right_cnt[b + 1] == 0) continue;
@@ -153,8 +236,11 @@ struct Builder {
         }
         const double parent_area = box.half_area();
         // SAH with traversal cost trav_cost and each primitive's test cost (relative to the parent's area)
-        double leaf_cost = 0.0;
-        for (uint32_t i = start; i < start + count; ++i) leaf_cost += weight(idx[i]);
+        double leaf_cost = total_w;
+        if (leaf_cost < 0.0) {   // no axis was binned (coincident centroids)
+            leaf_cost = 0.0;
+            for (uint32_t i = start; i < start + count; ++i) leaf_cost += double(prims[i].w);
+        }
         const double split_cost = trav_cost + (parent_area > 0 ? best_cost / parent_area : leaf_cost);
         if (count <= uint32_t(max_leaf) && (best_axis < 0 || leaf_cost <= split_cost)) {
             nd.start = start; nd.count = count; return;
@@ -167,26 +253,37 @@ struct Builder {
             int ax = 0;
             for (int k = 1; k < 3; ++k) if (cb.hi[k] - cb.lo[k] > cb.hi[ax] - cb.lo[ax]) ax = k;
             nl = count / 2;
-            std::nth_element(idx.begin() + start, idx.begin() + start + nl, idx.begin() + start + count,
-                             [&](uint32_t a, uint32_t b2) { return cen[3 * size_t(a) + ax] < cen[3 * size_t(b2) + ax]; });
+            std::nth_element(prims.begin() + start, prims.begin() + start + nl, prims.begin() + start + count,
+                             [ax](const Prim &a, const Prim &b2) { return a.c[ax] < b2.c[ax]; });
         } else if (best_axis < 0) {
             nl = count / 2;   // coincident centroids: split the range
         } else {
             const float ext = cb.hi[best_axis] - cb.lo[best_axis];
             const float scale = kBins / ext;
-            auto mid = std::partition(idx.begin() + start, idx.begin() + start + count, [&](uint32_t t) {
-                int b = int((cen[3 * size_t(t) + best_axis] - cb.lo[best_axis]) * scale);
+            auto mid = std::partition(prims.begin() + start, prims.begin() + start + count, [&](const Prim &q) {
+                int b = int((q.c[best_axis] - cb.lo[best_axis]) * scale);
                 b = std::min(std::max(b, 0), kBins - 1);
                 return b <= best_split;
             });
-            nl = uint32_t(mid - (idx.begin() + start));
+            nl = uint32_t(mid - (prims.begin() + start));
             if (nl == 0 || nl == count) nl = count / 2;
         }
-        const int l = alloc(), r = alloc();
+        const int l = ni + 1, r = ni + 2 * int(nl);
         nd.child[0] = l;
         nd.child[1] = r;
-        if (depth < par_depth && count > 65536) {
-            auto fut = std::async(std::launch::async, [&, l, start, nl, depth] { build(l, start, nl, depth + 1); });
+        // subtrees of more than kSpawnRange primitives go to their own thread while fewer than
+        // 2 x nthreads such threads run: SAH splits are uneven, so threads are handed out as the
+        // tree unfolds rather than by depth
+        bool spawn = false;
+        if (nl > kSpawnRange && count - nl > kSpawnRange) {
+            spawn = spawned.fetch_add(1) < 2 * nthreads;
+            if (!spawn) spawned.fetch_sub(1);
+        }
+        if (spawn) {
+            auto fut = std::async(std::launch::async, [&, l, start, nl, depth] {
+                build(l, start, nl, depth + 1);
+                spawned.fetch_sub(1);
+            });
             build(r, start + nl, count - nl, depth + 1);
             fut.get();
         } else {
@@ -220,13 +317,13 @@ BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_lea
     if (n >= (1u << 27)) throw Error(WR_ERR_UNSUPPORTED, "more than 2^27 triangles");
     if (prim_cost && prim_cost->size() != n) throw Error(WR_ERR_INVALID_ARGUMENT, "prim_cost size");
     Builder b(tri_vertices, max_leaf, threads, trav_cost, prim_cost);
-    const int root = b.alloc();
+    const int root = 0;
     if (n > 0) b.build(root, 0, n, 0);
     else b.nodes[root].count = 0;
 
     // depth-first linearisation; the device root is always an inner node
     std::vector<std::pair<int, int>> order;   // (tmp node, device slot)
-    std::vector<int> dev_of(size_t(b.next_node.load()), -1);
+    std::vector<int> dev_of(b.nodes.size(), -1);
     res.tri_order.reserve(n);
     std::vector<float> &out = res.nodes;
     struct Item { int tmp; int depth; };
@@ -256,7 +353,7 @@ BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_lea
         if (nd.child[0] < 0) {
             // the whole scene is one leaf: child 0 holds it, child 1 is empty
             const uint32_t first = uint32_t(res.tri_order.size());
-            for (uint32_t i = nd.start; i < nd.start + nd.count; ++i) res.tri_order.push_back(b.idx[i]);
+            for (uint32_t i = nd.start; i < nd.start + nd.count; ++i) res.tri_order.push_back(b.prims[i].id);
             put_child_box(o, 0, nd.box, nd.count == 0);
             put_child_box(o, 1, nd.box, true);
             child_code[0] = int32_t(0x80000000u | (uint32_t(std::max<uint32_t>(nd.count, 1) - 1) << 27) | first);
@@ -271,7 +368,7 @@ BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_lea
                     child_code[s] = dev_of[nd.child[s]];
                 } else {
                     const uint32_t first = uint32_t(res.tri_order.size());
-                    for (uint32_t i = c.start; i < c.start + c.count; ++i) res.tri_order.push_back(b.idx[i]);
+                    for (uint32_t i = c.start; i < c.start + c.count; ++i) res.tri_order.push_back(b.prims[i].id);
                     child_code[s] = int32_t(0x80000000u | ((c.count - 1) << 27) | first);
                     res.sah_cost += c.box.half_area() / root_area * c.count;
                 }
