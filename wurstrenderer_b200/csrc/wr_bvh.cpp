@@ -22,7 +22,9 @@
 #include <cmath>
 #include <cstring>
 #include <future>
+#include <new>
 #include <thread>
+#include <type_traits>
 
 #include "wr_host.h"
 
@@ -103,10 +105,31 @@ struct Prim {
     float w;         // SAH cost of its test
 };
 
+// Array of trivially destructible objects whose storage is not initialised on allocation: the
+// builder constructs its elements in parallel (hundreds of MB for 10M primitives).
+template <class T>
+struct RawArray {
+    static_assert(std::is_trivially_destructible<T>::value, "RawArray holds trivially destructible types");
+    T *p = nullptr;
+    size_t n = 0;
+    RawArray() = default;
+    RawArray(const RawArray &) = delete;
+    RawArray &operator=(const RawArray &) = delete;
+    ~RawArray() { ::operator delete(p); }
+    void allocate(size_t count) {
+        p = static_cast<T *>(::operator new(std::max<size_t>(count, 1) * sizeof(T)));
+        n = count;
+    }
+    T &operator[](size_t i) { return p[i]; }
+    const T &operator[](size_t i) const { return p[i]; }
+    T *begin() { return p; }
+    size_t size() const { return n; }
+};
+
 struct Builder {
     const std::vector<float> &v;       // 9 floats per triangle
-    std::vector<Prim> prims;
-    std::vector<TmpNode> nodes;
+    RawArray<Prim> prims;
+    RawArray<TmpNode> nodes;
     int max_leaf;
     double trav_cost;                  // SAH cost of a traversal step, relative to a triangle test
     const std::vector<float> *prim_cost;   // SAH cost of each primitive's test (null: 1 each)
@@ -116,18 +139,23 @@ struct Builder {
     Builder(const std::vector<float> &verts, int ml, int threads, double ct, const std::vector<float> *pc)
         : v(verts), max_leaf(ml), trav_cost(ct), prim_cost(pc), nthreads(threads) {
         const size_t n = v.size() / 9;
-        prims.resize(n);
-        nodes.resize(std::max<size_t>(2 * n + 1, 3));
+        const size_t nn = std::max<size_t>(2 * n + 1, 3);
+        prims.allocate(n);
+        nodes.allocate(nn);
         auto prep = [&](size_t a, size_t b) {
             for (size_t i = a; i < b; ++i) {
-                Prim &q = prims[i];
+                Prim *q = new (&prims[i]) Prim();
                 Aabb bb;
                 for (int c = 0; c < 3; ++c) bb.grow(&v[9 * i + 3 * c]);
-                q.box = bb;
-                for (int k = 0; k < 3; ++k) q.c[k] = 0.5f * (bb.lo[k] + bb.hi[k]);
-                q.id = uint32_t(i);
-                q.w = prim_cost ? (*prim_cost)[i] : 1.f;
+                q->box = bb;
+                for (int k = 0; k < 3; ++k) q->c[k] = 0.5f * (bb.lo[k] + bb.hi[k]);
+                q->id = uint32_t(i);
+                q->w = prim_cost ? (*prim_cost)[i] : 1.f;
             }
+            // the node slots, 2 per primitive
+            for (size_t i = 2 * a; i < std::min(2 * b, nn); ++i) new (&nodes[i]) TmpNode();
+            if (b == n)
+                for (size_t i = 2 * b; i < nn; ++i) new (&nodes[i]) TmpNode();
         };
         std::vector<std::thread> th;
         const size_t chunk = (n + threads - 1) / std::max(threads, 1);
@@ -136,6 +164,8 @@ struct Builder {
             if (a < b) th.emplace_back(prep, a, b);
         }
         for (auto &x : th) x.join();
+        if (n == 0)
+            for (size_t i = 0; i < nn; ++i) new (&nodes[i]) TmpNode();
     }
 
     // Node slots without a shared counter: a subtree over c primitives has at most 2c - 1 nodes,
@@ -146,11 +176,14 @@ struct Builder {
     void build(int ni, uint32_t start, uint32_t count, int depth) {
         TmpNode &nd = nodes[ni];
         Aabb box, cb;   // node box and centroid box
-        auto bound = [&](uint32_t a, uint32_t b, Aabb &bb, Aabb &cc) {
+        auto bound = [&](uint32_t a, uint32_t b, Aabb &bb_out, Aabb &cc_out) {
+            Aabb bb, cc;   // local: the per-thread outputs sit next to each other
             for (uint32_t i = a; i < b; ++i) {
                 bb.grow(prims[i].box);
                 cc.grow(prims[i].c);
             }
+            bb_out = bb;
+            cc_out = cc;
         };
         if (count < kParallelRange) {
             bound(start, start + count, box, cb);
