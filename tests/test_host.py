@@ -179,3 +179,36 @@ def test_inspect_build_options(wr_lib):
     opts.bvh_builder = wr_lib.BVH_DEVICE_LBVH
     info = wr_lib.SceneInfo()
     assert L.wr_scene_inspect_ex(path.encode(), ctypes.byref(opts), ctypes.byref(info)) == 4   # WR_ERR_UNSUPPORTED
+
+
+def test_obj_number_formats_parse_alike(wr_lib, tmp_path):
+    """The same float32 vertices written plainly and in the other forms strtof reads (hex floats,
+    '+' signs, exponents, tabs, CRLF, relative and '+' face indices) give the same scene: same
+    triangle count and a BVH with the same SAH cost, nodes and depth."""
+    import json
+    rng = np.random.default_rng(11)
+    pts = rng.normal(0.0, 3.0, (300, 3)).astype(np.float32)
+    tris = rng.integers(0, len(pts), (400, 3))
+
+    def fancy(x, k):
+        x = float(x)
+        forms = [x.hex(), ("+%.9g" % x) if x >= 0 else "%.9g" % x, "%.8e" % x, repr(x)]
+        return forms[k % len(forms)]
+
+    plain = ["mtllib m.mtl", "o a", "usemtl w"] + ["v %.9g %.9g %.9g" % tuple(p) for p in pts]
+    plain += ["f %d %d %d" % tuple(t + 1) for t in tris]
+    odd = ["mtllib m.mtl", "o a", "usemtl w"]
+    odd += ["v\t" + "\t ".join(fancy(c, 3 * i + k) for k, c in enumerate(p)) for i, p in enumerate(pts)]
+    odd += ["f %d +%d %d" % (t[0] - len(pts), t[1] + 1, t[2] + 1) for t in tris]   # relative and '+' indices
+    scene = json.load(open(golden_scene("cornell")[0]))
+    infos = []
+    for name, lines, eol in (("plain", plain, "\n"), ("odd", odd, "\r\n")):
+        d = tmp_path / name
+        d.mkdir()
+        (d / "a.obj").write_bytes(eol.join(lines).encode() + eol.encode())
+        (d / "m.mtl").write_text("newmtl w\nKd 0.5 0.5 0.5\n")
+        (d / "s.json").write_text(json.dumps(dict(scene, meshes=[{"path": "a.obj"}])))
+        infos.append(wr_lib.inspect_scene(str(d / "s.json")))
+    a, b = infos
+    assert a["num_triangles"] == b["num_triangles"] == len(tris)
+    assert (a["bvh_sah_cost"], a["bvh_nodes"], a["bvh_depth"]) == (b["bvh_sah_cost"], b["bvh_nodes"], b["bvh_depth"])

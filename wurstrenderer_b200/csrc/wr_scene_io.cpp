@@ -18,7 +18,9 @@
 // Errors are reported as wr::Error with a status code (the reference throws
 // std::runtime_error for the same conditions).
 
+#include <cctype>
 #include <cerrno>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -235,6 +237,36 @@ inline const char *token_end(const char *p, const char *e) {
     return p;
 }
 
+// Numbers of the vertex and face lines: std::from_chars after the line's spaces and an optional
+// '+' (correctly rounded like strtof, without the locale, several times faster); whatever it does
+// not take as a whole (hex floats, out of range, no number) is read by strtol / strtof from the
+// same position as before.
+inline float read_float(char *&p, const char *le) {
+    const char *s = p;
+    while (s < le && (*s == ' ' || *s == '\t')) ++s;
+    if (s < le && *s == '+') ++s;
+    float v = 0.f;
+    const auto r = std::from_chars(s, le, v);
+    // a letter right after the digits: a hex float ("0x1p3") that only strtof reads whole
+    if (r.ec == std::errc() && !(r.ptr < le && isalpha(static_cast<unsigned char>(*r.ptr)))) {
+        p = const_cast<char *>(r.ptr);
+        return v;
+    }
+    return strtof(p, &p);
+}
+
+inline long read_long(const char *p, const char *le, char **end) {
+    const char *s = p;
+    if (s < le && *s == '+') ++s;
+    long v = 0;
+    const auto r = std::from_chars(s, le, v);
+    if (r.ec == std::errc()) {
+        *end = const_cast<char *>(r.ptr);
+        return v;
+    }
+    return strtol(p, end, 10);
+}
+
 void parse_mtl(const std::string &path, std::vector<MtlEntry> &mats, std::unordered_map<std::string, int> &idx) {
     FILE *f = fopen(path.c_str(), "rb");
     if (!f) return;  // a missing library leaves named materials at their defaults
@@ -298,10 +330,10 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
         const char *q = skip_ws(p, le);
         if (q + 1 < le && q[0] == 'v' && (q[1] == ' ' || q[1] == '\t')) {
             char *e2 = const_cast<char *>(q + 1);
-            for (int k = 0; k < 3; ++k) verts.push_back(strtof(e2, &e2));
+            for (int k = 0; k < 3; ++k) verts.push_back(read_float(e2, le));
         } else if (q + 2 < le && q[0] == 'v' && q[1] == 'n' && (q[2] == ' ' || q[2] == '\t')) {
             char *e2 = const_cast<char *>(q + 2);
-            for (int k = 0; k < 3; ++k) norms.push_back(strtof(e2, &e2));
+            for (int k = 0; k < 3; ++k) norms.push_back(read_float(e2, le));
         } else if (q + 1 < le && q[0] == 'f' && (q[1] == ' ' || q[1] == '\t')) {
             if (meshes.empty()) start_mesh("defaultobject");
             poly.clear();
@@ -312,7 +344,7 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
                 r = skip_ws(r, le);
                 if (r >= le) break;
                 char *e2;
-                long v = strtol(r, &e2, 10);
+                long v = read_long(r, le, &e2);
                 if (e2 == r) break;
                 long gi = v < 0 ? nv + v : v - 1;
                 if (gi < 0 || gi >= nv) throw Error(WR_ERR_PARSE, "obj: vertex index out of range in " + path);
@@ -320,10 +352,10 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
                 long ni = -1;   // v, v/vt, v//vn or v/vt/vn
                 if (e2 < le && *e2 == '/') {
                     char *e3 = e2 + 1;
-                    if (e3 < le && *e3 != '/') strtol(e3, &e3, 10);
+                    if (e3 < le && *e3 != '/') read_long(e3, le, &e3);
                     if (e3 < le && *e3 == '/') {
                         char *e4 = e3 + 1;
-                        const long n = strtol(e4, &e3, 10);
+                        const long n = read_long(e4, le, &e3);
                         if (e3 != e4) {
                             ni = n < 0 ? nn + n : n - 1;
                             if (ni < 0 || ni >= nn) throw Error(WR_ERR_PARSE, "obj: normal index out of range in " + path);
