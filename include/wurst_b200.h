@@ -77,7 +77,8 @@ typedef struct wr_render_desc {
 typedef struct wr_render_stats {
     double render_ms;                 /* device time of the bounce loop + resolve */
     unsigned long long paths;         /* camera samples traced (W*H*spp) */
-    unsigned long long iterations;    /* wavefront iterations executed */
+    unsigned long long iterations;    /* bookkeeping launches of the wavefront loop, the first
+                                         wavefront's included (bounce iterations + 1) */
     unsigned int max_shadow_queue;    /* largest shadow-ray queue seen */
     unsigned int queue_capacity;      /* wavefront slots used */
     int grid_trace, grid_shade;       /* persistent blocks used */
