@@ -51,6 +51,7 @@ struct TmpNode {
     Aabb box;
     int child[2] = {-1, -1};
     uint32_t start = 0, count = 0;   // leaf when child[0] < 0
+    int depth = 0;
 };
 
 constexpr int kBins = 32;
@@ -175,6 +176,7 @@ struct Builder {
     // builds the subtree over prims[start, start+count) into node `ni`
     void build(int ni, uint32_t start, uint32_t count, int depth) {
         TmpNode &nd = nodes[ni];
+        nd.depth = depth;
         Aabb box, cb;   // node box and centroid box
         auto bound = [&](uint32_t a, uint32_t b, Aabb &bb_out, Aabb &cc_out) {
             Aabb bb, cc;   // local: the per-thread outputs sit next to each other
@@ -354,61 +356,108 @@ BvhBuildResult build_bvh_sah(const std::vector<float> &tri_vertices, int max_lea
     if (n > 0) b.build(root, 0, n, 0);
     else b.nodes[root].count = 0;
 
-    // depth-first linearisation; the device root is always an inner node
-    std::vector<std::pair<int, int>> order;   // (tmp node, device slot)
-    std::vector<int> dev_of(b.nodes.size(), -1);
-    res.tri_order.reserve(n);
-    std::vector<float> &out = res.nodes;
-    struct Item { int tmp; int depth; };
-    // assign device indices to inner nodes in DFS preorder
-    std::vector<int> inner_order;
-    {
-        std::vector<Item> st{{root, 0}};
-        while (!st.empty()) {
-            Item it = st.back(); st.pop_back();
-            const TmpNode &nd = b.nodes[it.tmp];
-            if (nd.child[0] < 0 && it.tmp != root) continue;
-            dev_of[it.tmp] = int(inner_order.size());
-            inner_order.push_back(it.tmp);
-            res.depth = std::max(res.depth, it.depth + 1);
-            if (nd.child[0] >= 0) {
-                st.push_back({nd.child[1], it.depth + 1});
-                st.push_back({nd.child[0], it.depth + 1});
-            }
+    // Depth-first linearisation; the device root is always an inner node. A node's left child
+    // sits in the next slot and its right subtree after the whole left subtree, so depth-first
+    // preorder is the order of the slots: device indices and triangle offsets are prefix sums
+    // over the slots, computed in parallel chunks.
+    const size_t nn = b.nodes.size();
+    auto inner = [&](size_t i) { return i == size_t(root) || b.nodes[i].child[0] >= 0; };
+    auto leaf_tris = [&](size_t i) -> uint32_t {   // triangles of the leaf children of inner slot i
+        const TmpNode &nd = b.nodes[i];
+        if (nd.child[0] < 0) return nd.count;       // the whole scene is one leaf
+        uint32_t c = 0;
+        for (int s = 0; s < 2; ++s) {
+            const TmpNode &ch = b.nodes[size_t(nd.child[s])];
+            if (ch.child[0] < 0) c += ch.count;
         }
+        return c;
+    };
+    const int parts = int(std::max<size_t>(1, std::min<size_t>(size_t(threads), nn / kChunk)));
+    const size_t step = (nn + size_t(parts) - 1) / size_t(parts);
+    std::vector<size_t> inner_base(size_t(parts) + 1, 0), tri_base(size_t(parts) + 1, 0);
+    std::vector<int> part_depth(size_t(parts), 0);
+    auto run_parts = [&](auto &&fn) {
+        std::vector<std::future<void>> fut;
+        for (int p = 1; p < parts; ++p) fut.push_back(std::async(std::launch::async, [&fn, p] { fn(p); }));
+        fn(0);
+        for (auto &x : fut) x.get();
+    };
+    run_parts([&](int p) {
+        size_t ci = 0, ct = 0;
+        int d = 0;
+        for (size_t i = size_t(p) * step; i < std::min(nn, size_t(p + 1) * step); ++i)
+            if (inner(i)) {
+                ++ci;
+                ct += leaf_tris(i);
+                d = std::max(d, b.nodes[i].depth + 1);
+            }
+        inner_base[size_t(p) + 1] = ci;
+        tri_base[size_t(p) + 1] = ct;
+        part_depth[size_t(p)] = d;
+    });
+    for (int p = 0; p < parts; ++p) {
+        inner_base[size_t(p) + 1] += inner_base[size_t(p)];
+        tri_base[size_t(p) + 1] += tri_base[size_t(p)];
+        res.depth = std::max(res.depth, part_depth[size_t(p)]);
     }
-    out.assign(inner_order.size() * 16, 0.f);
-    const double root_area = std::max(b.nodes[root].box.half_area(), 1e-30);
-    for (size_t di = 0; di < inner_order.size(); ++di) {
-        const TmpNode &nd = b.nodes[inner_order[di]];
-        float *o = &out[di * 16];
-        int32_t child_code[2];
-        if (nd.child[0] < 0) {
-            // the whole scene is one leaf: child 0 holds it, child 1 is empty
-            const uint32_t first = uint32_t(res.tri_order.size());
-            for (uint32_t i = nd.start; i < nd.start + nd.count; ++i) res.tri_order.push_back(b.prims[i].id);
-            put_child_box(o, 0, nd.box, nd.count == 0);
-            put_child_box(o, 1, nd.box, true);
-            child_code[0] = int32_t(0x80000000u | (uint32_t(std::max<uint32_t>(nd.count, 1) - 1) << 27) | first);
-            child_code[1] = int32_t(0x80000000u);
-            res.sah_cost += nd.box.half_area() / root_area * nd.count;
-        } else {
-            res.sah_cost += nd.box.half_area() / root_area;
-            for (int s = 0; s < 2; ++s) {
-                const TmpNode &c = b.nodes[nd.child[s]];
-                put_child_box(o, s, c.box, false);
-                if (c.child[0] >= 0) {
-                    child_code[s] = dev_of[nd.child[s]];
-                } else {
-                    const uint32_t first = uint32_t(res.tri_order.size());
-                    for (uint32_t i = c.start; i < c.start + c.count; ++i) res.tri_order.push_back(b.prims[i].id);
-                    child_code[s] = int32_t(0x80000000u | ((c.count - 1) << 27) | first);
-                    res.sah_cost += c.box.half_area() / root_area * c.count;
+    const size_t n_inner = inner_base[size_t(parts)];
+    RawArray<int> dev_of;
+    dev_of.allocate(nn);
+    run_parts([&](int p) {
+        int di = int(inner_base[size_t(p)]);
+        for (size_t i = size_t(p) * step; i < std::min(nn, size_t(p + 1) * step); ++i)
+            if (inner(i)) dev_of[i] = di++;
+    });
+    std::vector<float> &out = res.nodes;
+    out.assign(n_inner * 16, 0.f);
+    res.tri_order.resize(tri_base[size_t(parts)]);
+    run_parts([&](int p) {
+        size_t di = inner_base[size_t(p)];
+        uint32_t first = uint32_t(tri_base[size_t(p)]);
+        for (size_t i = size_t(p) * step; i < std::min(nn, size_t(p + 1) * step); ++i) {
+            if (!inner(i)) continue;
+            const TmpNode &nd = b.nodes[i];
+            float *o = &out[di++ * 16];
+            int32_t child_code[2];
+            if (nd.child[0] < 0) {
+                // the whole scene is one leaf: child 0 holds it, child 1 is empty
+                for (uint32_t k = 0; k < nd.count; ++k) res.tri_order[first + k] = b.prims[nd.start + k].id;
+                put_child_box(o, 0, nd.box, nd.count == 0);
+                put_child_box(o, 1, nd.box, true);
+                child_code[0] = int32_t(0x80000000u | (uint32_t(std::max<uint32_t>(nd.count, 1) - 1) << 27) | first);
+                child_code[1] = int32_t(0x80000000u);
+                first += nd.count;
+            } else {
+                for (int s = 0; s < 2; ++s) {
+                    const TmpNode &c = b.nodes[size_t(nd.child[s])];
+                    put_child_box(o, s, c.box, false);
+                    if (c.child[0] >= 0) {
+                        child_code[s] = dev_of[size_t(nd.child[s])];
+                    } else {
+                        for (uint32_t k = 0; k < c.count; ++k) res.tri_order[first + k] = b.prims[c.start + k].id;
+                        child_code[s] = int32_t(0x80000000u | ((c.count - 1) << 27) | first);
+                        first += c.count;
+                    }
                 }
             }
+            memcpy(&o[12], &child_code[0], 4);
+            memcpy(&o[13], &child_code[1], 4);
         }
-        memcpy(&o[12], &child_code[0], 4);
-        memcpy(&o[13], &child_code[1], 4);
+    });
+    // SAH cost of the tree, summed in device order
+    const double root_area = std::max(b.nodes[root].box.half_area(), 1e-30);
+    for (size_t i = 0; i < nn; ++i) {
+        if (!inner(i)) continue;
+        const TmpNode &nd = b.nodes[i];
+        if (nd.child[0] < 0) {
+            res.sah_cost += nd.box.half_area() / root_area * nd.count;
+            continue;
+        }
+        res.sah_cost += nd.box.half_area() / root_area;
+        for (int s = 0; s < 2; ++s) {
+            const TmpNode &c = b.nodes[size_t(nd.child[s])];
+            if (c.child[0] < 0) res.sah_cost += c.box.half_area() / root_area * c.count;
+        }
     }
     return res;
 }
