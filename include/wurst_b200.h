@@ -71,7 +71,11 @@ typedef struct wr_render_desc {
                                 0 = 1000, < 0 = no clamp */
     int fetch_threshold;     /* traversal: a warp hands new rays to its idle lanes when fewer than this
                                 many of its 32 lanes are still traversing; 1..32, 0 = 20 */
-    int reserved[3];
+    int max_iterations;      /* debugging: lowers the wavefront's iteration bound (0 = the bound derived
+                                from the work, (waves + 2) * (num_path_vertices + 2) + 64). A render
+                                that has not drained when its bound is reached stops and returns
+                                WR_ERR_TIMEOUT; the handle stays usable */
+    int reserved[2];
 } wr_render_desc;
 
 typedef struct wr_render_stats {
@@ -213,7 +217,10 @@ int wr_get_render_stats(const wr_scene *scene, wr_render_stats *stats);
  * allocate device memory while running (fixed memory budgets, or no implicit
  * synchronisation from cudaMalloc/cudaFree). Limits: films of at most 65,536
  * pixels (larger: WR_ERR_INVALID_ARGUMENT), a 32,768-path wavefront, plain
- * kernel launches. Every call clears and reuses the same array, so calls that
+ * kernel launches (desc->queue_capacity, use_graph and profile are ignored).
+ * The integrator is resolved as wr_render_device resolves it; the learned
+ * proposal needs buffers of its own, so desc->guiding != 0 returns
+ * WR_ERR_UNSUPPORTED. Every call clears and reuses the same array, so calls that
  * overlap on the GPU race; the first call on a device resolves the array's
  * address and should precede any stream capture. */
 int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc, double *out_rgb_device);

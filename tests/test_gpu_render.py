@@ -207,3 +207,22 @@ def test_profiled_schedules_agree(wr_lib):
         assert abs(p3[key] / sep[key] - 1.0) < 0.01, key
     assert fused["kernel_launches"] == 2 + 4 * (fused["iterations"] - 1) + 2
     assert sep["kernel_launches"] == 3 + 5 * (sep["iterations"] - 1) + 1
+
+
+@pytest.mark.parametrize("mode", ["graph", "launches", "guided"])
+def test_iteration_bound_reports_timeout_and_handle_recovers(wr_lib, mode):
+    """The wavefront's iteration bound (the device-side loop limit of every render) stops a render
+    that has not drained and reports WR_ERR_TIMEOUT; nothing is left in flight, so the next render
+    on the same handle is the right image. The bound is lowered through the debugging field
+    max_iterations to make it trip."""
+    path, _ = golden_scene("zoo")
+    use_graph = mode != "launches"
+    guiding = 1 if mode == "guided" else 0
+    with wr_lib.Scene.from_file(path) as sc:
+        ref = sc.render(spp=32, seed=11, use_graph=use_graph)
+        with pytest.raises(wr_lib.WurstError) as e:
+            sc.render(spp=32, seed=11, use_graph=use_graph, guiding=guiding, max_iterations=3)
+        assert e.value.status == 7          # WR_ERR_TIMEOUT
+        again = sc.render(spp=32, seed=11, use_graph=use_graph)
+        assert sc.stats["iterations"] > 3
+    assert np.allclose(again, ref, rtol=1e-9, atol=1e-12)

@@ -623,6 +623,8 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     const unsigned long long waves = (total + capacity - 1) / capacity;
     r.iter_limit = uint32_t(std::min<unsigned long long>((waves + 2) * (unsigned long long)(max_nverts + 2) + 64,
                                                          0xffffffffull));
+    if (desc.max_iterations < 0) throw Error(WR_ERR_INVALID_ARGUMENT, "max_iterations must be >= 0");
+    if (desc.max_iterations > 0) r.iter_limit = std::min(r.iter_limit, uint32_t(desc.max_iterations));
     r.trace_block = (desc.trace_block == 64 || desc.trace_block == 256) ? desc.trace_block : 128;
     r.grid_trace = desc.grid_trace > 0 ? desc.grid_trace : sms * std::max(1, wrk::occupancy_blocks(0, r.trace_block, s.dev.patches != nullptr, s.dev.wnodes != nullptr));
     r.grid_shade = desc.grid_shade > 0 ? desc.grid_shade : sms * std::max(1, wrk::occupancy_blocks(1));
@@ -1703,6 +1705,18 @@ bool scene_view(wr_scene *s, SceneView *v) {
 }
 
 wrd::DevCamera camera_constants(const wr::Camera &c) { return make_camera(c); }
+
+int resolve_request(const wr::Scene &h, const wr_render_desc &desc, int *spp, int *nverts, int *integrator) {
+    try {
+        const HostJob j = scene_job(h, desc);
+        *spp = j.spp;
+        *nverts = j.nverts;
+        *integrator = j.integrator;
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
 
 void set_last_error(const std::string &m) { g_last_error = m; }
 
