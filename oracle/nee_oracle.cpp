@@ -68,6 +68,11 @@ static inline double Length2(V3 v) { return Dot(v, v); }
 static inline double Length(V3 v) { return std::sqrt(Length2(v)); }
 static inline V3 Normalize(V3 v) { return v / Length(v); }
 static inline bool IsZero(V3 v) { return v.x == 0.0 && v.y == 0.0 && v.z == 0.0; }
+// SpectrumConvertUtil::FromSrgb (src/common/math/spectrum.h:13-17): the sRGB transfer curve
+static inline double FromSrgb(double v) {
+    if (v <= 0.04045) return v * (1.0 / 12.92);
+    return std::pow((v + 0.055) * (1.0 / 1.055), 2.4);
+}
 static inline V3 FlipY(V3 v) { return V3(v.x, -v.y, v.z); }
 static inline double Clamp(double v, double a, double b) { return std::max(std::min(v, b), a); }
 static inline bool IsApprox(double a, double b) {
@@ -905,6 +910,9 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
     if (root.has("meshes")) {
         for (const Json &mj : root.at("meshes").arr) {
             const bool phong_file = mj.getb("phong_tessellation", false);
+            // "mitsuba_srgb" (simple2parser.h:36): Kd and Ks go through FromSrgb, Ke and Ns do not
+            // (assimpio.h:178-181, 317-325)
+            const bool srgb = mj.getb("mitsuba_srgb", false);
             ObjFile of = load_obj(dir + "/" + mj.get("path", std::string("")), phong_file);
             std::map<std::string, double> sigma;
             if (mj.has("oren_nayar_sigma"))
@@ -914,7 +922,10 @@ static Scene *load_scene(const std::string &json_path, int render_index) {
             std::vector<Spectrum> ke(of.materials.size());
             for (size_t i = 0; i < of.materials.size(); ++i) {
                 const ObjMaterial &om = of.materials[i];
-                const V3 kd(om.kd[0], om.kd[1], om.kd[2]), ks(om.ks[0], om.ks[1], om.ks[2]);
+                const V3 kd = srgb ? V3(FromSrgb(om.kd[0]), FromSrgb(om.kd[1]), FromSrgb(om.kd[2]))
+                                   : V3(om.kd[0], om.kd[1], om.kd[2]);
+                const V3 ks = srgb ? V3(FromSrgb(om.ks[0]), FromSrgb(om.ks[1]), FromSrgb(om.ks[2]))
+                                   : V3(om.ks[0], om.ks[1], om.ks[2]);
                 ke[i] = V3(om.ke[0], om.ke[1], om.ke[2]);
                 if (!IsZero(ke[i])) {
                     if (om.ns / 4.0 != 0.0) throw std::runtime_error("emitter with Ns != 0 (SimpleMetal light) is not supported");
@@ -1235,6 +1246,19 @@ void oracle_trace_occluded(void *sp, const float *rays, int n, int *occluded) {
     for (int i = 0; i < n; ++i) {
         const float *r = rays + 8 * size_t(i);
         occluded[i] = s->rc.occluded(r, r + 4, r[3], r[7]) ? 1 : 0;
+    }
+}
+
+// Occlusion bounds per ray (RayCaster::occluded_bracket): lo[i] = blocked beyond doubt,
+// hi[i] = possibly blocked, with tolerance eps (barycentric, and relative on the segment ends).
+void oracle_trace_occluded_bracket(void *sp, const float *rays, int n, double eps, int *lo, int *hi) {
+    auto *s = static_cast<oracle::Scene *>(sp);
+    for (int i = 0; i < n; ++i) {
+        const float *r = rays + 8 * size_t(i);
+        bool l = false, h = false;
+        s->rc.occluded_bracket(r, r + 4, r[3], r[7], eps, &l, &h);
+        lo[i] = l ? 1 : 0;
+        hi[i] = h ? 1 : 0;
     }
 }
 

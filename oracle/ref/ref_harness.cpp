@@ -10,7 +10,9 @@
 // need cmake to build:
 //   * Assimp's OBJ import: meshes come from the oracle's OBJ/MTL reader
 //     (oracle/oracle_scene.h) and are turned into BSDFs and lights with the
-//     mapping of AssimpInOut::LoadFromObj (src/sceneio/meshio/assimpio.h:79-150);
+//     mapping of AssimpInOut::LoadFromObj (src/sceneio/meshio/assimpio.h:79-150),
+//     "mitsuba_srgb" converting Kd and Ks through the reference's own
+//     SpectrumConvertUtil::SpectrumFromSrgb as AimatToTexture does (:287-337);
 //     the "oren_nayar_sigma" mesh key selects OrenNayarBsdf for the diffuse part;
 //   * Embree: see embree_shim.cpp.
 //
@@ -74,6 +76,7 @@ shared_ptr<const Scene> parse_scene(const json &meshesJson, const shared_ptr<Env
     for (const json &mj : meshesJson) {
         const std::string rel = Util::Json::GetValue<std::string>(mj, "path", "");
         const bool doUsePhongTessellation = Util::Json::GetValue<bool>(mj, "phong_tessellation", false);
+        const bool doSrgbConversionTheMitsubaWay = Util::Json::GetValue<bool>(mj, "mitsuba_srgb", false);
         oracle::ObjFile of = oracle::load_obj((dir / rel).string(), doUsePhongTessellation);
         std::map<std::string, double> sigma;
         if (mj.find("oren_nayar_sigma") != mj.end())
@@ -82,8 +85,14 @@ shared_ptr<const Scene> parse_scene(const json &meshesJson, const shared_ptr<Env
         std::vector<shared_ptr<const Bsdf>> bsdfs;
         std::vector<shared_ptr<Light>> areaLights;
         for (const oracle::ObjMaterial &om : of.materials) {
-            auto kdT = make_shared<ConstantTexture<Spectrum>>(SpectrumConvertUtil::SpectrumFromRgb(om.kd[0], om.kd[1], om.kd[2]));
-            auto ksT = make_shared<ConstantTexture<Spectrum>>(SpectrumConvertUtil::SpectrumFromRgb(om.ks[0], om.ks[1], om.ks[2]));
+            // AimatToTexture (assimpio.h:287-337): Kd and Ks through the reference's own
+            // SpectrumFromSrgb when the entry asks for it, Ke never
+            auto color = [&](const double *c) {
+                return doSrgbConversionTheMitsubaWay ? SpectrumConvertUtil::SpectrumFromSrgb(c[0], c[1], c[2])
+                                                     : SpectrumConvertUtil::SpectrumFromRgb(c[0], c[1], c[2]);
+            };
+            auto kdT = make_shared<ConstantTexture<Spectrum>>(color(om.kd));
+            auto ksT = make_shared<ConstantTexture<Spectrum>>(color(om.ks));
             auto keT = make_shared<ConstantTexture<Spectrum>>(SpectrumConvertUtil::SpectrumFromRgb(om.ke[0], om.ke[1], om.ke[2]));
             auto nT = make_shared<ConstantTexture<double>>(om.ns / 4.0);
             if (!Math::IsZero(keT->average())) {

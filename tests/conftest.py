@@ -9,7 +9,7 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt", "cornell_ls", "hf_ls", "phong", "phong_pt",
-            "phong_ls"]
+            "phong_ls", "srgb", "lens", "lens_ls"]
 
 
 def pytest_configure(config):

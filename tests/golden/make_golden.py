@@ -33,7 +33,7 @@ import oracle  # noqa: E402
 from wurstrenderer_b200 import scenes  # noqa: E402
 
 FIXTURES = ["cornell", "zoo", "env", "hf", "cornell_pt", "env_pt", "cornell_ls", "hf_ls", "phong", "phong_pt",
-            "phong_ls"]
+            "phong_ls", "srgb", "lens", "lens_ls"]
 
 
 def with_integrator(path, integrator):
@@ -63,6 +63,11 @@ def write_fixture_scene(name, out_dir):
                                                n_lights=4, light_ke=(30.0, 28.0, 25.0))
         cam = dict(scenes.HEIGHTFIELD_CAMERA, pos=[0.0, 2.2, 5.5])
         return scenes.write_spec(out_dir, "hf", spec, cam, (48, 24), 4, 12)
+    if name == "srgb":    # sRGB-encoded reflectances (a "mitsuba_srgb": true mesh entry)
+        return scenes.write_srgb_zoo(out_dir, name="srgb", resolution=(48, 40), spp=4, num_path_vertices=10)
+    if name == "lens":    # thin-lens camera: aperture radius and focal distance 0.1 ("radius")
+        return scenes.write_cornell_lens(out_dir, name="lens", resolution=(48, 48), spp=4, num_path_vertices=10,
+                                         radius=0.1)
     if name == "phong":   # Phong tessellation surfaces (a "phong_tessellation": true mesh entry)
         return scenes.write_phong_cornell(out_dir, name="phong", resolution=(48, 48), spp=4, num_path_vertices=8)
     raise KeyError(name)

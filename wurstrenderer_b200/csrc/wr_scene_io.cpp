@@ -309,7 +309,16 @@ struct ObjMeshRaw {
 // tessellation patches (Simple2Parser::ParseScene, src/sceneio/simple2parser.h:37-55) with one
 // vertex per distinct (position, normal) pair, as Assimp's JoinIdenticalVertices leaves them;
 // its emitters stay triangle meshes (simple2parser.h:58).
-void load_obj(const std::string &path, const std::map<std::string, double> &sigma, bool phong, Scene &scene) {
+// sRGB-encoded reflectance to linear (IEC 61966-2-1 transfer curve), in FP64 as the reference
+// converts it (SpectrumConvertUtil::FromSrgb, src/common/math/spectrum.h:13-17)
+double srgb_to_linear(double v) {
+    if (v <= 0.04045) return v * (1.0 / 12.92);
+    return std::pow((v + 0.055) * (1.0 / 1.055), 2.4);
+}
+
+// srgb: the mesh entry's "mitsuba_srgb" -- Kd and Ks are sRGB-encoded (assimpio.h:178-181, 317-325)
+void load_obj(const std::string &path, const std::map<std::string, double> &sigma, bool phong, bool srgb,
+              Scene &scene) {
     const std::string data = slurp(path);
     std::vector<MtlEntry> mats(1);
     mats[0].name = "DefaultMaterial";
@@ -415,10 +424,17 @@ void load_obj(const std::string &path, const std::map<std::string, double> &sigm
             emitter[i] = true;
         }
         Material mat;
-        for (int k = 0; k < 3; ++k) { mat.kd[k] = m.kd[k]; mat.ks[k] = m.ks[k]; }
+        double kd[3], ks[3];
+        for (int k = 0; k < 3; ++k) {
+            kd[k] = srgb ? srgb_to_linear(double(m.kd[k])) : double(m.kd[k]);
+            ks[k] = srgb ? srgb_to_linear(double(m.ks[k])) : double(m.ks[k]);
+            mat.kd[k] = float(kd[k]);
+            mat.ks[k] = float(ks[k]);
+        }
         mat.exponent = float(double(m.ns) / 4.0);
-        const bool kd_zero = m.kd[0] == 0.f && m.kd[1] == 0.f && m.kd[2] == 0.f;
-        const bool ks_zero = m.ks[0] == 0.f && m.ks[1] == 0.f && m.ks[2] == 0.f;
+        // the component choice sees the FP64 reflectances, as the reference's does
+        const bool kd_zero = kd[0] == 0.0 && kd[1] == 0.0 && kd[2] == 0.0;
+        const bool ks_zero = ks[0] == 0.0 && ks[1] == 0.0 && ks[2] == 0.0;
         if (kd_zero) { mat.has_glossy = true; }
         else if (ks_zero) { mat.has_diffuse = true; }
         else { mat.has_diffuse = true; mat.has_glossy = true; }
@@ -514,9 +530,8 @@ Scene load_from_node(const JNode &root, const std::string &base_dir) {
             if (const JNode *sj = mj.find("oren_nayar_sigma")) {
                 for (size_t i = 0; i < sj->keys.size(); ++i) sigma[sj->keys[i]] = sj->items[i].n;
             }
-            if (mj.num("mitsuba_srgb", 0.0) != 0.0)
-                throw Error(WR_ERR_UNSUPPORTED, "mitsuba_srgb colour conversion is not supported");
-            load_obj(join_path(base_dir, mj.str("path", "")), sigma, phong, s);
+            const bool srgb = mj.num("mitsuba_srgb", 0.0) != 0.0;
+            load_obj(join_path(base_dir, mj.str("path", "")), sigma, phong, srgb, s);
         }
     }
     if (const JNode *cj = root.find("camera")) {

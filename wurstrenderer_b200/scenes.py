@@ -326,6 +326,21 @@ def write_cornell(out_dir, name="cornell", resolution=(256, 256), spp=16,
                        [nee_render(output or name + ".pfm", spp, num_path_vertices)])
 
 
+def write_cornell_lens(out_dir, name="lens", resolution=(48, 48), spp=4, num_path_vertices=10, radius=0.1):
+    """The Cornell box seen through a thin lens: the simple2 camera's "radius" key is both the
+    aperture radius and the focal distance (src/camera/thinlens.h:22-23)."""
+    cam = dict(CORNELL_CAMERA, resolution=list(resolution), radius=float(radius))
+    return write_scene(out_dir, name, cornell_spec(), cam, [nee_render(name + ".pfm", spp, num_path_vertices)])
+
+
+def write_srgb_zoo(out_dir, name="srgb", resolution=(48, 40), spp=4, num_path_vertices=10):
+    """The material zoo in one mesh entry with "mitsuba_srgb": true: its Kd and Ks are read as
+    sRGB-encoded and linearised, its Ke and Ns are not (src/sceneio/meshio/assimpio.h:178-181)."""
+    cam = dict(CORNELL_CAMERA, resolution=list(resolution))
+    return write_scene_entries(out_dir, name, [("zoo", material_zoo_spec(), {"mitsuba_srgb": True})], cam,
+                               [nee_render(name + ".pfm", spp, num_path_vertices)])
+
+
 def phong_objects_spec(seed=1007, n_objects=5):
     """Smooth low-poly objects for Phong tessellation: icospheres (1-2 subdivisions) and
     radially perturbed blobs, each with area-weighted vertex normals; diffuse, glossy
@@ -659,6 +674,26 @@ def write_full_combination(out_dir, name="full_combination", resolution=(3840, 2
     cam = dict(FULL_COMBINATION_CAMERA, resolution=list(resolution))
     return write_scene(out_dir, name, full_combination_spec(seed, **kw), cam,
                        [nee_render(name + ".pfm", spp, num_path_vertices)], envmap=env_name)
+
+
+# the full-size plain NEE+MIS workloads whose FP64 reference crops live in tests/golden:
+# c1, the whole 256^2 frame of the procedural Cornell box (36 triangles, 10 vertices); c2 and c2h,
+# two crops (spheres in the middle distance, the horizon) of the 1024x512 frame of the
+# 1,162,250-triangle heightfield-and-spheres scene (18 vertices)
+PLAIN_WORKLOADS = {
+    "c1": {"resolution": (256, 256), "num_path_vertices": 10, "crop": (0, 0, 256, 256)},
+    "c2": {"resolution": (1024, 512), "num_path_vertices": 18, "crop": (448, 288, 576, 352)},
+    "c2h": {"resolution": (1024, 512), "num_path_vertices": 18, "crop": (768, 160, 896, 224)},
+}
+
+
+def write_plain_workload(name, out_dir, spp=64):
+    """Writes the Cornell box (c1) or the heightfield-and-spheres scene (c2, c2h) at full size."""
+    w = PLAIN_WORKLOADS[name]
+    if name == "c1":
+        return write_cornell(out_dir, resolution=w["resolution"], spp=spp, num_path_vertices=w["num_path_vertices"])
+    return write_heightfield_spheres(out_dir, resolution=w["resolution"], spp=spp,
+                                     num_path_vertices=w["num_path_vertices"])
 
 
 # the full-size guided-vs-plain workloads whose FP64 reference crops live in tests/golden
