@@ -19,7 +19,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_nee.so")
 REF_BIN = os.path.join(HERE, "_ref", "wurst_ref")
-REFERENCE_ROOT = "/root/reference"
+# where the reference's sources lie (read-only); only the build recipe reads them there
+REFERENCE_ROOT = os.environ.get("WURST_REFERENCE_ROOT", "/root/reference")
 
 _lib = None
 
