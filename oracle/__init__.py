@@ -52,6 +52,8 @@ def lib():
         L.oracle_trace_closest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_trace_occluded.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.oracle_trace_occluded_bracket.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                                    ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_trace_hits.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
@@ -131,6 +133,17 @@ class OracleScene:
         occ = np.zeros(rays.shape[0], np.int32)
         lib().oracle_trace_occluded(self._h, _ptr(rays), rays.shape[0], _ptr(occ))
         return occ
+
+    def trace_occluded_bracket(self, rays: np.ndarray, eps: float = 1e-5):
+        """Bounds on a correct any-hit answer per ray: (blocked beyond doubt, possibly blocked),
+        each (n,) bool. Triangles are tested in FP64 grown / shrunk by eps in barycentric
+        coordinates, segment ends moved by eps * max(|t|, 1), grazing rays (|cos| < 1e-4) never
+        count as blocked beyond doubt."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        lo = np.zeros(rays.shape[0], np.int32)
+        hi = np.zeros(rays.shape[0], np.int32)
+        lib().oracle_trace_occluded_bracket(self._h, _ptr(rays), rays.shape[0], float(eps), _ptr(lo), _ptr(hi))
+        return lo.astype(bool), hi.astype(bool)
 
 
 def reference_available() -> bool:

@@ -366,6 +366,99 @@ struct RayCaster {
         return false;
     }
 
+    // Occlusion bounds for checking another ray caster's any-hit answers. Each triangle is tested
+    // in FP64 from its float vertices: *hi = the segment may be blocked (a triangle grown by eps in
+    // barycentric coordinates, or a hit within eps * max(|t|, 1) outside either end of the segment),
+    // *lo = it is blocked beyond doubt (a triangle shrunk by eps, the segment shortened by the same
+    // tolerance, and a ray not grazing the plane: |cos| >= 1e-4). Two correct FP32 tests of the same
+    // ray -- Embree's and a watertight one -- answer between *lo and *hi. User primitives count for
+    // both bounds through user_any on the shortened / lengthened segment.
+    void occluded_bracket(const float o[3], const float d[3], float tnear, float tfar, double eps,
+                          bool *lo, bool *hi) const {
+        *lo = false;
+        *hi = false;
+        const double tol_n = eps * std::max(std::fabs(double(tnear)), 1.0);
+        const bool far_inf = std::isinf(tfar);
+        const double tol_f = far_inf ? 0.0 : eps * std::max(std::fabs(double(tfar)), 1.0);
+        const double n_hi = double(tnear) - tol_n, f_hi = double(tfar) + tol_f;   // lengthened
+        const double n_lo = double(tnear) + tol_n, f_lo = double(tfar) - tol_f;   // shortened
+        double diag = 0.0;
+        for (int k = 0; k < 3; ++k) diag = std::max(diag, double(scene_hi[k]) - double(scene_lo[k]));
+        const float margin = float(4.0 * eps * diag) + 1e-6f;
+        const double dd[3] = {d[0], d[1], d[2]};
+        const double dlen = std::sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+        float inv[3];
+        for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];
+        if (!nodes.empty()) {
+            int stack[128]; int sp = 0;
+            stack[sp++] = 0;
+            while (sp && !*lo) {
+                RcNode nd = nodes[stack[--sp]];
+                for (int k = 0; k < 3; ++k) { nd.lo[k] -= margin; nd.hi[k] += margin; }
+                float te;
+                if (!box_hit(nd, o, inv, float(n_hi), float(f_hi) * 1.0001f, &te)) continue;
+                if (nd.left >= 0) {
+                    stack[sp++] = nd.right;
+                    stack[sp++] = nd.left;
+                    continue;
+                }
+                for (int i = nd.first; i < nd.first + nd.count; ++i) {
+                    const RcTri &tr = tris[i];
+                    double e1[3], e2[3], C[3];
+                    for (int k = 0; k < 3; ++k) {
+                        e1[k] = double(tr.e1[k]);
+                        e2[k] = double(tr.e2[k]);
+                        C[k] = double(tr.v0[k]) - double(o[k]);
+                    }
+                    const double ng[3] = {e2[1] * e1[2] - e2[2] * e1[1], e2[2] * e1[0] - e2[0] * e1[2],
+                                          e2[0] * e1[1] - e2[1] * e1[0]};
+                    const double R[3] = {C[1] * dd[2] - C[2] * dd[1], C[2] * dd[0] - C[0] * dd[2],
+                                         C[0] * dd[1] - C[1] * dd[0]};
+                    const double den = ng[0] * dd[0] + ng[1] * dd[1] + ng[2] * dd[2];
+                    const double absden = std::fabs(den);
+                    if (!(absden > 0.0)) continue;
+                    const double sgn = den < 0.0 ? -1.0 : 1.0;
+                    const double u = (R[0] * e2[0] + R[1] * e2[1] + R[2] * e2[2]) * sgn / absden;
+                    const double v = (R[0] * e1[0] + R[1] * e1[1] + R[2] * e1[2]) * sgn / absden;
+                    const double t = (ng[0] * C[0] + ng[1] * C[1] + ng[2] * C[2]) * sgn / absden;
+                    const double nlen = std::sqrt(ng[0] * ng[0] + ng[1] * ng[1] + ng[2] * ng[2]);
+                    const double cosv = absden / (nlen * dlen);
+                    if (u >= -eps && v >= -eps && u + v <= 1.0 + eps && t > n_hi && (far_inf || t <= f_hi))
+                        *hi = true;
+                    if (cosv >= 1e-4 && u >= eps && v >= eps && u + v <= 1.0 - eps && t > n_lo && (far_inf || t <= f_lo)) {
+                        *lo = true;
+                        break;
+                    }
+                }
+            }
+        }
+        if (!*lo && !unodes.empty() && user_any) {
+            if (occluded_users(o, d, float(n_lo), far_inf ? tfar : float(f_lo))) *lo = true;
+            if (occluded_users(o, d, float(n_hi), far_inf ? tfar : float(f_hi))) *hi = true;
+        }
+        if (*lo) *hi = true;
+    }
+
+    bool occluded_users(const float o[3], const float d[3], float tnear, float tfar) const {
+        float inv[3];
+        for (int k = 0; k < 3; ++k) inv[k] = 1.0f / d[k];
+        int stack[128]; int sp = 0;
+        stack[sp++] = 0;
+        while (sp) {
+            const RcNode &nd = unodes[stack[--sp]];
+            float te;
+            if (!box_hit(nd, o, inv, tnear, tfar, &te)) continue;
+            if (nd.left < 0) {
+                for (int i = nd.first; i < nd.first + nd.count; ++i)
+                    if (user_box_hit(users[i], o, inv, tnear, tfar) && user_any(users[i], o, d, tnear, tfar)) return true;
+            } else {
+                stack[sp++] = nd.right;
+                stack[sp++] = nd.left;
+            }
+        }
+        return false;
+    }
+
     bool occluded_tris(const float o[3], const float d[3], float tnear, float tfar) const {
         if (nodes.empty()) return false;
         float inv[3];

@@ -6,6 +6,12 @@ triangle test). The B200 kernel uses a watertight test, so ids must agree
 exactly except on rays whose two candidate hits tie in distance within
 1e-5 relative, or that graze a triangle edge (barycentric within 1e-5 of an
 edge), where the two tests may legitimately pick different triangles.
+
+Any-hit answers are held to the same rule: every GPU answer must lie between the
+oracle's FP64 bounds for the ray (occluded_bracket: triangles shrunk / grown by 1e-5
+in barycentric coordinates, segment ends moved by 1e-5 relative, grazing rays
+excused), so an answer may differ from the reference's only on an edge graze or an
+end-point tie, and nowhere else.
 """
 import numpy as np
 import pytest
@@ -65,23 +71,52 @@ def test_wide_bvh_hits_match_reference(wr_lib, oracle_lib, name):
     assert np.array_equal(t[both], t2[both])
     # the two trees test tied candidates (a ray through a shared edge) in different orders
     assert (~both & ~_tie_or_edge(t2, t, uv_ref)).sum() == 0
-    assert (occ != occ2).sum() <= max(1, int(0.002 * len(rays)))
+    lo, hi = oracle_lib.OracleScene(path).trace_occluded_bracket(rays)
+    assert_within_bracket(occ, lo, hi)
+    assert_within_bracket(occ2, lo, hi)
+
+
+def assert_within_bracket(occ, lo, hi, max_ambiguous=0.005):
+    """Any-hit answers against the oracle's bounds: blocked where it is blocked beyond doubt,
+    free where nothing can block it."""
+    occ = np.asarray(occ).astype(bool)
+    bad = (occ & ~hi) | (~occ & lo)
+    assert bad.sum() == 0, "any-hit answers outside the oracle's bounds: rays %s" % np.nonzero(bad)[0][:10]
+    assert (hi & ~lo).mean() <= max_ambiguous, "too many ambiguous rays: %d" % (hi & ~lo).sum()
+
+
+def shadow_segments(rays, hits, lo, hi, seed=5):
+    """Three kinds of finite segments over a ray batch: ending halfway to the reference's closest
+    hit, ending beyond it, and from the ray's origin to a random point of the scene box (the shape
+    of a shadow ray toward a light sample, tmax = length - 1e-4)."""
+    rng = np.random.default_rng(seed)
+    t_ref = hits[:, 2].view(np.float32)
+    n = len(rays)
+    out = np.repeat(rays[None], 3, axis=0).reshape(3 * n, 8).copy()
+    out[:n, 7] = np.where(hits[:, 0] >= 0, 0.5 * t_ref, 10.0)
+    out[n:2 * n, 7] = np.where(hits[:, 0] >= 0, 1.5 * t_ref, 10.0)
+    tgt = lo + rng.uniform(size=(n, 3)) * (hi - lo)
+    d = tgt - rays[:, 0:3]
+    ln = np.linalg.norm(d, axis=1)
+    out[2 * n:, 4:7] = d / ln[:, None]
+    out[2 * n:, 3] = 1e-4
+    out[2 * n:, 7] = ln - 1e-4
+    return out
 
 
 @pytest.mark.parametrize("name", FIXTURES)
 def test_occlusion_matches_oracle(wr_lib, oracle_lib, name):
     path, _ = golden_scene(name)
-    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name)).copy()
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name))
     hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
-    t_ref = hits[:, 2].view(np.float32)
-    # finite segments: half of them end before the closest hit, half after it
-    rng = np.random.default_rng(5)
-    tmax = np.where(hits[:, 0] >= 0, t_ref * np.where(rng.uniform(size=len(rays)) < 0.5, 0.5, 1.5), 10.0)
-    rays[:, 7] = tmax.astype(np.float32)
+    osc = oracle_lib.OracleScene(path)
+    segs = shadow_segments(rays, hits, osc.bbox_lo, osc.bbox_hi)
     with wr_lib.Scene.from_file(path) as sc:
-        occ = sc.trace_occluded(rays)
-    occ_ref = oracle_lib.OracleScene(path).trace_occluded(rays)
-    assert (occ != occ_ref).mean() < 2e-3
+        occ = sc.trace_occluded(segs)
+    lo, hi = osc.trace_occluded_bracket(segs)
+    assert_within_bracket(occ, lo, hi)
+    # the reference's own answers lie inside the same bounds
+    assert_within_bracket(osc.trace_occluded(segs), lo, hi)
 
 
 def test_empty_and_tiny_batches(wr_lib, oracle_lib):
@@ -137,7 +172,9 @@ def test_patch_hits_and_normals_match_reference(wr_lib, oracle_lib, name):
     assert np.abs(nrm[m] - ng_ref[m]).max() < 1e-5
     assert np.abs(np.linalg.norm(nrm[m], axis=1) - 1.0).max() < 1e-5
     occ_ref = hng[:, 4] > 0.5
-    assert (occ.astype(bool) != occ_ref).sum() <= max(1, int(0.001 * len(rays)))
+    lo, hi = oracle_lib.OracleScene(path).trace_occluded_bracket(rays)
+    assert_within_bracket(occ_ref, lo, hi)
+    assert_within_bracket(occ, lo, hi)
 
 
 @pytest.mark.parametrize("name", ["hf", "phong"])
@@ -164,7 +201,9 @@ def test_tree_shape_options_keep_the_hits(wr_lib, oracle_lib, name, opts):
     both = (g == g2) & (p == p2)
     assert np.array_equal(t[both], t2[both])
     assert (~both & ~_tie_or_edge(t2, t, uv_ref)).sum() == 0
-    assert (occ != occ2).sum() <= max(1, int(0.002 * len(rays)))
+    lo, hi = oracle_lib.OracleScene(path).trace_occluded_bracket(rays)
+    assert_within_bracket(occ, lo, hi)
+    assert_within_bracket(occ2, lo, hi)
 
 
 def test_tree_shape_option_errors(wr_lib):

@@ -1,0 +1,134 @@
+"""Parity of the benchmarked workloads at their full sizes, against the reference.
+
+  c1:  the procedural Cornell box (36 triangles) at 256 x 256, 10 vertices: the whole frame;
+  c2:  the 1,162,250-triangle heightfield-and-spheres scene at 1024 x 512, 18 vertices -- the
+       workload bench.py measures -- through two 128 x 64 crops (c2: spheres in the middle
+       distance, c2h: the horizon, distant small spheres).
+
+Reference images: the reference's own PathNeeRenderer code renders each crop twice
+(tests/golden/make_crop_golden.py, salts 11 / 22). The GPU renders the full frame as K
+independent seeds and must land within 2 x the crop's own noise floor (relMSE against the
+mean of the two halves <= 2 x relMSE between the halves), with every 8 x 8 block |z| < 4
+(z with both estimators' variances) and the crop mean within 1 %.
+
+Ray batches (c1: 16,384 rays, c2: 65,536 rays; half through the scene box, half camera
+rays): the reference's closest hits and occlusion answers. Ids must be equal except on
+distance ties and edge grazes; t within 2e-5 relative; any-hit answers within the oracle's
+FP64 bounds, for infinite rays and three kinds of finite segments.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from test_gpu_render import block_z, relmse
+from test_gpu_trace import _tie_or_edge, assert_within_bracket, shadow_segments
+
+pytestmark = pytest.mark.gpu
+
+# workload -> (GPU seeds, spp per seed)
+RENDER = {"c1": (4, 1024), "c2": (4, 2048)}
+
+
+@pytest.fixture(scope="module")
+def workload_scene(tmp_path_factory):
+    from wurstrenderer_b200 import scenes
+    paths = {}
+
+    def get(name):
+        base = "c2" if name == "c2h" else name
+        if base not in paths:
+            paths[base] = scenes.write_plain_workload(base, str(tmp_path_factory.mktemp(base)))
+        return paths[base]
+    return get
+
+
+@pytest.fixture(scope="module")
+def frames(wr_lib, workload_scene):
+    """Full-frame GPU renders per workload, K seeds each, kept for every crop of the frame."""
+    cache = {}
+
+    def get(name):
+        base = "c2" if name == "c2h" else name
+        if base not in cache:
+            k, spp = RENDER[base]
+            with wr_lib.Scene.from_file(workload_scene(base)) as sc:
+                cache[base] = np.stack([sc.render(spp=spp, seed=4000 + i) for i in range(k)])
+        return cache[base]
+    return get
+
+
+def _crop_reference(name):
+    meta_p = os.path.join(GOLDEN, "%s_crop_meta.json" % name)
+    meta = json.load(open(meta_p))
+    a = np.load(os.path.join(GOLDEN, "%s_crop_ref_a.npy" % name)).astype(np.float64)
+    b = np.load(os.path.join(GOLDEN, "%s_crop_ref_b.npy" % name)).astype(np.float64)
+    return meta, a, b
+
+
+@pytest.mark.parametrize("name", ["c1", "c2", "c2h"])
+def test_workload_crop_matches_reference(wr_lib, frames, name):
+    from wurstrenderer_b200 import scenes
+    meta, ref_a, ref_b = _crop_reference(name)
+    w = scenes.PLAIN_WORKLOADS[name]
+    assert tuple(meta["crop"]) == tuple(w["crop"]) and meta["num_path_vertices"] == w["num_path_vertices"]
+    x0, y0, x1, y1 = meta["crop"]
+    runs = frames(name)[:, y0:y1, x0:x1]
+    assert np.isfinite(runs).all()
+    ref = 0.5 * (ref_a + ref_b)
+    img = runs.mean(axis=0)
+    floor = relmse(ref_a, ref_b)
+    err = relmse(img, ref)
+    print("%s: relMSE %.3g, reference noise floor %.3g" % (name, err, floor))
+    assert err <= 2.0 * floor, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
+    z = block_z(runs, ref, ref_pair=(ref_a, ref_b))
+    assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
+    assert abs(img.mean() / ref.mean() - 1.0) < 0.01
+
+
+def test_heightfield_workload_size(wr_lib, workload_scene):
+    with wr_lib.Scene.from_file(workload_scene("c2")) as sc:
+        inf = sc.info
+    assert (inf["width"], inf["height"], inf["num_path_vertices"]) == (1024, 512, 18)
+    assert inf["num_triangles"] == 1162250 and inf["num_lights"] == 4
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_workload_closest_hits_match_reference(wr_lib, oracle_lib, workload_scene, name):
+    path = workload_scene(name)
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name))
+    hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
+    with wr_lib.Scene.from_file(path) as sc:
+        g, p, t, uv = sc.trace_closest(rays)
+    osc = oracle_lib.OracleScene(path)
+    go, po, to, uv_ref = osc.trace_closest(rays)
+    # the oracle's answers are the reference's, bit for bit
+    assert np.array_equal(go, hits[:, 0]) and np.array_equal(po, hits[:, 1])
+    t_ref = hits[:, 2].view(np.float32)
+    same = (g == hits[:, 0]) & (p == hits[:, 1])
+    bad = ~same & ~_tie_or_edge(t_ref, t, uv_ref)
+    assert bad.sum() == 0, "mismatching rays: %s" % np.nonzero(bad)[0][:10]
+    assert same.mean() > 0.995
+    hit = same & (g >= 0)
+    assert hit.sum() > 0.3 * len(rays)
+    assert np.allclose(t[hit], t_ref[hit], rtol=2e-5, atol=1e-6)
+    assert np.allclose(uv[hit], uv_ref[hit], atol=2e-4)
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_workload_occlusion_matches_reference(wr_lib, oracle_lib, workload_scene, name):
+    path = workload_scene(name)
+    rays = np.load("%s/%s_rays.npy" % (GOLDEN, name))
+    hits = np.load("%s/%s_hits.npy" % (GOLDEN, name))
+    osc = oracle_lib.OracleScene(path)
+    segs = shadow_segments(rays, hits, osc.bbox_lo, osc.bbox_hi)
+    with wr_lib.Scene.from_file(path) as sc:
+        occ_inf = sc.trace_occluded(rays)
+        occ_seg = sc.trace_occluded(segs)
+    lo, hi = osc.trace_occluded_bracket(rays)
+    assert_within_bracket(hits[:, 3], lo, hi)       # the reference's own answers (tfar = inf)
+    assert_within_bracket(occ_inf, lo, hi)
+    lo, hi = osc.trace_occluded_bracket(segs)
+    assert_within_bracket(occ_seg, lo, hi)
