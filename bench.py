@@ -13,9 +13,16 @@ Under torchrun every rank renders the whole image with its own random streams
 with one NCCL reduce per step. Rank 0 prints one JSON line.
 
 `value` is device time (CUDA events on the renderer's stream, summed over the K
-steps, max over ranks); `e2e` is the same metric through the public C ABI call
-with host output (wr_render: film copied device->host into pinned host memory inside the timed
-region).
+steps, max over ranks; at N > 1 each step also includes the FP64 film reduce,
+timed by CUDA events on the stream it is issued on); `e2e` is the same metric
+through the public C ABI call with host output (wr_render: film copied
+device->host into pinned host memory inside the timed region; at N > 1 render,
+reduce and read-back of the reduced film).
+
+The default run also carries the guided-vs-plain equal-time studies of the two
+guided workloads against their FP64 reference crops: the door-gap room (config 4,
+`equal_time_relmse`) and the 10M-triangle full combination (config 5, `c5`, with
+its plain Mpaths/s).
 The CPU baseline runs the oracle (the reference's own renderer code compiled
 here, or its FP64 restatement) on the box's host cores on a bounded sample of
 the same workload (full frame at reduced spp; per-path work is unchanged).
@@ -193,6 +200,15 @@ def traffic_per_ray():
     return {}
 
 
+def l1_profile():
+    """L1/TEX figures of the traversal kernel from the committed single-launch ncu capture."""
+    p = os.path.join(ROOT, "profiles", "k_trace_pair_l1.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
 def cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -352,9 +368,12 @@ def guided_vs_plain(wr, name="door", plain_spp=256, seeds=2):
             steps, records = st["guide_steps"], st["guide_records"]
     pe, ge = float(np.mean(plain_err)), float(np.mean(g_err))
     pm, gm = float(np.mean(plain_ms)), float(np.mean(g_ms))
-    out.update({"plain": {"spp": plain_spp, "relmse": pe, "ms": pm, "runs": seeds},
+    npix = img.shape[0] * img.shape[1]
+    out.update({"plain": {"spp": plain_spp, "relmse": pe, "ms": pm, "runs": seeds,
+                          "mpaths_s": npix * plain_spp / (pm * 1e3)},
                 "guided": {"spp": g_spp, "relmse": ge, "ms": gm, "train_ms": float(np.mean(g_train)),
-                           "adam_steps": steps, "records": records, "runs": seeds},
+                           "adam_steps": steps, "records": records, "runs": seeds,
+                           "mpaths_s": npix * g_spp / (gm * 1e3)},
                 "relmse_ratio_equal_time": (ge * gm) / (pe * pm),
                 # the same with the 1e-3 epsilon of the reference's error image (util/errorimage.h:18)
                 "relmse_eps1e-3": {"plain": float(np.mean(plain_err3)), "guided": float(np.mean(g_err3)),
@@ -377,7 +396,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="use the default wavefront settings")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8],
                     help="2: binary BVH, 8: compressed 8-wide BVH, 0: the library default")
-    ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time study")
+    ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time studies")
+    ap.add_argument("--no-c5", action="store_true", help="skip the config-5 (10M triangles) study of the default run")
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven launches instead of one graph per render (profiling runs: ncu does not "
                          "profile kernels inside conditional graph nodes)")
@@ -423,9 +443,25 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
     tune = {}
     tune_ms = None
-    if not args.no_autotune and args.workload != "jobs128":
-        # (the autotuner probes renders of the scene's own camera, which do not represent a batch)
-        tune, tune_ms = scene.autotune(probe_spp=16)
+    tune_probe = None
+    batch_jobs = None
+    if args.workload == "jobs128":
+        from wurstrenderer_b200 import scenes
+        batch_jobs = scenes.batch_jobs(seed=1003, n_jobs=128, num_path_vertices=14)
+        paths_batch = sum(j["camera"]["resolution"][0] * j["camera"]["resolution"][1] * j["num_spp"]
+                          for j in batch_jobs)
+    if not args.no_autotune:
+        if batch_jobs is None:
+            tune, tune_ms = scene.autotune(probe_spp=16)
+            tune_probe = "the scene's camera at 16 spp"
+        else:
+            # the batch itself is the probe: every 4th job (a quarter of the cameras and resolutions)
+            # at a quarter of its spp, about 1/16 of the batch's paths
+            probe = [dict(j, num_spp=max(1, j["num_spp"] // 4), seed=77 + k) for k, j in enumerate(batch_jobs[::4])]
+            tune, tune_ms = scene.autotune_batch(probe)
+            tune_probe = "wr_autotune_batch over every 4th job of the batch at 1/4 of its spp (%d jobs, %d paths)" % (
+                len(probe), sum(j["camera"]["resolution"][0] * j["camera"]["resolution"][1] * j["num_spp"]
+                                for j in probe))
         tune = {k: v for k, v in tune.items() if k != "use_graph"}
     if args.queue_capacity:
         tune["queue_capacity"] = args.queue_capacity
@@ -434,14 +470,9 @@ def main():
                  trace_block=tune.get("trace_block"), fetch_threshold=tune.get("fetch_threshold"),
                  use_graph=not args.no_graph)
 
-    batch_jobs = None
-    if args.workload == "jobs128":
-        from wurstrenderer_b200 import scenes
-        batch_jobs = scenes.batch_jobs(seed=1003, n_jobs=128, num_path_vertices=14)
-        paths_batch = sum(j["camera"]["resolution"][0] * j["camera"]["resolution"][1] * j["num_spp"]
-                          for j in batch_jobs)
-
     from wurstrenderer_b200.distributed import combine_films, max_over_ranks, rank_seed
+
+    red0, red1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def step(seed):
         seed = rank_seed(seed, rank)
@@ -453,7 +484,15 @@ def main():
         scene.render_device(film.data_ptr(), spp=spp, seed=seed, queue_capacity=qc,
                             guiding=1 if args.workload == "door" else 0, **knobs)
         st = scene.stats
-        combine_films(film, world, dist)
+        if world > 1:
+            # the one exchange of the step: the FP64 film reduce (NCCL), timed with CUDA events on the
+            # stream it is issued on, after the render (which has synchronised its own stream)
+            red0.record()
+            combine_films(film, world, dist)
+            red1.record()
+            red1.synchronize()
+            st["reduce_ms"] = red0.elapsed_time(red1)
+            st["render_ms"] += st["reduce_ms"]
         return st
 
     for i in range(args.warmup):
@@ -464,13 +503,14 @@ def main():
 
     clocks = ClockSampler(local_rank, torch.cuda.current_device())
     clocks.start()
-    dev_ms, launches, iters = 0.0, 0, 0
+    dev_ms, reduce_ms, launches, iters = 0.0, 0.0, 0, 0
     wall0 = time.perf_counter()
     for i in range(args.steps):
         flush.fill_(float(i))               # evict L2 between timed steps (outside the per-step device timing)
         torch.cuda.synchronize()
         st = step(7919 * (rank + 1) + i)
         dev_ms += st["render_ms"]
+        reduce_ms += st.get("reduce_ms", 0.0)
         launches += st["kernel_launches"]
         iters += st["iterations"]
     torch.cuda.synchronize()
@@ -504,13 +544,20 @@ def main():
         return
 
     # end to end through the public C ABI with host output (device->host copy of the film inside)
-    host = torch.empty((H, W, 3), dtype=torch.float64, pin_memory=True).numpy()   # pinned host film
+    host_t = torch.empty((H, W, 3), dtype=torch.float64, pin_memory=True)   # pinned host film
+    host = host_t.numpy()
     e2e_ms = 0.0
     for i in range(args.steps):
         torch.cuda.synchronize()
         a = time.perf_counter()
         if batch_jobs is not None:
             step(424242 + 1000 * i)
+        elif world > 1:
+            # per rank: render into device memory, reduce the films onto rank 0, read the film back
+            scene.render_device(film.data_ptr(), spp=spp, seed=rank_seed(424242 + i, rank), queue_capacity=qc,
+                                guiding=1 if args.workload == "door" else 0, **knobs)
+            combine_films(film, world, dist)
+            host_t.copy_(film)
         else:
             scene.render(spp=spp, seed=424242 + i, out=host, queue_capacity=qc,
                          guiding=1 if args.workload == "door" else 0, **knobs)
@@ -580,6 +627,15 @@ def main():
                 "tri_tests_per_ray": (p3["extend_tri_tests"] + p3["shadow_tri_tests"]) / max(1, rays_e + rays_s),
                 "traversal_share_fused": (k3_ms["extend"] + k3_ms["shadow"]) / max(1e-9, sum(k3_ms.values())),
                 "k_extend_alone": extend_alone,
+                # the bound the traversal actually meets: L1/TEX throughput (one ncu capture, one launch)
+                "l1": (lambda l1: None if l1 is None else {
+                    "bound": "l1tex", "frac": l1["l1tex_data_pipe_lsu_wavefronts_pct_of_peak_elapsed"] / 100.0,
+                    "unit": "fraction of the L1/TEX data-pipe LSU wavefront peak (elapsed)",
+                    "throughput_active": l1["l1tex_throughput_pct_of_peak_active"] / 100.0,
+                    "global_ld_bytes_per_launch": 32 * l1["global_ld_sectors"],
+                    "global_ld_gbs": 32 * l1["global_ld_sectors"] / (l1["duration_us"] * 1e-6) / 1e9,
+                    "l1_hit_rate": l1["l1tex_sectors_hit"] / max(1, l1["l1tex_sectors_hit"] + l1["l1tex_sectors_miss"]),
+                    "source": l1["source"]})(l1_profile()),
                 "kernel_share": {k: k_ms[k] / max(1e-9, sum(k_ms.values())) for k in kn}}
 
     if batch_jobs is None:
@@ -596,7 +652,8 @@ def main():
                                     "c5": C5_WORKLOAD + ", 1024 spp, plain NEE+MIS",
                                     "phong": WORKLOAD_PHONG}[args.workload],
                        "parallelism": "replicas x%d, FP64 film reduce" % world,
-                       "autotuned": tune, "autotune_probe_ms": tune_ms,
+                       "reduce_ms_per_step": reduce_ms / args.steps if world > 1 else None,
+                       "autotuned": tune, "autotune_probe_ms": tune_ms, "autotune_probe": tune_probe,
                        "l2": "256 MB buffer written between timed steps; path state > L2",
                        "queue_capacity": prof["queue_capacity"], "grid_trace": prof["grid_trace"],
                        "grid_shade": prof["grid_shade"], "scene_load_s": load_s,
@@ -614,6 +671,10 @@ def main():
         study = "c5" if args.workload == "c5" else "door"
         line["equal_time_relmse"] = guided_vs_plain(wr, study, plain_spp=1024 if study == "c5" else 256,
                                                     seeds=1 if study == "c5" else 3)
+        if args.workload == "heightfield" and not args.no_c5:
+            # the second guided-vs-plain target (config 5, 10M triangles): plain Mpaths/s and the
+            # equal-time ratio at 256 spp, one seed
+            line["c5"] = guided_vs_plain(wr, "c5", plain_spp=256, seeds=1)
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()

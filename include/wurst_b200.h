@@ -234,6 +234,12 @@ int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *desc, double
  * its time per render into *best_ms. */
 int wr_autotune(wr_scene *scene, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms);
 
+/* The same search for a batch (no counterpart in the reference): each candidate is timed on
+ * wr_render_batch over the n probe jobs (their cameras, spp and depths as given; a caller
+ * usually passes a subset of its batch at reduced spp). */
+int wr_autotune_batch(wr_scene *scene, const wr_job *jobs, int n, const wr_render_desc *base, wr_render_desc *best,
+                      double *best_ms);
+
 /* ---- Learned guiding proposal (no counterpart in the reference) ----
  * A 64-64-64-64-64-64 ReLU MLP (BF16 weights and activations, FP32 accumulation on
  * the tensor cores, FP32 master weights) maps 64 encoded inputs -- the hit position

@@ -93,7 +93,7 @@ EXPORTS = ["wr_scene_create", "wr_scene_create_ex", "wr_scene_create_from_json",
            "wr_scene_set_camera_json", "wr_render", "wr_render_device", "wr_get_render_stats",
            "wr_trace_closest", "wr_trace_hits", "wr_trace_occluded", "wr_trace_stats", "wr_write_pfm", "wr_read_image", "wr_run_simple2",
            "wr_run_jsimple2", "wr_set_device", "wr_last_error", "wr_abi_version", "wr_render_device_noalloc", "wr_render_batch",
-           "wr_render_batch_device", "wr_autotune", "wr_guide_reset", "wr_guide_get_params", "wr_guide_set_params",
+           "wr_render_batch_device", "wr_autotune", "wr_autotune_batch", "wr_guide_reset", "wr_guide_get_params", "wr_guide_set_params",
            "wr_guide_box", "wr_guide_eval", "wr_guide_gradient", "wr_guide_train"]
 
 _lib = None
@@ -126,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     L.wr_autotune.argtypes = [vp, ctypes.POINTER(RenderDesc), ip, ctypes.POINTER(RenderDesc),
                               ctypes.POINTER(ctypes.c_double)]
     L.wr_render_batch_device.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), fp]
+    L.wr_autotune_batch.argtypes = [vp, ctypes.POINTER(Job), ip, ctypes.POINTER(RenderDesc), ctypes.POINTER(RenderDesc),
+                                    ctypes.POINTER(ctypes.c_double)]
     L.wr_get_render_stats.argtypes = [vp, ctypes.POINTER(RenderStats)]
     L.wr_trace_closest.argtypes = [vp, fp, ip, fp, fp, fp, fp]
     L.wr_trace_hits.argtypes = [vp, fp, ip, fp, fp, fp, fp]
@@ -278,10 +280,7 @@ class Scene:
         keys = ("queue_capacity", "grid_trace", "grid_shade", "trace_block", "use_graph", "fetch_threshold")
         return {k: getattr(best, k) for k in keys}, ms.value
 
-    def render_batch(self, jobs, queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
-                     trace_block=None, fetch_threshold=None):
-        """jobs: list of dicts {camera (dict or JSON text), num_spp, num_path_vertices, seed}.
-        Returns one (H, W, 3) float64 image per job, rendered in one wavefront."""
+    def _job_array(self, jobs):
         import json as _json
         n = len(jobs)
         arr = (Job * n)()
@@ -302,6 +301,28 @@ class Scene:
             arr[i].num_spp = int(j.get("num_spp", 0))
             arr[i].num_path_vertices = int(j.get("num_path_vertices", 0))
             arr[i].seed = int(j.get("seed", 0)) & 0xFFFFFFFF
+        return arr, keep, shapes
+
+    def autotune_batch(self, jobs, **base):
+        """The autotuner timed on render_batch over `jobs` (a probe subset of a batch); returns
+        (settings dict, ms per probe batch)."""
+        arr, keep, _ = self._job_array(jobs)
+        d0 = self._desc(None, None, 0, 0, base.get("queue_capacity"), base.get("grid_trace"), base.get("grid_shade"),
+                        base.get("use_graph", True), 0, base.get("trace_block"))
+        best = RenderDesc()
+        ms = ctypes.c_double(0.0)
+        _check(load_library().wr_autotune_batch(self._h, arr, len(jobs), ctypes.byref(d0), ctypes.byref(best),
+                                                ctypes.byref(ms)))
+        del keep
+        keys = ("queue_capacity", "grid_trace", "grid_shade", "trace_block", "use_graph", "fetch_threshold")
+        return {k: getattr(best, k) for k in keys}, ms.value
+
+    def render_batch(self, jobs, queue_capacity=None, grid_trace=None, grid_shade=None, use_graph=True, profile=0,
+                     trace_block=None, fetch_threshold=None):
+        """jobs: list of dicts {camera (dict or JSON text), num_spp, num_path_vertices, seed}.
+        Returns one (H, W, 3) float64 image per job, rendered in one wavefront."""
+        n = len(jobs)
+        arr, keep, shapes = self._job_array(jobs)
         total = sum(h * w for h, w in shapes)
         out = np.empty(total * 3, np.float64)
         d = self._desc(None, None, 0, 0, queue_capacity, grid_trace, grid_shade, use_graph, profile, trace_block,

@@ -1345,11 +1345,73 @@ int wr_render_batch_device(wr_scene *s, const wr_job *jobs, int n, const wr_rend
     }
 }
 
+}  // extern "C"
+
+namespace {
+
+// Coordinate descent over the wavefront knobs: traversal block size, wavefront capacity,
+// persistent-CTA counts of the traversal and shading kernels, dynamic-fetch threshold. `probe`
+// renders once with a candidate and returns its device time (ms); each candidate is scored by
+// the mean of two probes after a warm-up probe. A setting replaces the current one only when it
+// is 2 % faster: smaller differences are within the run-to-run spread of a probe render.
+template <class Probe>
+wr_render_desc tune_knobs(wr_scene &s, wr_render_desc cur, Probe probe, double *best_ms) {
+    constexpr double kTuneMargin = 0.98;
+    int sms = 148;
+    WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device));
+    auto trial = [&](const wr_render_desc &d) {
+        probe(d);   // warm (allocations, caches)
+        return 0.5 * (probe(d) + probe(d));
+    };
+    double bt = trial(cur);
+    // 1) traversal block size (its persistent grid follows the occupancy of that size)
+    for (int blk : {64, 128, 256}) {
+        wr_render_desc d = cur;
+        d.trace_block = blk;
+        d.grid_trace = 0;
+        const double t = trial(d);
+        if (t < bt * kTuneMargin) { bt = t; cur = d; }
+    }
+    // 2) wavefront capacity
+    for (int cap : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
+        wr_render_desc d = cur;
+        d.queue_capacity = cap;
+        const double t = trial(d);
+        if (t < bt * kTuneMargin) { bt = t; cur = d; }
+    }
+    // 3) persistent-CTA count of the traversal and shading kernels
+    const int blk = (cur.trace_block == 64 || cur.trace_block == 256) ? cur.trace_block : 128;
+    const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk, s.dev.patches != nullptr, s.dev.wnodes != nullptr));
+    const int occ_s = sms * std::max(1, wrk::occupancy_blocks(1));
+    for (double f : {0.5, 1.0}) {
+        wr_render_desc d = cur;
+        d.grid_trace = std::max(sms, int(occ_t * f));
+        const double t = trial(d);
+        if (t < bt * kTuneMargin) { bt = t; cur = d; }
+    }
+    for (double f : {0.5, 1.0}) {
+        wr_render_desc d = cur;
+        d.grid_shade = std::max(sms, int(occ_s * f));
+        const double t = trial(d);
+        if (t < bt * kTuneMargin) { bt = t; cur = d; }
+    }
+    // 4) dynamic ray fetching threshold
+    for (int th : {12, 16, 24, 28}) {
+        wr_render_desc d = cur;
+        d.fetch_threshold = th;
+        const double t = trial(d);
+        if (t < bt * kTuneMargin) { bt = t; cur = d; }
+    }
+    if (best_ms) *best_ms = bt;
+    return cur;
+}
+
+}  // namespace
+
+extern "C" {
+
 int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_render_desc *best, double *best_ms) {
     if (!s || !best) { g_last_error = "null argument"; return WR_ERR_INVALID_ARGUMENT; }
-    // a setting replaces the current one only when its probe is 2 % faster: smaller differences are
-    // within the run-to-run spread of a probe render
-    constexpr double kTuneMargin = 0.98;
     try {
         wr_render_desc cur{};
         if (base) cur = *base;
@@ -1359,60 +1421,39 @@ int wr_autotune(wr_scene *s, const wr_render_desc *base, int probe_spp, wr_rende
         if (!s->host.has_camera) throw Error(WR_ERR_INVALID_ARGUMENT, "scene has no camera");
         DevBuf out;
         out.alloc(size_t(c.width) * c.height * 3 * 8);
-        int sms = 148;
-        WR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
-        auto trial = [&](const wr_render_desc &d) {
-            render(*s, &d, out.as<double>(), false);   // warm (allocations, caches)
-            double t = 0.0;
-            for (int k = 0; k < 2; ++k) {
-                render(*s, &d, out.as<double>(), false);
-                t += s->stats.render_ms;
-            }
-            return t / 2.0;
+        auto probe = [&](const wr_render_desc &d) {
+            render(*s, &d, out.as<double>(), false);
+            return s->stats.render_ms;
         };
-        double bt = trial(cur);
-        // 1) traversal block size (its persistent grid follows the occupancy of that size)
-        for (int blk : {64, 128, 256}) {
-            wr_render_desc d = cur;
-            d.trace_block = blk;
-            d.grid_trace = 0;
-            const double t = trial(d);
-            if (t < bt * kTuneMargin) { bt = t; cur = d; }
-        }
-        // 2) wavefront capacity
-        for (int cap : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
-            wr_render_desc d = cur;
-            d.queue_capacity = cap;
-            const double t = trial(d);
-            if (t < bt * kTuneMargin) { bt = t; cur = d; }
-        }
-        // 3) persistent-CTA count of the traversal and shading kernels
-        const int blk = (cur.trace_block == 64 || cur.trace_block == 256) ? cur.trace_block : 128;
-        const int occ_t = sms * std::max(1, wrk::occupancy_blocks(0, blk, s->dev.patches != nullptr, s->dev.wnodes != nullptr));
-        const int occ_s = sms * std::max(1, wrk::occupancy_blocks(1));
-        for (double f : {0.5, 1.0}) {
-            wr_render_desc d = cur;
-            d.grid_trace = std::max(sms, int(occ_t * f));
-            const double t = trial(d);
-            if (t < bt * kTuneMargin) { bt = t; cur = d; }
-        }
-        for (double f : {0.5, 1.0}) {
-            wr_render_desc d = cur;
-            d.grid_shade = std::max(sms, int(occ_s * f));
-            const double t = trial(d);
-            if (t < bt * kTuneMargin) { bt = t; cur = d; }
-        }
-        // 4) dynamic ray fetching threshold
-        for (int th : {12, 16, 24, 28}) {
-            wr_render_desc d = cur;
-            d.fetch_threshold = th;
-            const double t = trial(d);
-            if (t < bt * kTuneMargin) { bt = t; cur = d; }
-        }
-        *best = cur;
+        *best = tune_knobs(*s, cur, probe, best_ms);
         if (base) { best->num_spp = base->num_spp; best->profile = base->profile; }
         else { best->num_spp = 0; }
-        if (best_ms) *best_ms = bt;
+        return WR_OK;
+    } catch (const Error &e) {
+        return fail(e);
+    }
+}
+
+int wr_autotune_batch(wr_scene *s, const wr_job *jobs, int n, const wr_render_desc *base, wr_render_desc *best,
+                      double *best_ms) {
+    if (!s || !best || !jobs || n <= 0) { g_last_error = "null argument or empty job list"; return WR_ERR_INVALID_ARGUMENT; }
+    try {
+        wr_render_desc cur{};
+        if (base) cur = *base;
+        cur.profile = 0;
+        size_t pix = 0;
+        for (int i = 0; i < n; ++i) {
+            const wr::Camera c = jobs[i].camera_json ? wr::parse_camera_json(jobs[i].camera_json) : s->host.camera;
+            pix += size_t(c.width) * size_t(c.height);
+        }
+        DevBuf out;
+        out.alloc(pix * 3 * 8);
+        auto probe = [&](const wr_render_desc &d) {
+            render_batch(*s, jobs, n, &d, out.as<double>(), false);
+            return s->stats.render_ms;
+        };
+        *best = tune_knobs(*s, cur, probe, best_ms);
+        if (base) best->profile = base->profile;
         return WR_OK;
     } catch (const Error &e) {
         return fail(e);
