@@ -77,3 +77,46 @@ def test_traversal_block_sizes_agree(wr_lib, block):
         a = sc.render(spp=16, seed=2, trace_block=block)
         b = sc.render(spp=16, seed=2)
     assert np.allclose(a, b, rtol=1e-9, atol=1e-12)
+
+
+def test_batch_jobs_pass_the_reference_image_bar(wr_lib):
+    """Eight jobs of one batch render the cornell fixture's own camera with different seeds,
+    between jobs of other cameras and resolutions; together they are K = 8 independent renders
+    and must pass the image bar of the single renders against the reference's 4096-spp images
+    (relMSE within 2 x the reference noise floor, every 8x8 block |z| < 4, mean within 1 %)."""
+    from conftest import GOLDEN
+    from test_gpu_render import block_z, relmse
+    path, meta = golden_scene("cornell")
+    cam = json.load(open(path))["camera"]
+    ref_a = np.load("%s/cornell_ref_hi_a.npy" % GOLDEN).astype(np.float64)
+    ref_b = np.load("%s/cornell_ref_hi_b.npy" % GOLDEN).astype(np.float64)
+    others = jobs_for_test()
+    jobs = []
+    for k in range(8):
+        jobs.append({"camera": cam, "num_spp": meta["hi_spp"] // 8, "num_path_vertices": 10, "seed": 3000 + 7 * k})
+        jobs.append(others[k % len(others)])
+    with wr_lib.Scene.from_file(path) as sc:
+        imgs = sc.render_batch(jobs)
+    runs = np.stack(imgs[0::2])
+    assert runs.shape[1:] == ref_a.shape and np.isfinite(runs).all()
+    img = runs.mean(axis=0)
+    floor = relmse(ref_b, ref_a)
+    err = relmse(img, ref_a)
+    assert err <= 2.0 * floor + 1e-6, "relMSE %.3g vs reference noise floor %.3g" % (err, floor)
+    z = block_z(runs, ref_a)
+    assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
+    assert abs(img.mean() / ref_a.mean() - 1.0) < 0.01
+
+
+def test_batch_autotuner_returns_valid_settings(wr_lib):
+    """wr_autotune_batch times probe batches; its settings change the schedule, not the images."""
+    path, _ = golden_scene("cornell")
+    jobs = jobs_for_test()
+    with wr_lib.Scene.from_file(path) as sc:
+        best, ms = sc.autotune_batch(jobs[:3])
+        assert best["trace_block"] in (0, 64, 128, 256) and ms > 0
+        assert best["queue_capacity"] in (0, 1 << 19, 1 << 20, 1 << 21, 1 << 22)
+        a = sc.render_batch(jobs, **{k: v for k, v in best.items() if k != "use_graph"})
+        b = sc.render_batch(jobs)
+    for x, y in zip(a, b):
+        assert np.allclose(x, y, rtol=1e-9, atol=1e-12)
