@@ -665,6 +665,23 @@ def main():
             "roofline": roofline,
             "clocks": clk,
             "mrays_per_s": (k_items["extend"] + k_items["shadow"]) * world * args.steps / (max_ms / 1e3) / 1e6}
+    if world == 1 and args.workload == "heightfield" and args.bvh_width in (0, 2):
+        # the on-device LBVH build (Morton codes, radix sort, Karras topology, refit) of the same
+        # scene: its device build time and the throughput of renders on that tree
+        with wr.Scene.from_file(path, bvh_builder=wr.BVH_DEVICE_LBVH) as ls:
+            li = ls.info
+            for i in range(2):
+                ls.render_device(film.data_ptr(), spp=spp, seed=31 + i, queue_capacity=qc, **knobs)
+            lms = []
+            for i in range(3):
+                flush.fill_(float(i))
+                torch.cuda.synchronize()
+                ls.render_device(film.data_ptr(), spp=spp, seed=41 + i, queue_capacity=qc, **knobs)
+                lms.append(ls.stats["render_ms"])
+        line["lbvh"] = {"build_ms_device": li["bvh_ms"], "scene_create_ms": li["build_ms"], "bvh_nodes": li["bvh_nodes"],
+                        "bvh_depth": li["bvh_depth"], "mpaths_s": W * H * spp / (sorted(lms)[1] * 1e3),
+                        "host_sah": {"build_ms": info["bvh_ms"], "bvh_nodes": info["bvh_nodes"], "mpaths_s": value},
+                        "note": "same workload and settings, tree built on the device instead of by the host binned SAH"}
     if rank == 0 and not args.no_cpu_baseline and batch_jobs is None:
         line["cpu_baseline"] = cpu_baseline(path)
     if world == 1 and not args.no_guiding and args.workload in ("heightfield", "c5"):

@@ -72,75 +72,157 @@ __device__ __forceinline__ bool fetch_point(const InferSource &s, uint32_t i, f3
     return true;
 }
 
-// Inference: kGroups warpgroups per CTA, each running its own chain of 128-row tiles
-// (its own activation tile, TMEM columns, mbarrier and named barrier) over weights
-// loaded once per CTA, so one group's tensor-core work overlaps another's epilogue.
+// Inference: kGroups warpgroups per CTA, and each warpgroup keeps kPair 128-row tiles in
+// flight, each with its own activation tile, 64 TMEM columns and mbarrier. The group's
+// first thread issues a tile's layer as soon as that tile's previous epilogue is stored, so
+// while the group converts one tile's accumulators (tcgen05.ld, ReLU, bf16, st.shared) the
+// tensor core runs the other tile's MMAs: kGroups x kPair = 4 tiles per CTA, 8 per SM, over
+// weights loaded once per CTA. The next pair's path records are prefetched into L2 while the
+// current pair runs.
 // Output: lobes as FP32 (kLobeFloat4 float4 per row, the validation API) or packed
 // halves (chunk-major with `packed_stride`, the render).
 constexpr int kGroups = 2;
-constexpr size_t kInferSmem = size_t(kWeightBytesInfer) + size_t(kGroups) * kActBytes + 64;
+constexpr int kPair = 2;
+constexpr int kInferCtasPerSm = 2;
+constexpr size_t kInferSmem = size_t(kWeightBytesInfer) + size_t(kGroups * kPair) * kActBytes + 64;
 
-__global__ void __launch_bounds__(kTile *kGroups, 3) k_guide_infer(GuideNet g, InferSource src, float4 *lobes_f,
-                                                                  uint4 *lobes_packed, size_t packed_stride) {
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// gathers and encodes row `row` of a tile into `at` (all-zero features when the row is past the
+// end or its path did not hit a surface); returns whether the row has a guide point
+__device__ __forceinline__ bool stage_row(const InferSource &src, const GuideNet &g, unsigned char *at, int r,
+                                          uint32_t row, uint32_t n_rows) {
+    float x[kW];
+    f3 p, n, wo;
+    const bool valid = row < n_rows && fetch_point(src, row, p, n, wo);
+    if (valid) encode(p, n, wo, g, x);
+    else {
+#pragma unroll
+        for (int k = 0; k < kW; ++k) x[k] = 0.f;
+    }
+    store_row(at, r, x);
+    return valid;
+}
+
+__device__ __forceinline__ void issue_layer(unsigned char *at, const unsigned char *wt, int l, uint32_t tmem,
+                                            uint64_t *mbar) {
+    const uint32_t idesc = idesc_bf16(128, l == kLayers - 1 ? kLastRows : kW, 0, 0);
+    const uint32_t a0 = smem_addr(at), b0 = smem_addr(wt + l * 8192);
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks)
+        mma_bf16(tmem, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 256, 128, 1024), idesc,
+                 ks > 0 ? 1u : 0u);
+    mma_commit(smem_addr(mbar));
+}
+
+__global__ void __launch_bounds__(kTile *kGroups, kInferCtasPerSm) k_guide_infer(GuideNet g, InferSource src,
+                                                                                float4 *lobes_f, uint4 *lobes_packed,
+                                                                                size_t packed_stride) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *wt = smem;                                   // weight tiles (last layer: 48 rows)
     const int tid = threadIdx.x, grp = tid >> 7, r = tid & 127, warp = tid >> 5;
-    unsigned char *at = smem + kWeightBytesInfer + grp * kActBytes;   // this group's activation tile
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kWeightBytesInfer + kGroups * kActBytes) + grp;
-    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kWeightBytesInfer + kGroups * kActBytes + 8 * kGroups);
-    if (warp == 0) tmem_alloc(smem_addr(slot), 64 * kGroups);
-    if (r == 0) mbar_init(smem_addr(mbar), 1);
+    unsigned char *act[kPair];                                  // this group's activation tiles
+#pragma unroll
+    for (int j = 0; j < kPair; ++j) act[j] = smem + kWeightBytesInfer + (grp * kPair + j) * kActBytes;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kWeightBytesInfer + kGroups * kPair * kActBytes) + grp * kPair;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kWeightBytesInfer + kGroups * kPair * kActBytes +
+                                                  8 * kGroups * kPair);
+    if (warp == 0) tmem_alloc(smem_addr(slot), 64 * kGroups * kPair);
+    if (r == 0)
+        for (int j = 0; j < kPair; ++j) mbar_init(smem_addr(mbar + j), 1);
     load_weights(wt, g.w, kLastRows);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
-    const uint32_t tmem = *slot + uint32_t(64 * grp);
+    const uint32_t tmem0 = *slot + uint32_t(64 * kPair * grp);
+    const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
     const int bar = 1 + grp;
     const uint32_t n_rows = src.rows ? src.nrows : *src.count;
-    const uint32_t ntiles = (n_rows + kTile - 1) / kTile;
-    uint32_t phase = 0;
-    for (uint32_t tile = blockIdx.x * kGroups + grp; tile < ntiles; tile += gridDim.x * kGroups) {
-        const uint32_t row = tile * kTile + r;
-        float x[kW];
-        f3 p, n, wo;
-        const bool valid = row < n_rows && fetch_point(src, row, p, n, wo);
-        if (valid) encode(p, n, wo, g, x);
-        else {
+    const uint32_t npairs = (n_rows + kTile * kPair - 1) / (kTile * kPair);
+    const uint32_t pair_step = gridDim.x * kGroups;
+    uint32_t phase[kPair] = {0u, 0u};
+    bool failed = false;
+    for (uint32_t pr = blockIdx.x * kGroups + grp; pr < npairs && !failed; pr += pair_step) {
+        if (!src.rows) {   // the next pair's path records toward L2 while this pair runs
+            const uint32_t nrow = (pr + pair_step) * (kTile * kPair) + r;
 #pragma unroll
-            for (int k = 0; k < kW; ++k) x[k] = 0.f;
+            for (int j = 0; j < kPair; ++j)
+                if (nrow + j * kTile < n_rows) {
+                    prefetch_l2(src.hit + nrow + j * kTile);
+                    prefetch_l2(src.o + nrow + j * kTile);
+                    prefetch_l2(src.d + nrow + j * kTile);
+                }
         }
-        store_row(at, r, x);
+        uint32_t row[kPair];
+        bool valid[kPair];
+#pragma unroll
+        for (int j = 0; j < kPair; ++j) {
+            row[j] = (pr * kPair + j) * kTile + r;
+            valid[j] = stage_row(src, g, act[j], r, row[j], n_rows);
+        }
         fence_async_smem();
         fence_before_sync();
         group_sync(bar);
         fence_after_sync();
-        if (!mlp_forward_tile(at, wt, mbar, tmem, phase, x, bar, kLastRows)) {
-            if (r == 0) atomicExch(g.err, 1u);
-            break;
-        }
-        if (row < n_rows) {
-            Lobes L;
-            raw_to_lobes(x, L);
-            if (lobes_packed) {
-                store_packed_lobes(lobes_packed, packed_stride, row, L, valid);
-            } else {
-                float4 *out = lobes_f + kLobeFloat4 * size_t(row);
-                if (valid) {
+        if (r == 0)
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) out[k] = make_float4(L.mu[k][0], L.mu[k][1], L.mu[k][2], L.lam[k]);
-                    out[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
-                    out[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
-                } else {
-                    out[8] = make_float4(0.f, 0.f, 0.f, 0.f);   // zero weights: no lobe
-                    out[9] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int j = 0; j < kPair; ++j) issue_layer(act[j], wt, 0, tmem0 + 64 * j, mbar + j);
+        float out[kW];
+        for (int l = 0; l < kLayers; ++l) {
+#pragma unroll
+            for (int j = 0; j < kPair; ++j) {
+                const uint32_t tm = tmem0 + 64 * j;
+                // every thread waits on the tile's mbarrier (bounded); a wait that gave up is
+                // voted on once per pair, so that the group's barriers stay in step
+                if (!mbar_wait(smem_addr(mbar + j), phase[j], kWaitIters)) failed = true;
+                phase[j] ^= 1u;
+                fence_after_sync();
+                if (l < kLayers - 1) {   // hidden layer: ReLU, bf16, back into the tile in place
+                    tmem_ld32(tm + lane_base, out);
+                    store_row_relu(act[j], r, out, 0, 4);
+                    tmem_ld32(tm + lane_base + 32, out);
+                    store_row_relu(act[j], r, out, 32, 4);
+                    fence_async_smem();
+                    fence_before_sync();
+                    group_sync(bar);
+                    fence_after_sync();
+                    if (r == 0) issue_layer(act[j], wt, l + 1, tm, mbar + j);
+                    continue;
+                }
+                tmem_ld32(tm + lane_base, out);   // outputs 0..47
+                tmem_ld16(tm + lane_base + 32, out + 32);
+                if (row[j] < n_rows) {
+                    Lobes L;
+                    raw_to_lobes(out, L);
+                    if (lobes_packed) {
+                        store_packed_lobes(lobes_packed, packed_stride, row[j], L, valid[j]);
+                    } else {
+                        float4 *o4 = lobes_f + kLobeFloat4 * size_t(row[j]);
+                        if (valid[j]) {
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) o4[k] = make_float4(L.mu[k][0], L.mu[k][1], L.mu[k][2], L.lam[k]);
+                            o4[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
+                            o4[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
+                        } else {
+                            o4[8] = make_float4(0.f, 0.f, 0.f, 0.f);   // zero weights: no lobe
+                            o4[9] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        }
+                    }
                 }
             }
         }
+        // every thread has read its TMEM lanes and the tensor core no longer reads the tiles;
+        // the vote ends the group's work when any of its waits gave up
+        fence_before_sync();
+        failed = group_any(bar, failed);
+        fence_after_sync();
+        if (failed) break;
     }
+    if (failed && r == 0) atomicExch(g.err, 1u);
     fence_before_sync();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(*slot, 64 * kGroups);
+    if (warp == 0) tmem_dealloc(*slot, 64 * kGroups * kPair);
 }
 
 // ----------------------------------------------------------------- training ----
@@ -504,7 +586,7 @@ void guide_get_master(const GuideNet &g, float *host_w, cudaStream_t st) {
     check(cudaStreamSynchronize(st), "guide get");
 }
 
-int infer_grid(int sms) { return sms * 3; }   // three CTAs per SM (shared memory and registers)
+int infer_grid(int sms) { return sms * kInferCtasPerSm; }   // CTAs per SM allowed by shared memory and TMEM
 
 void guide_infer_rows(const GuideNet &g, const float *rows_dev, uint32_t n, float4 *lobes_dev, int sms, cudaStream_t st) {
     InferSource s{};

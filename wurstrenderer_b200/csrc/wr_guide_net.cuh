@@ -1,8 +1,7 @@
-// The guiding network's per-tile building blocks, shared by the stand-alone
-// inference / training kernels (wr_guide.cu) and the fused guided shade kernel
-// (wr_kernels.cu): feature encoding, the bf16 canonical operand tiles, the
-// five-layer tcgen05 forward pass over one 128-row tile, and the output
-// transform to von Mises-Fisher lobes.
+// The guiding network's per-tile building blocks, shared by the inference and
+// training kernels (wr_guide.cu) and the guided shade kernel (wr_kernels.cu):
+// feature encoding, the bf16 canonical operand tiles, the output transform to
+// von Mises-Fisher lobes and their packed form.
 #pragma once
 
 #include <cstdint>
@@ -122,53 +121,6 @@ __device__ __forceinline__ void store_row_relu(unsigned char *tile, int row, con
         q.w = relu_bf16x2(v[8 * j + 6], v[8 * j + 7]);
         *reinterpret_cast<uint4 *>(tile + tile_offset(row, c0 + 8 * j)) = q;
     }
-}
-
-// ------------------------------------------------------------------ forward ----
-// The five layers over the 128-row tile whose features are stored in `at` by the 128
-// threads of one warpgroup (stores fenced for the async proxy, the group synchronised
-// on named barrier `bar` by the caller). Thread r of the group (r = threadIdx.x % 128)
-// receives row r's raw outputs in `out`. The group's first thread issues each layer's
-// four K=16 MMAs (M=128, N=64; N=last_n for the last layer) into the 64 TMEM columns at
-// `tmem`; every thread waits on the group's mbarrier (bounded) and reads its TMEM lane
-// back. Returns false on every thread of the group when a wait timed out (the caller
-// then does not use the outputs). On return the tensor core no longer reads `at`;
-// out[0..47] hold the last layer's outputs (out[48..63] are undefined).
-__device__ __forceinline__ bool mlp_forward_tile(unsigned char *at, const unsigned char *wt, uint64_t *mbar,
-                                                 uint32_t tmem, uint32_t &phase, float *out, int bar,
-                                                 int last_n = kW) {
-    const int r = threadIdx.x & 127;
-    const uint32_t lane_base = uint32_t(((threadIdx.x >> 5) & 3) * 32) << 16;
-    for (int l = 0; l < kLayers; ++l) {
-        if (r == 0) {
-            const uint32_t idesc = idesc_bf16(128, l == kLayers - 1 ? last_n : kW, 0, 0);
-            const uint32_t a0 = smem_addr(at), b0 = smem_addr(wt + l * 8192);
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks)
-                mma_bf16(tmem, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 256, 128, 1024), idesc,
-                         ks > 0 ? 1u : 0u);
-            mma_commit(smem_addr(mbar));
-        }
-        // one warp polls the mbarrier; the others wait on the group barrier without issuing
-        const bool ok = r >= 32 || mbar_wait(smem_addr(mbar), phase, kWaitIters);
-        phase ^= 1u;
-        if (group_any(bar, !ok)) return false;
-        fence_after_sync();
-        if (l < kLayers - 1) {   // hidden layer: two halves of 32 columns (fewer live registers)
-            tmem_ld32(tmem + lane_base, out);
-            store_row_relu(at, r, out, 0, 4);
-            tmem_ld32(tmem + lane_base + 32, out);
-            store_row_relu(at, r, out, 32, 4);
-            fence_async_smem();
-        } else {                 // outputs 0..47
-            tmem_ld32(tmem + lane_base, out);
-            tmem_ld16(tmem + lane_base + 32, out + 32);
-        }
-        fence_before_sync();
-        group_sync(bar);
-        fence_after_sync();
-    }
-    return true;
 }
 
 // -------------------------------------------------------------- output lobes ----
