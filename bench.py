@@ -680,7 +680,8 @@ def main():
                 lms.append(ls.stats["render_ms"])
         line["lbvh"] = {"build_ms_device": li["bvh_ms"], "scene_create_ms": li["build_ms"], "bvh_nodes": li["bvh_nodes"],
                         "bvh_depth": li["bvh_depth"], "mpaths_s": W * H * spp / (sorted(lms)[1] * 1e3),
-                        "host_sah": {"build_ms": info["bvh_ms"], "bvh_nodes": info["bvh_nodes"], "mpaths_s": value},
+                        "host_sah": {"build_ms": info["bvh_ms"], "bvh_nodes": info["bvh_nodes"],
+                                     "bvh_depth": info["bvh_depth"], "mpaths_s": value},
                         "note": "same workload and settings, tree built on the device instead of by the host binned SAH"}
     if rank == 0 and not args.no_cpu_baseline and batch_jobs is None:
         line["cpu_baseline"] = cpu_baseline(path)
