@@ -634,7 +634,8 @@ def main():
                     "throughput_active": l1["l1tex_throughput_pct_of_peak_active"] / 100.0,
                     "global_ld_bytes_per_launch": 32 * l1["global_ld_sectors"],
                     "global_ld_gbs": 32 * l1["global_ld_sectors"] / (l1["duration_us"] * 1e-6) / 1e9,
-                    "l1_hit_rate": l1["l1tex_sectors_hit"] / max(1, l1["l1tex_sectors_hit"] + l1["l1tex_sectors_miss"]),
+                    "l1_hit_rate": l1["l1tex_sector_hit_rate_pct"] / 100.0,
+                    "active_threads_per_instruction": l1["active_threads_per_instruction"],
                     "source": l1["source"]})(l1_profile()),
                 "kernel_share": {k: k_ms[k] / max(1e-9, sum(k_ms.values())) for k in kn}}
 

@@ -65,7 +65,7 @@ typedef struct wr_render_desc {
                                 least four passes */
     int guide_batch;         /* training records per Adam step; 0 = 16384 */
     int guide_steps;         /* Adam steps of the training phase, spread evenly over its passes; 0 = a
-                                budget of about 12 % of the render's device time (estimated from the first
+                                budget of about 18 % of the render's device time (estimated from the first
                                 pass), 256 to 8192 steps */
     float guide_clamp;       /* loss weights are clamped at guide_clamp x their mean over the pass;
                                 0 = 1000, < 0 = no clamp */
