@@ -1,9 +1,10 @@
 """Test infrastructure only: Python access to the CPU oracle.
 
 The oracle is the FP64 CPU restatement of the reference's
-``nextevent_path_tracer`` (``oracle/nee_oracle.cpp``) and, where
-``/root/reference`` is present, the reference's own renderer code compiled
-from its sources (``oracle/_ref/wurst_ref``, built by ``oracle/Makefile``).
+``nextevent_path_tracer`` (``oracle/nee_oracle.cpp``) and, where the
+reference's sources are present (``REFERENCE_ROOT``), the reference's own
+renderer code compiled from them (``oracle/_ref/wurst_ref``, built by
+``oracle/Makefile``).
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg use this module, always as the checker, never as the measured product.
 """
