@@ -213,3 +213,38 @@ def test_tree_shape_option_errors(wr_lib):
         with pytest.raises(wr_lib.WurstError) as e:
             wr_lib.Scene.from_file(path, **bad)
         assert e.value.status == 1     # WR_ERR_INVALID_ARGUMENT
+
+
+def test_degenerate_and_coincident_triangles(wr_lib, oracle_lib, tmp_path):
+    """Zero-area triangles (collinear and repeated vertices) and exact duplicates of the Cornell
+    box's triangles in one scene: the build and traversal take them, closest hits match the oracle
+    except on ties (a duplicate is a tie), and no ray reports a degenerate triangle."""
+    from wurstrenderer_b200 import scenes
+    spec = scenes.cornell_spec()
+    dup = [m for m in spec.meshes if m.name in ("tall_box", "floor")]
+    for m in dup:
+        spec.add(m.name + "_copy", spec.materials[m.material], m.positions.copy(), m.triangles.copy())
+    mat = spec.materials["m_floor"]
+    spec.add("degenerate", mat, np.array([[0, 0.5, 0], [0.5, 0.5, 0], [1.0, 0.5, 0], [0.2, 1.0, 0.2]], np.float32),
+             np.array([[0, 1, 2], [3, 3, 3], [0, 0, 1]], np.int64))
+    path = scenes.write_scene(str(tmp_path), "degenerate", spec, dict(scenes.CORNELL_CAMERA, resolution=[16, 16]),
+                              [scenes.nee_render("o.pfm", 4, 6)])
+    rng = np.random.default_rng(11)
+    n = 4096
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = rng.uniform([-0.95, 0.05, -0.95], [0.95, 1.95, 0.95], size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3] = 1e-4
+    rays[:, 7] = np.inf
+    osc = oracle_lib.OracleScene(path)
+    go, po, to, uv_ref = osc.trace_closest(rays)
+    with wr_lib.Scene.from_file(path) as sc:
+        g, p, t, uv = sc.trace_closest(rays)
+        occ = sc.trace_occluded(rays)
+        img = sc.render(spp=16, seed=1)
+    same = (g == go) & (p == po)
+    assert (~same & ~_tie_or_edge(to, t, uv_ref)).sum() == 0
+    assert np.isfinite(img).all() and img.mean() > 0
+    lo, hi = osc.trace_occluded_bracket(rays)
+    assert_within_bracket(occ, lo, hi)
