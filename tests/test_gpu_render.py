@@ -27,14 +27,20 @@ def relmse(x, ref, eps=1e-2):
     return float(np.mean((x - ref) ** 2 / (ref ** 2 + eps)))
 
 
-def block_z(runs, ref, block=8, ref_pair=None):
+def block_z(runs, ref, block=8, ref_pair=None, ref_var=None):
     """z scores of 8x8 block means; runs: K x H x W x 3 independent renders.
 
     Without ref_pair the reference's variance is taken equal to the GPU's (same spp, same
     estimator): z = (gpu - ref) / sqrt(2 var_gpu). With ref_pair = (ref_a, ref_b), two independent
     halves whose mean is `ref`, the reference's own variance is estimated from them per pixel,
     (a - b)^2 / 4, and z = (gpu - ref) / sqrt(var_gpu + var_ref) -- needed when the GPU estimator
-    is much less noisy than the reference (the learned proposal)."""
+    is much less noisy than the reference (the learned proposal).
+
+    ref_var (H x W x 3): a second per-pixel estimate of the variance of `ref`, from more samples of
+    the reference's own estimator; each block then takes the larger of the two. Two halves give
+    one degree of freedom per pixel, and for path-traced light through a narrow gap their sample
+    variance is often well below the true one (rare high-contribution paths are missing from
+    both halves), which would make the test reject a correct renderer whose own noise is low."""
     k, h, w, _ = runs.shape
     hb, wb = h // block, w // block
     r = runs[:, :hb * block, :wb * block].reshape(k, hb, block, wb, block, 3)
@@ -45,8 +51,11 @@ def block_z(runs, ref, block=8, ref_pair=None):
     if ref_pair is None:
         return (mean_b - ref_b) / np.sqrt(2.0 * var_b + 1e-30)
     a, b = ref_pair
-    ref_var = ((a - b) ** 2 / 4.0)[:hb * block, :wb * block]
-    var_r = ref_var.reshape(hb, block, wb, block, 3).sum(axis=(1, 3)) / (block * block) ** 2
+    pair_var = ((a - b) ** 2 / 4.0)[:hb * block, :wb * block]
+    var_r = pair_var.reshape(hb, block, wb, block, 3).sum(axis=(1, 3)) / (block * block) ** 2
+    if ref_var is not None:
+        other = ref_var[:hb * block, :wb * block].reshape(hb, block, wb, block, 3).sum(axis=(1, 3)) / (block * block) ** 2
+        var_r = np.maximum(var_r, other)
     return (mean_b - ref_b) / np.sqrt(var_b + var_r + 1e-30)
 
 

@@ -904,9 +904,11 @@ double train_records(wr_scene &s, const float4 *records, uint32_t n, uint32_t ba
         const uint32_t first = uint32_t((uint64_t(k) * batch) % n);
         const uint32_t cnt = std::min(batch, n - first);
         if (per_step) WR_CUDA(cudaMemsetAsync(s.g_loss.p, 0, 8, st));
+        // each kernel may be scheduled while the one before it ends (its set-up and the first
+        // records' gather overlap that kernel); it waits for it before reading its results
         const int nslots = wrg::guide_gradient(s.guide, records, first + cnt, first, n, stride, c_max,
-                                               s.g_loss.as<double>(), st);
-        wrg::guide_adam(s.guide, lr, 1.f / float(cnt), ++s.guide_step, nslots, st);
+                                               s.g_loss.as<double>(), st, k > 0 && !per_step);
+        wrg::guide_adam(s.guide, lr, 1.f / float(cnt), ++s.guide_step, nslots, st, true);
         if (per_step) {
             double l = 0.0;
             WR_CUDA(cudaMemcpyAsync(&l, s.g_loss.p, 8, cudaMemcpyDeviceToHost, st));

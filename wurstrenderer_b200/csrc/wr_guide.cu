@@ -35,9 +35,6 @@
 
 namespace wrg {
 
-// training kernel shared memory: W 40 KB, W^T 40 KB, X_0..X_4 80 KB, dH 16 KB + 8 KB pad, barrier
-constexpr int kTrainBarrier = 163840 + 16384 + 8192;
-
 // --------------------------------------------------------------- inference ----
 // Inputs come either from the wavefront (hit point of every live path) or from an
 // explicit array of (p, n, wo) rows (validation).
@@ -130,7 +127,7 @@ __global__ void __launch_bounds__(kTile *kGroups, kInferCtasPerSm) k_guide_infer
     if (warp == 0) tmem_alloc(smem_addr(slot), 64 * kGroups * kPair);
     if (r == 0)
         for (int j = 0; j < kPair; ++j) mbar_init(smem_addr(mbar + j), 1);
-    load_weights(wt, g.w, kLastRows);
+    load_weight_image(wt, g.w, kWeightBytesInfer);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
@@ -226,82 +223,172 @@ __global__ void __launch_bounds__(kTile *kGroups, kInferCtasPerSm) k_guide_infer
 }
 
 // ----------------------------------------------------------------- training ----
-// Gradient of -c log p(w) with respect to the 40 used outputs (oracle: loss_grad_output).
-__device__ __forceinline__ float loss_grad(const float *o, f3 d, float c, float c_max, float *go) {
+// A training tile is 128 rows (records); the CTA's 512 threads are four warpgroups over the same
+// rows. Warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31, so the thread of warpgroup j and
+// row r takes, in every epilogue, columns [16 j, 16 j + 16) of row r, and in the loss gradient
+// lobes 2 j and 2 j + 1 (the row's mixture density is summed over the four threads through
+// shared memory). One elected thread issues the MMAs; the dW products of a backward layer are
+// issued after the commit that the epilogue waits for, so they run under it.
+constexpr int kTrainGroups = 4;
+constexpr int kTrainThreads = kTile * kTrainGroups;
+
+// shared memory: W and W^T images 40 KB each, X_0..X_4 80 KB, two dH tiles of 16 KB, each
+// followed by 8 KB of zeros (the operand reach of the weight-gradient MMA stays inside the
+// allocation for either reading of the descriptor's two strides), the density exchange
+// (4 x 128 floats), two mbarriers and the TMEM address slot
+constexpr int kTrainW = 0, kTrainWt = kWeightBytes, kTrainX = 2 * kWeightBytes;
+constexpr int kTrainDh = kTrainX + kLayers * kActBytes;
+constexpr int kTrainDhStride = kActBytes + 8192;
+constexpr int kTrainExch = kTrainDh + 2 * kTrainDhStride;
+constexpr int kTrainBarrier = kTrainExch + kTrainGroups * kTile * 4;
+constexpr size_t kTrainSmem = size_t(kTrainBarrier) + 64;
+static_assert(kTrainSmem <= 227 * 1024, "training tile does not fit in shared memory");
+
+// Terms of the mixture-NLL gradient (oracle: loss_grad_output) for lobes 2 J and 2 J + 1 of a
+// row, from the row's 40 used outputs o (5 per lobe: axis, sharpness, weight logit) and the
+// sample direction d. Returns the two lobes' share of the mixture density p(d).
+struct LobeTerms {
+    float w[2], f[2], lam[2], cosk[2], mu[2][3], inr[2], e2[2], s[2];
+};
+
+template <int J>
+__device__ __forceinline__ float lobe_terms(const float *o, f3 d, LobeTerms &t) {
     float amax = -1e30f;
+#pragma unroll
     for (int k = 0; k < 8; ++k) amax = fmaxf(amax, o[5 * k + 4]);
-    float w[8], f[8], lam[8], cosk[8], mu[8][3], nr[8], s[8], wsum = 0.f;
+    float ew[8], wsum = 0.f;
+#pragma unroll
     for (int k = 0; k < 8; ++k) {
+        ew[k] = __expf(o[5 * k + 4] - amax);
+        wsum += ew[k];
+    }
+    const float inv_wsum = __fdividef(1.f, wsum);
+    float pp = 0.f;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int k = 2 * J + j;
         const float rx = o[5 * k], ry = o[5 * k + 1], rz = o[5 * k + 2];
-        nr[k] = fmaxf(sqrtf(rx * rx + ry * ry + rz * rz), 1e-12f);
-        mu[k][0] = rx / nr[k]; mu[k][1] = ry / nr[k]; mu[k][2] = rz / nr[k];
-        s[k] = o[5 * k + 3];
-        lam[k] = fminf(softplus(s[k]) + kLambdaMin, kLambdaMax);
-        w[k] = __expf(o[5 * k + 4] - amax);
-        wsum += w[k];
+        t.inr[j] = __fdividef(1.f, fmaxf(sqrtf(rx * rx + ry * ry + rz * rz), 1e-12f));
+        t.mu[j][0] = rx * t.inr[j];
+        t.mu[j][1] = ry * t.inr[j];
+        t.mu[j][2] = rz * t.inr[j];
+        t.s[j] = o[5 * k + 3];
+        t.lam[j] = fminf(softplus(t.s[j]) + kLambdaMin, kLambdaMax);
+        t.w[j] = ew[k] * inv_wsum;
+        t.cosk[j] = t.mu[j][0] * d.x + t.mu[j][1] * d.y + t.mu[j][2] * d.z;
+        t.e2[j] = __expf(-2.f * t.lam[j]);   // lam >= kLambdaMin: 1 - e2 >= 0.63
+        t.f[j] = __fdividef(t.lam[j], 2.f * wrd::kPi * (1.f - t.e2[j])) * __expf(t.lam[j] * (t.cosk[j] - 1.f));
+        pp += t.w[j] * t.f[j];
     }
-    float p = 0.f;
-    for (int k = 0; k < 8; ++k) {
-        w[k] /= wsum;
-        cosk[k] = mu[k][0] * d.x + mu[k][1] * d.y + mu[k][2] * d.z;
-        f[k] = lam[k] / (2.f * wrd::kPi * -expm1f(-2.f * lam[k])) * __expf(lam[k] * (cosk[k] - 1.f));
-        p += w[k] * f[k];
+    return pp;
+}
+
+// d(-c log p)/d(outputs) of the two lobes (cc = the clamped loss weight, ip = 1 / p) into
+// columns [10 J, 10 J + 10) of a row of the dH tile; the thread of lobes 6 and 7 also zeroes
+// the unused columns 40..63
+template <int J>
+__device__ __forceinline__ void lobe_grads_store(const LobeTerms &t, f3 d, float cc, float ip, bool active,
+                                                 unsigned char *tile, int row) {
+    float go[10];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const float resp = t.w[j] * t.f[j] * ip;
+        const float dldl = __fdividef(1.f, t.lam[j]) - __fdividef(2.f * t.e2[j], 1.f - t.e2[j]) + (t.cosk[j] - 1.f);
+        const float sig = __fdividef(1.f, 1.f + __expf(-t.s[j]));
+        const float a = -cc * resp * t.lam[j] * t.inr[j];
+        go[5 * j + 0] = a * (d.x - t.mu[j][0] * t.cosk[j]);
+        go[5 * j + 1] = a * (d.y - t.mu[j][1] * t.cosk[j]);
+        go[5 * j + 2] = a * (d.z - t.mu[j][2] * t.cosk[j]);
+        go[5 * j + 3] = -cc * resp * dldl * sig;
+        go[5 * j + 4] = -cc * (resp - t.w[j]);
     }
-    p = fmaxf(p, 1e-30f);
-    const float cc = fminf(c, c_max);
-    for (int k = 0; k < 8; ++k) {
-        const float resp = w[k] * f[k] / p;
-        const float e2 = __expf(-2.f * lam[k]);
-        const float dldl = 1.f / lam[k] - 2.f * e2 / -expm1f(-2.f * lam[k]) + (cosk[k] - 1.f);
-        const float sig = 1.f / (1.f + __expf(-s[k]));
-        go[5 * k + 4] = -cc * (resp - w[k]);
-        go[5 * k + 3] = -cc * resp * dldl * sig;
-        const float a = -cc * resp * lam[k] / nr[k];
-        go[5 * k + 0] = a * (d.x - mu[k][0] * cosk[k]);
-        go[5 * k + 1] = a * (d.y - mu[k][1] * cosk[k]);
-        go[5 * k + 2] = a * (d.z - mu[k][2] * cosk[k]);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const __nv_bfloat162 h = active ? __floats2bfloat162_rn(go[2 * i], go[2 * i + 1]) : __floats2bfloat162_rn(0.f, 0.f);
+        *reinterpret_cast<__nv_bfloat162 *>(tile + tile_offset(row, 10 * J + 2 * i)) = h;
     }
-    for (int k = 40; k < kW; ++k) go[k] = 0.f;
-    return -cc * logf(p);
+    if (J == 3)
+#pragma unroll
+        for (int c = 40; c < kW; c += 8) *reinterpret_cast<uint4 *>(tile + tile_offset(row, c)) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+__device__ __forceinline__ float lobe_terms_of(int j, const float *o, f3 d, LobeTerms &t) {
+    switch (j) {
+    case 0: return lobe_terms<0>(o, d, t);
+    case 1: return lobe_terms<1>(o, d, t);
+    case 2: return lobe_terms<2>(o, d, t);
+    default: return lobe_terms<3>(o, d, t);
+    }
+}
+
+__device__ __forceinline__ void lobe_grads_store_of(int j, const LobeTerms &t, f3 d, float cc, float ip, bool active,
+                                                    unsigned char *tile, int row) {
+    switch (j) {
+    case 0: lobe_grads_store<0>(t, d, cc, ip, active, tile, row); break;
+    case 1: lobe_grads_store<1>(t, d, cc, ip, active, tile, row); break;
+    case 2: lobe_grads_store<2>(t, d, cc, ip, active, tile, row); break;
+    default: lobe_grads_store<3>(t, d, cc, ip, active, tile, row); break;
+    }
+}
+
+// columns [16 j, 16 j + 16) of a 64-wide row x into a tile
+__device__ __forceinline__ void store_row_part(unsigned char *tile, int row, const float *x, int j) {
+    switch (j) {
+    case 0: store_row(tile, row, x, 0, 2); break;
+    case 1: store_row(tile, row, x + 16, 16, 2); break;
+    case 2: store_row(tile, row, x + 32, 32, 2); break;
+    default: store_row(tile, row, x + 48, 48, 2); break;
+    }
 }
 
 // training records: kRecordFloat4 float4 each (layout in wr_guide.h)
 // rows [first, count) of the minibatch map to records (row * stride) % total (a fixed shuffle
 // when stride and total are coprime)
-__global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 *records, uint32_t count,
-                                                      uint32_t first, uint32_t total,
-                                                      uint32_t stride, float c_max, double *loss_out) {
+__global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, const float4 *records, uint32_t count,
+                                                                 uint32_t first, uint32_t total, uint32_t stride,
+                                                                 float c_max, double *loss_out) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *wt = smem;                       // W tiles   5 x 8 KB
-    unsigned char *wtt = smem + 40960;              // W^T tiles 5 x 8 KB
-    unsigned char *xt = smem + 81920;               // X_0..X_4  5 x 16 KB
-    // dH: 16 KB + 8 KB of zeroed padding, so that the operand reach of the weight-gradient
-    // MMA stays inside this allocation for either reading of the descriptor's two strides
-    unsigned char *dh = smem + 163840;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kTrainBarrier);
-    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kTrainBarrier + 8);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    unsigned char *wt = smem + kTrainW;      // W image   5 x 8 KB
+    unsigned char *wtt = smem + kTrainWt;    // W^T image 5 x 8 KB
+    unsigned char *xt = smem + kTrainX;      // X_0..X_4  5 x 16 KB (the layer inputs, kept for backward)
+    float *exch = reinterpret_cast<float *>(smem + kTrainExch);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kTrainBarrier);   // [0] MMA completion, [1] weights
+    uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kTrainBarrier + 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = warp >> 2;                 // column slice and lobe pair of this thread
+    const int r = (warp & 3) * 32 + lane;      // row of the tile = TMEM lane
+    const uint32_t n = count > first ? count - first : 0u;
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    const bool has_tiles = blockIdx.x < ntiles;
+    const uint32_t mb = smem_addr(mbar), mbw = smem_addr(mbar + 1);
+    // The optimiser step that follows may be scheduled now: it waits for this grid before it reads
+    // the partial gradients. In turn this kernel runs its set-up and the first tile's gather and
+    // encoding before it waits for the previous optimiser step, whose weights it then loads.
+    griddep_launch_dependents();
     if (warp == 0) tmem_alloc(smem_addr(slot), 512);
-    if (tid == 0) mbar_init(smem_addr(mbar), 1);
-    load_weights(wt, g.w);
-    load_weights(wtt, g.wt);
-    for (int i = tid; i < 8192 / 4; i += blockDim.x) reinterpret_cast<uint32_t *>(dh + 16384)[i] = 0u;
+    if (tid == 0) {
+        mbar_init(mb, 1);
+        mbar_init(mbw, 1);
+    }
+    for (int i = tid; i < 2 * 512; i += kTrainThreads)   // the zeros behind both dH tiles
+        reinterpret_cast<uint4 *>(smem + kTrainDh + (i >> 9) * kTrainDhStride + kActBytes)[i & 511] =
+            make_uint4(0u, 0u, 0u, 0u);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = *slot;
-    const uint32_t tD = tmem, tdW = tmem + 64;       // columns [0,64) scratch, [64, 384) dW of layers 0..4
-    const uint32_t lane_base = uint32_t(warp * 32) << 16;
-    const uint32_t n = count > first ? count - first : 0u;
-    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    const uint32_t tD = tmem, tdW = tmem + 64;   // columns [0, 64) scratch, [64, 384) dW of layers 0..4
+    const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
     const uint32_t id_fwd = idesc_bf16(128, 64, 0, 0);
     const uint32_t id_dw = idesc_bf16(64, 64, 1, 1);
     uint32_t phase = 0;
-    bool failed = false, any_tile = false;
+    // failed: a wait of this thread gave up; stop: the CTA's vote on it at the next barrier (a
+    // failure is acted on only after the vote, so that every thread leaves at the same barrier)
+    bool failed = false, stop = false, any_tile = false, weights_in = !has_tiles;
     double loss = 0.0;
-    for (uint32_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        const uint32_t row = tile * kTile + tid;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t row = tile * kTile + r;
         const bool valid = row < n;
         float x[kW];
         f3 dir = mk(0.f, 1.f, 0.f);
@@ -317,112 +404,149 @@ __global__ void __launch_bounds__(kTile) k_guide_train(GuideNet g, const float4 
 #pragma unroll
             for (int k = 0; k < kW; ++k) x[k] = 0.f;
         }
-        store_row(xt, tid, x);
+        store_row_part(xt, r, x, grp);
+        if (tile == blockIdx.x) {
+            // the previous kernels of the stream are complete from here on: the weight images may
+            // be read and this CTA's partial-gradient slot written
+            griddep_wait();
+            if (tid == 0) {   // both weight images in two bulk copies
+                mbar_expect_tx(mbw, 2 * kWeightBytes);
+                bulk_load(smem_addr(wt), g.w, kWeightBytes, mbw);
+                bulk_load(smem_addr(wtt), g.wt, kWeightBytes, mbw);
+            }
+        }
         fence_async_smem();
         fence_before_sync();
         __syncthreads();
         fence_after_sync();
         // forward; X_l kept for the backward pass
-        float out[kW];
+        float out[48];
         for (int l = 0; l < kLayers; ++l) {
             if (tid == 0) {
-                const uint32_t a0 = smem_addr(xt + l * 16384), b0 = smem_addr(wt + l * 8192);
+                if (!weights_in) {
+                    weights_in = mbar_wait(mbw, 0, kWaitIters);
+                    failed = failed || !weights_in;
+                }
+                if (weights_in) {
+                    const uint32_t a0 = smem_addr(xt + l * kActBytes), b0 = smem_addr(wt + l * 8192);
 #pragma unroll
-                for (int ks = 0; ks < 4; ++ks)
-                    mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 256, 128, 1024), id_fwd,
-                             ks > 0 ? 1u : 0u);
-                mma_commit(smem_addr(mbar));
+                    for (int ks = 0; ks < 4; ++ks)
+                        mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 256, 128, 1024), id_fwd,
+                                 ks > 0 ? 1u : 0u);
+                }
+                mma_commit(mb);
             }
-            const bool ok = warp != 0 || mbar_wait(smem_addr(mbar), phase, kWaitIters);   // warp 0 polls
+            if (!mbar_wait(mb, phase, kWaitIters)) failed = true;
             phase ^= 1u;
-            if (__syncthreads_or(!ok)) { failed = true; break; }
             fence_after_sync();
-            tmem_ld64(tD + lane_base, out);
-            if (l < kLayers - 1) store_row_relu(xt + (l + 1) * 16384, tid, out);
+            if (l == kLayers - 1) {   // outputs 0..47 for the loss
+                tmem_ld32(tD + lane_base, out);
+                tmem_ld16(tD + lane_base + 32, out + 32);
+                break;
+            }
+            float v[16];
+            tmem_ld16(tD + lane_base + 16 * grp, v);
+            store_row_relu(xt + (l + 1) * kActBytes, r, v, 16 * grp, 2);
             fence_async_smem();
             fence_before_sync();
-            __syncthreads();
+            stop = __syncthreads_or(failed);
             fence_after_sync();
+            if (stop) break;
         }
-        if (failed) break;
-        // loss gradient at the outputs -> dH (bf16)
-        float go[kW];
-        if (valid && c > 0.f) {
-            loss += double(loss_grad(out, dir, c, c_max, go));
-        } else {
-#pragma unroll
-            for (int k = 0; k < kW; ++k) go[k] = 0.f;
-        }
-        store_row(dh, tid, go);
+        if (stop) break;
+        // loss gradient at the outputs -> dH tile 0 (bf16)
+        const bool active = valid && c > 0.f;
+        LobeTerms lt{};
+        exch[grp * kTile + r] = active ? lobe_terms_of(grp, out, dir, lt) : 0.f;
+        fence_before_sync();
+        stop = __syncthreads_or(failed);
+        fence_after_sync();
+        if (stop) break;
+        const float p = fmaxf(exch[r] + exch[kTile + r] + exch[2 * kTile + r] + exch[3 * kTile + r], 1e-30f);
+        const float cc = fminf(c, c_max);
+        if (active && grp == 0) loss += double(-cc * __logf(p));
+        lobe_grads_store_of(grp, lt, dir, cc, __fdividef(1.f, p), active, smem + kTrainDh, r);
         fence_async_smem();
         fence_before_sync();
         __syncthreads();
         fence_after_sync();
-        // backward
+        // backward: dH alternates between the two tiles
+        int cur = 0;
         for (int l = kLayers - 1; l >= 0; --l) {
+            unsigned char *dh = smem + kTrainDh + cur * kTrainDhStride;
+            unsigned char *dh_next = smem + kTrainDh + (cur ^ 1) * kTrainDhStride;
             if (tid == 0) {
-                // dW_l += dH^T X_l : M = 64 (out), N = 64 (in), K = 128 (rows), MN-major operands
-                const uint32_t a0 = smem_addr(dh), b0 = smem_addr(xt + l * 16384);
-#pragma unroll
-                for (int ks = 0; ks < 8; ++ks)
-                    mma_bf16(tdW + 64 * l, smem_desc(a0 + ks * 2048, 1024, 128), smem_desc(b0 + ks * 2048, 1024, 128),
-                             id_dw, (any_tile || ks > 0) ? 1u : 0u);
+                const uint32_t a0 = smem_addr(dh);
                 if (l > 0) {
-                    // dX = dH W_l : M = 128, N = 64 (in), K = 64 (out); B = W^T tile
+                    // dX = dH W_l : M = 128, N = 64 (in), K = 64 (out); B = the W^T tile
                     const uint32_t c0 = smem_addr(wtt + l * 8192);
 #pragma unroll
                     for (int ks = 0; ks < 4; ++ks)
                         mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(c0 + ks * 256, 128, 1024), id_fwd,
                                  ks > 0 ? 1u : 0u);
+                    mma_commit(mb);
                 }
-                mma_commit(smem_addr(mbar));
+                // dW_l += dH^T X_l : M = 64 (out), N = 64 (in), K = 128 (rows), MN-major operands.
+                // Issued after the commit: it runs under this layer's epilogue and the next
+                // commit covers it (the epilogue after that one overwrites this dH tile)
+                const uint32_t b0 = smem_addr(xt + l * kActBytes);
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks)
+                    mma_bf16(tdW + 64 * l, smem_desc(a0 + ks * 2048, 1024, 128), smem_desc(b0 + ks * 2048, 1024, 128),
+                             id_dw, (any_tile || ks > 0) ? 1u : 0u);
+                if (l == 0) mma_commit(mb);
             }
-            const bool ok = warp != 0 || mbar_wait(smem_addr(mbar), phase, kWaitIters);   // warp 0 polls
+            if (!mbar_wait(mb, phase, kWaitIters)) failed = true;
             phase ^= 1u;
-            if (__syncthreads_or(!ok)) { failed = true; break; }
             fence_after_sync();
             if (l > 0) {
-                float v[kW];
-                tmem_ld64(tD + lane_base, v);
-                relu_mask_row(xt + l * 16384, tid, v);   // input of layer l = ReLU output of layer l-1
-                store_row(dh, tid, v);
+                float v[16];
+                tmem_ld16(tD + lane_base + 16 * grp, v);
+                relu_mask_row(xt + l * kActBytes, r, v, 16 * grp, 2);   // input of layer l = ReLU output of layer l-1
+                store_row(dh_next, r, v, 16 * grp, 2);
             }
             fence_async_smem();
             fence_before_sync();
-            __syncthreads();
+            stop = __syncthreads_or(failed);
             fence_after_sync();
+            if (stop) break;
+            cur ^= 1;
         }
+        if (stop) break;
         any_tile = true;
     }
-    if (failed) {
+    if (tid == 0 && !weights_in) mbar_wait(mbw, 0, kWaitIters);   // no copy into shared memory outlives the CTA
+    if (stop) {
         if (tid == 0) atomicExch(g.err, 1u);
     } else if (any_tile) {
         // this CTA's dW into its own partial slot (summed in a fixed order by the optimiser, so
         // the gradient is deterministic). M = 64 accumulator row n lives in TMEM lane
         // (n % 16) + 32 (n / 16). CTA b has tiles exactly when b < ceil(rows / 128), and only
         // those slots are summed.
-        const int lane = tid & 31;
         float *slot_base = g.partial + size_t(blockIdx.x) * kParams;
+        const int nrow = 16 * (warp & 3) + lane;
         for (int l = 0; l < kLayers; ++l) {
-            float v[kW];
-            tmem_ld64(tdW + 64 * l + lane_base, v);
+            float v[16];
+            tmem_ld16(tdW + 64 * l + 16 * grp + lane_base, v);
             if (lane < 16) {
-                float4 *gr = reinterpret_cast<float4 *>(slot_base + l * kW * kW + (16 * warp + lane) * kW);
+                float4 *gr = reinterpret_cast<float4 *>(slot_base + l * kW * kW + nrow * kW + 16 * grp);
 #pragma unroll
-                for (int k = 0; k < kW / 4; ++k) gr[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+                for (int k = 0; k < 4; ++k) gr[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
             }
         }
     }
-    if (loss_out) {
-        // block reduction of the loss
-        __shared__ double red[kTile];
-        red[tid] = loss;
+    if (loss_out) {   // only the first warpgroup carries loss terms
+        __shared__ double red[kTrainThreads / 32];
+        double v = loss;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp] = v;
         __syncthreads();
-        for (int s = kTile / 2; s > 0; s >>= 1) {
-            if (tid < s) red[tid] += red[tid + s];
-            __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < kTrainThreads / 32; ++w) t += red[w];
+            atomicAdd(loss_out, t);
         }
-        if (tid == 0) atomicAdd(loss_out, red[0]);
     }
     fence_before_sync();
     __syncthreads();
@@ -469,6 +593,8 @@ __global__ void __launch_bounds__(kRedThreads) k_guide_sum(GuideNet g, int nslot
 // copies are refreshed from the master weights)
 __global__ void __launch_bounds__(kRedThreads) k_guide_adam(GuideNet g, float lr, float scale, int step, int apply,
                                                             int nslots) {
+    griddep_launch_dependents();   // the next training step may set up; it waits for this grid
+    griddep_wait();                // the partial gradients are complete; no kernel reads the weights
     const int i = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
     const float gsum = apply ? reduce_partials(g, i, nslots) : 0.f;
     if (threadIdx.x >= kRedParams) return;
@@ -487,8 +613,8 @@ __global__ void __launch_bounds__(kRedThreads) k_guide_adam(GuideNet g, float lr
     if (l < kLayers - 1 && nrow == kW - 1) w = (k == kW - 1) ? 1.f : 0.f;   // the constant unit
     g.master[i] = w;
     const __nv_bfloat16 h = __float2bfloat16_rn(w);
-    g.w[i] = h;
-    g.wt[l * kW * kW + k * kW + nrow] = h;
+    g.w[weight_image_index(l, nrow, k)] = h;
+    g.wt[weight_image_index(l, k, nrow)] = h;
 }
 
 // sum of c and number of records with c > 0 over records [0, n)
@@ -538,8 +664,6 @@ static void check(cudaError_t e, const char *what) {
         throw wr::Error(e == cudaErrorMemoryAllocation ? WR_ERR_OUT_OF_MEMORY : WR_ERR_CUDA,
                         std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-constexpr size_t kTrainSmem = kTrainBarrier + 64;
 
 void guide_alloc(GuideNet &g) {
     check(cudaMalloc(&g.w, kParams * 2), "guide alloc");
@@ -604,11 +728,29 @@ void guide_infer_wavefront(const GuideNet &g, const float4 *o, const float4 *d, 
     k_guide_infer<<<infer_grid(sms), kTile * kGroups, kInferSmem, st>>>(g, s, nullptr, lobes_packed, stride);
 }
 
+// launches a kernel, with programmatic stream serialization when `overlap` is set (the kernel
+// may then start before the previous one ends and waits for it with griddepcontrol.wait)
+template <class... Params, class... Args>
+static void launch(void (*kernel)(Params...), int grid, int block, size_t smem, cudaStream_t st, bool overlap,
+                   const char *what, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+    check(cudaLaunchKernelEx(&cfg, kernel, args...), what);
+}
+
 int guide_gradient(GuideNet &g, const float4 *records_dev, uint32_t count, uint32_t first, uint32_t total,
-                   uint32_t stride, float c_max, double *loss_dev, cudaStream_t st) {
+                   uint32_t stride, float c_max, double *loss_dev, cudaStream_t st, bool overlap) {
     // one CTA per partial-gradient slot (the shared memory allows one CTA per SM)
-    k_guide_train<<<g.slots, kTile, kTrainSmem, st>>>(g, records_dev, count, first, total, stride, c_max, loss_dev);
-    check(cudaGetLastError(), "guide train");
+    launch(k_guide_train, g.slots, kTrainThreads, kTrainSmem, st, overlap, "guide train", g, records_dev, count, first,
+           total, stride, c_max, loss_dev);
     const uint32_t rows = count > first ? count - first : 0u;
     return int(std::min<uint32_t>(uint32_t(g.slots), (rows + kTile - 1) / kTile));
 }
@@ -624,9 +766,8 @@ void guide_sum_gradient(GuideNet &g, int nslots, cudaStream_t st) {
     check(cudaGetLastError(), "guide sum");
 }
 
-void guide_adam(GuideNet &g, float lr, float scale, int step, int nslots, cudaStream_t st) {
-    k_guide_adam<<<kParams / kRedParams, kRedThreads, 0, st>>>(g, lr, scale, step, 1, nslots);
-    check(cudaGetLastError(), "guide adam");
+void guide_adam(GuideNet &g, float lr, float scale, int step, int nslots, cudaStream_t st, bool overlap) {
+    launch(k_guide_adam, kParams / kRedParams, kRedThreads, 0, st, overlap, "guide adam", g, lr, scale, step, 1, nslots);
 }
 
 }  // namespace wrg

@@ -73,8 +73,10 @@ void guide_infer_wavefront(const GuideNet &g, const float4 *o, const float4 *d, 
 // the loss gradient of minibatch rows [first, count) into the per-CTA partial slots (and the
 // summed loss added to *loss_dev when given); row r reads record (r * stride) % total. Returns
 // the number of partial slots written (pass it to guide_sum_gradient / guide_adam).
+// overlap: launched with programmatic stream serialization, so that its set-up and first gather
+// run under the previous kernel of the stream (which must be a guide_adam step or need no wait).
 int guide_gradient(GuideNet &g, const float4 *records_dev, uint32_t count, uint32_t first, uint32_t total,
-                   uint32_t stride, float c_max, double *loss_dev, cudaStream_t st);
+                   uint32_t stride, float c_max, double *loss_dev, cudaStream_t st, bool overlap = false);
 // out_dev[0] = sum of c over records [0, n) with c > 0, out_dev[1] = their number (FP64)
 void guide_cstats(const float4 *records_dev, uint32_t n, double *out_dev, int sms, cudaStream_t st);
 // the gradient of the last guide_gradient call, summed over its nslots partial slots in a fixed
@@ -82,6 +84,6 @@ void guide_cstats(const float4 *records_dev, uint32_t n, double *out_dev, int sm
 void guide_sum_gradient(GuideNet &g, int nslots, cudaStream_t st);
 // one Adam step on the gradient of the last guide_gradient call (nslots partial slots), scaled by
 // `scale`
-void guide_adam(GuideNet &g, float lr, float scale, int step, int nslots, cudaStream_t st);
+void guide_adam(GuideNet &g, float lr, float scale, int step, int nslots, cudaStream_t st, bool overlap = false);
 
 }  // namespace wrg

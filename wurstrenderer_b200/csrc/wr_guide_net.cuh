@@ -64,26 +64,30 @@ __device__ __forceinline__ void encode(f3 p, f3 n, f3 wo, const GuideNet &g, flo
     x[63] = 1.f;
 }
 
-// one 64-wide row of a canonical tile: 8 stores of 16 bytes (8 bf16 each)
-__device__ __forceinline__ void store_row(unsigned char *tile, int row, const float *v) {
+// columns [c0, c0 + 8 * chunks) of a row of a canonical tile from v[0..]: 16-byte stores of
+// 8 bf16 each (the whole 64-wide row by default)
+__device__ __forceinline__ void store_row(unsigned char *tile, int row, const float *v, int c0 = 0,
+                                          int chunks = kW / 8) {
 #pragma unroll
-    for (int c = 0; c < kW; c += 8) {
+    for (int j = 0; j < chunks; ++j) {
+        const float *u = v + 8 * j;
         uint4 q;
-        __nv_bfloat162 h0 = __floats2bfloat162_rn(v[c], v[c + 1]), h1 = __floats2bfloat162_rn(v[c + 2], v[c + 3]),
-                       h2 = __floats2bfloat162_rn(v[c + 4], v[c + 5]), h3 = __floats2bfloat162_rn(v[c + 6], v[c + 7]);
+        __nv_bfloat162 h0 = __floats2bfloat162_rn(u[0], u[1]), h1 = __floats2bfloat162_rn(u[2], u[3]),
+                       h2 = __floats2bfloat162_rn(u[4], u[5]), h3 = __floats2bfloat162_rn(u[6], u[7]);
         q.x = *reinterpret_cast<uint32_t *>(&h0);
         q.y = *reinterpret_cast<uint32_t *>(&h1);
         q.z = *reinterpret_cast<uint32_t *>(&h2);
         q.w = *reinterpret_cast<uint32_t *>(&h3);
-        *reinterpret_cast<uint4 *>(tile + tile_offset(row, c)) = q;
+        *reinterpret_cast<uint4 *>(tile + tile_offset(row, c0 + 8 * j)) = q;
     }
 }
 
-// multiplies v by the mask (x > 0) of a stored row
-__device__ __forceinline__ void relu_mask_row(const unsigned char *tile, int row, float *v) {
+// multiplies v[0..] by the mask (x > 0) of columns [c0, c0 + 8 * chunks) of a stored row
+__device__ __forceinline__ void relu_mask_row(const unsigned char *tile, int row, float *v, int c0 = 0,
+                                              int chunks = kW / 8) {
 #pragma unroll
-    for (int c = 0; c < kW; c += 8) {
-        const uint4 q = *reinterpret_cast<const uint4 *>(tile + tile_offset(row, c));
+    for (int c = 0; c < 8 * chunks; c += 8) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(tile + tile_offset(row, c0 + c));
         const uint32_t wds[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -95,17 +99,18 @@ __device__ __forceinline__ void relu_mask_row(const unsigned char *tile, int row
     }
 }
 
-// bf16 weights [l][n][k] -> canonical tiles (rows n, columns k), 16 bytes at a time; consecutive
-// threads take consecutive rows n of one 8-column chunk, so each group of 8 threads fills one
-// 128-byte core-matrix row set without shared-memory bank conflicts. Rows >= last_rows of the
-// last layer are not loaded.
-__device__ __forceinline__ void load_weights(unsigned char *dst, const __nv_bfloat16 *src, int last_rows = kW) {
+// The bf16 weight copies in global memory are kept as the kernels' shared-memory operand image:
+// tile l (8 KB) holds W_l (or W_l^T) in the canonical layout above, so a kernel brings them in
+// with a linear copy. Offset of element (row, column) of tile l, in bf16 elements:
+__device__ __forceinline__ int weight_image_index(int l, int row, int col) {
+    return (l * 8192 + tile_offset(row, col)) >> 1;
+}
+
+// the first `bytes` of a weight image into shared memory, 16 bytes per thread and step
+__device__ __forceinline__ void load_weight_image(unsigned char *dst, const __nv_bfloat16 *src, int bytes) {
     const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
-    for (int i = threadIdx.x; i < kParams / 8; i += blockDim.x) {
-        const int n = i % kW, kc = (i / kW) % (kW / 8), l = i / (kW * kW / 8);
-        if (l == kLayers - 1 && n >= last_rows) continue;
-        *reinterpret_cast<uint4 *>(dst + l * 8192 + tile_offset(n, 8 * kc)) = __ldg(s4 + (l * kW + n) * (kW / 8) + kc);
-    }
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+    for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d4[i] = __ldg(s4 + i);
 }
 
 // columns [c0, c0 + 8 * chunks) of a row of a canonical tile from FP32 values v[0..] with

@@ -83,6 +83,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar_saddr, uint32_t parity, 
     return false;
 }
 
+// announces `bytes` of asynchronous copies that will complete on the mbarrier (and arrives once)
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar_saddr, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_saddr), "r"(bytes) : "memory");
+}
+
+// bulk copy (no tensor map, no multicast) of `bytes` from this GPU's global memory into this
+// CTA's shared memory, completing on the mbarrier; both addresses 16-byte aligned, bytes a
+// multiple of 16
+__device__ __forceinline__ void bulk_load(uint32_t dst_saddr, const void *src, uint32_t bytes, uint32_t mbar_saddr) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst_saddr),
+                 "l"(src), "r"(bytes), "r"(mbar_saddr)
+                 : "memory");
+}
+
+// Programmatic dependent launch: lets the next kernel of the stream (launched with programmatic
+// stream serialization) be scheduled now; it still waits for this grid before it reads its results
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+// waits until the grids this kernel depends on have completed and their writes are visible (returns
+// at once when the kernel was launched without programmatic serialization)
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_alloc(uint32_t slot_saddr, uint32_t ncols) {   // whole warp
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot_saddr), "r"(ncols)
                  : "memory");
