@@ -842,7 +842,7 @@ HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
 }
 
 // ------------------------------------------------------------ guiding ----
-constexpr float kGuideLr = 1e-3f;          // Adam learning rate
+constexpr float kGuideLr = 2e-3f;          // Adam learning rate
 constexpr double kGuideTimeShare = 0.18;   // default training budget: share of the render's device time
 constexpr double kGuideStepMsGuess = 0.035; // Adam step time assumed before the first one is measured
 

@@ -232,6 +232,19 @@ __global__ void __launch_bounds__(kTile *kGroups, kInferCtasPerSm) k_guide_infer
 constexpr int kTrainGroups = 4;
 constexpr int kTrainThreads = kTile * kTrainGroups;
 
+// Layout of a partial-gradient slot, in the order the training CTA writes it: for layer l,
+// column block col / 16 and column quad (col % 16) / 4, the 64 output rows n hold their 4
+// consecutive columns, so the 16 threads of a warp that own rows n..n+15 store 256 contiguous
+// bytes per instruction.
+__host__ __device__ constexpr int partial_offset(int l, int n, int col) {
+    return ((l * 4 + (col >> 4)) * 4 + ((col >> 2) & 3)) * 256 + n * 4 + (col & 3);
+}
+// the inverse: parameter index (l * 4096 + n * 64 + col) of slot offset u
+__device__ __forceinline__ int partial_param(int u) {
+    const int l = u >> 12, col = ((u >> 10) & 3) * 16 + ((u >> 8) & 3) * 4 + (u & 3), n = (u >> 2) & 63;
+    return (l * kW + n) * kW + col;
+}
+
 // shared memory: W and W^T images 40 KB each, X_0..X_4 80 KB, two dH tiles of 16 KB, each
 // followed by 8 KB of zeros (the operand reach of the weight-gradient MMA stays inside the
 // allocation for either reading of the descriptor's two strides), the density exchange
@@ -529,9 +542,10 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
             float v[16];
             tmem_ld16(tdW + 64 * l + 16 * grp + lane_base, v);
             if (lane < 16) {
-                float4 *gr = reinterpret_cast<float4 *>(slot_base + l * kW * kW + nrow * kW + 16 * grp);
+                float4 *gr = reinterpret_cast<float4 *>(slot_base + partial_offset(l, nrow, 16 * grp));
 #pragma unroll
-                for (int k = 0; k < 4; ++k) gr[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+                for (int k = 0; k < 4; ++k)   // column quad k: 256 floats further on
+                    gr[64 * k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
             }
         }
     }
@@ -556,24 +570,28 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
 
 // ------------------------------------------------------------- optimiser ----
 // Deterministic sum of the per-CTA partial gradients: a block covers kRedParams consecutive
-// parameters with kRedGroups groups of threads; group j adds slots j, j + kRedGroups, ... (two
-// accumulators), then group 0 adds the group sums in order. Returns the total on group-0 threads.
+// slot offsets with kRedGroups groups of threads; group j adds slots j, j + kRedGroups, ... eight
+// loads at a time in a fixed order, then group 0 adds the group sums in order. Returns the total
+// on group-0 threads.
 constexpr int kRedParams = 64;
 constexpr int kRedGroups = 8;
 constexpr int kRedThreads = kRedParams * kRedGroups;
 
-__device__ __forceinline__ float reduce_partials(const GuideNet &g, int i, int nslots) {
+__device__ __forceinline__ float reduce_partials(const GuideNet &g, int u, int nslots) {
     __shared__ float red[kRedGroups][kRedParams];
     const int p = threadIdx.x % kRedParams, grp = threadIdx.x / kRedParams;
-    const float *part = g.partial + i;
-    float s0 = 0.f, s1 = 0.f;
-    int k = grp;
-    for (; k + kRedGroups < nslots; k += 2 * kRedGroups) {
-        s0 += part[size_t(k) * kParams];
-        s1 += part[size_t(k + kRedGroups) * kParams];
+    const float *part = g.partial + u;
+    float s = 0.f;
+    for (int k0 = grp; k0 < nslots; k0 += 8 * kRedGroups) {
+        float v[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int k = k0 + t * kRedGroups;
+            v[t] = k < nslots ? part[size_t(k) * kParams] : 0.f;
+        }
+        s += ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
     }
-    if (k < nslots) s0 += part[size_t(k) * kParams];
-    red[grp][p] = s0 + s1;
+    red[grp][p] = s;
     __syncthreads();
     float total = 0.f;
     if (grp == 0)
@@ -584,9 +602,9 @@ __device__ __forceinline__ float reduce_partials(const GuideNet &g, int i, int n
 
 // the summed gradient into g.grad (for callers that read it)
 __global__ void __launch_bounds__(kRedThreads) k_guide_sum(GuideNet g, int nslots) {
-    const int i = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
-    const float total = reduce_partials(g, i, nslots);
-    if (threadIdx.x < kRedParams) g.grad[i] = total;
+    const int u = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
+    const float total = reduce_partials(g, u, nslots);
+    if (threadIdx.x < kRedParams) g.grad[partial_param(u)] = total;
 }
 
 // one Adam step on the summed gradient (apply = 0: only the constant-unit rows and the bf16
@@ -595,9 +613,10 @@ __global__ void __launch_bounds__(kRedThreads) k_guide_adam(GuideNet g, float lr
                                                             int nslots) {
     griddep_launch_dependents();   // the next training step may set up; it waits for this grid
     griddep_wait();                // the partial gradients are complete; no kernel reads the weights
-    const int i = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
-    const float gsum = apply ? reduce_partials(g, i, nslots) : 0.f;
+    const int u = blockIdx.x * kRedParams + threadIdx.x % kRedParams;
+    const float gsum = apply ? reduce_partials(g, u, nslots) : 0.f;
     if (threadIdx.x >= kRedParams) return;
+    const int i = partial_param(u);
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
     const int l = i / (kW * kW), nrow = (i / kW) % kW, k = i % kW;
