@@ -27,29 +27,51 @@ __device__ __forceinline__ float guide_weight_sum(const wrg::PackedLobes &L) {
     return ((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + (w[6] + w[7]));
 }
 
-// vMF normaliser lambda / (2 pi (1 - exp(-2 lambda))) (lambda >= 0.5: no cancellation)
-__device__ __forceinline__ float vmf_norm(float lam) { return lam / (2.f * kPi * (1.f - __expf(-2.f * lam))); }
+// The lobes of one path vertex, prepared once for that vertex's density evaluations and its
+// sample: the packed halves, and per lobe the factor a_k = lambda_k / |m_k| (the sharpness over the
+// length of the stored axis m_k, so that lambda_k (mu_k . d) = a_k (m_k . d)) and the coefficient
+// coef_k = (w_k / sum w) lambda_k / (2 pi (1 - exp(-2 lambda_k))). The density
+//     q(d) = sum_k coef_k exp(a_k (m_k . d) - lambda_k)
+// is the same mixture as the one guide_sample draws from (lobe k with probability w_k / sum w,
+// then the vMF lobe with axis m_k / |m_k| and sharpness lambda_k).
+struct GuideVertex {
+    const wrg::PackedLobes *L;
+    float a[8], coef[8];
+};
 
-__device__ __forceinline__ float guide_pdf(const wrg::PackedLobes &L, f3 d) {
+__device__ __forceinline__ void guide_prepare(const wrg::PackedLobes &L, GuideVertex &g) {
     float mx[8], my[8], mz[8], lam[8], w[8];
     L.load(0, mx);
     L.load(1, my);
     L.load(2, mz);
     L.load(3, lam);
     L.load(4, w);
-    const float total = ((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + (w[6] + w[7]));
-    float p = 0.f;
+    const float inv_total = __fdividef(1.f, ((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + (w[6] + w[7])));
+    g.L = &L;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const float inv = rsqrtf(mx[k] * mx[k] + my[k] * my[k] + mz[k] * mz[k]);
-        const float c = (mx[k] * d.x + my[k] * d.y + mz[k] * d.z) * inv;
-        p += w[k] * vmf_norm(lam[k]) * __expf(lam[k] * (c - 1.f));
+        g.a[k] = lam[k] * rsqrtf(mx[k] * mx[k] + my[k] * my[k] + mz[k] * mz[k]);
+        // lambda >= 0.5: 1 - exp(-2 lambda) >= 0.63, no cancellation
+        g.coef[k] = w[k] * inv_total * __fdividef(lam[k], 2.f * kPi * (1.f - __expf(-2.f * lam[k])));
     }
-    return p / total;
+}
+
+__device__ __forceinline__ float guide_pdf(const GuideVertex &g, f3 d) {
+    float mx[8], my[8], mz[8], lam[8];
+    g.L->load(0, mx);
+    g.L->load(1, my);
+    g.L->load(2, mz);
+    g.L->load(3, lam);
+    float p = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        p = fmaf(g.coef[k], __expf(fmaf(g.a[k], mx[k] * d.x + my[k] * d.y + mz[k] * d.z, -lam[k])), p);
+    return p;
 }
 
 // draws a direction from the mixture: u_sel picks the lobe (by weight), (u1, u2) the direction
-__device__ __forceinline__ f3 guide_sample(const wrg::PackedLobes &L, float u_sel, float u1, float u2) {
+__device__ __forceinline__ f3 guide_sample(const GuideVertex &g, float u_sel, float u1, float u2) {
+    const wrg::PackedLobes &L = *g.L;
     float w[8], mx[8], my[8], mz[8], lam[8];
     L.load(4, w);
     const float total = ((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + (w[6] + w[7]));
@@ -71,7 +93,7 @@ __device__ __forceinline__ f3 guide_sample(const wrg::PackedLobes &L, float u_se
         if (k == pick) { ax = mx[k]; ay = my[k]; az = mz[k]; lm = lam[k]; }
     const float inv = rsqrtf(ax * ax + ay * ay + az * az);
     const float v = 1.f - u1;   // in (0, 1]
-    float ct = 1.f + __logf(v + (1.f - v) * __expf(-2.f * lm)) / lm;
+    float ct = 1.f + __fdividef(__logf(v + (1.f - v) * __expf(-2.f * lm)), lm);
     ct = fminf(fmaxf(ct, -1.f), 1.f);
     const float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
     float sp, cp;

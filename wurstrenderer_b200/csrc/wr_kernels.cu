@@ -654,6 +654,8 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                 const uint32_t lpix = pixel - J.pix_offset, seed = job_seed(J, job);
                 // learned proposal at this vertex (one-sample MIS with BSDF sampling)
                 const bool guided = gl && !primitive && guide_weight_sum(*gl) > 0.f;
+                GuideVertex gv;
+                if (guided) guide_prepare(*gl, gv);
                 // strategy A: next-event estimation toward this sample's light vertex
                 const Rand4 r0 = rand4(lpix, sample, 0, seed);
                 LightVtx l{};
@@ -680,7 +682,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                     const f3 f = bsdf_eval(mm, inL, outL);
                     if (!is_zero(f)) {
                         float pdfW = bsdf_pdf(mm, inL, outL);
-                        if (guided) pdfW = kGuideAlpha * guide_pdf(*gl, wo) + (1.f - kGuideAlpha) * pdfW;
+                        if (guided) pdfW = kGuideAlpha * guide_pdf(gv, wo) + (1.f - kGuideAlpha) * pdfW;
                         const float bsdfPdfA = pdfW * convA;
                         const float mis = l.pdfA / (l.pdfA + bsdfPdfA);
                         const float le1 = l.env ? 1.f : kInvPi;
@@ -705,14 +707,14 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                     // the density evaluation (no divergent second evaluation)
                     f3 dw;
                     if (rb.c < kGuideAlpha) {
-                        dw = guide_sample(*gl, rb.c * (1.f / kGuideAlpha), rb.a, rb.b);
+                        dw = guide_sample(gv, rb.c * (1.f / kGuideAlpha), rb.a, rb.b);
                         outL = fr.to_local(dw);
                     } else {
                         float pb_unused;
                         bsdf_sample(mm, inL, rb.a, rb.b, outL, pb_unused);
                         dw = normalize(fr.to_world(outL));
                     }
-                    pdfW = kGuideAlpha * guide_pdf(*gl, dw) + (1.f - kGuideAlpha) * bsdf_pdf(mm, inL, outL);
+                    pdfW = kGuideAlpha * guide_pdf(gv, dw) + (1.f - kGuideAlpha) * bsdf_pdf(mm, inL, outL);
                     const f3 f = bsdf_eval(mm, inL, outL);
                     wgt = (pdfW > 0.f && !is_zero(f)) ? f * (fabsf(outL.y) / pdfW) : mk(0.f, 0.f, 0.f);
                 }
@@ -760,9 +762,12 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
 }
 
 // GUIDED: the learned proposal is on (w.lobes); a separate instantiation keeps the plain
-// shade kernel's register count (and occupancy) unchanged
+// shade kernel's register count unchanged. Both run 3 blocks per SM: the guided kernel is
+// latency-bound, and at 80 registers (with spills) it measured faster than at 128 registers and
+// 2 blocks per SM (80.2 against 93.6 ms of shading in a 64-spp render of the door-gap room); 4
+// blocks (64 registers) gained nothing on it and cost 0.7 % on the plain 1M-triangle render.
 template <bool GUIDED>
-__global__ void __launch_bounds__(kShadeBlock, GUIDED ? 2 : 3) k_shade(DevScene s, WaveArgs w) {
+__global__ void __launch_bounds__(kShadeBlock, 3) k_shade(DevScene s, WaveArgs w) {
     const uint32_t n = w.ctr[CTR_ACTIVE];
     if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 1, (unsigned long long)n);
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
