@@ -323,11 +323,13 @@ def workload_scene(name):
     return p
 
 
-def guided_vs_plain(wr, name="door", plain_spp=256, seeds=2):
+def guided_vs_plain(wr, name="door", plain_spp=256, seeds=2, extra_lrs=()):
     """Equal-time relMSE of the learned proposal against plain NEE+MIS on a full-size workload,
     both measured against the reference's own FP64 render of a crop at 16384 spp
     (tests/golden/<name>_crop_ref_{a,b}.npy, two independent 8192-spp halves). The guided render
-    (training on its first 32 spp included) gets the device time of the plain render."""
+    (training on its first 32 spp included) gets the device time of the plain render. The guided
+    renders train with the workload's Adam learning rate (1e-3); each rate in `extra_lrs` adds the
+    same guided study at that rate under "lr_<rate>" (same plain renders)."""
     import numpy as np
     gdir = os.path.join(ROOT, "tests", "golden")
     meta_p = os.path.join(gdir, "%s_crop_meta.json" % name)
@@ -353,19 +355,27 @@ def guided_vs_plain(wr, name="door", plain_spp=256, seeds=2):
             plain_err.append(relmse(img[y0:y1, x0:x1], ref))
             plain_err3.append(relmse(img[y0:y1, x0:x1], ref, eps=1e-3))
         t_budget = float(np.mean(plain_ms))
-        img = sc.render(spp=plain_spp, seed=200, guiding=1)     # calibration: guided time per spp
-        st = sc.stats
-        per_spp = (st["render_ms"] - st["guide_train_ms"]) / plain_spp
-        g_spp = max(33, int((t_budget - st["guide_train_ms"]) / per_spp))
-        g_err, g_err3, g_ms, g_train = [], [], [], []
-        for i in range(seeds):
-            img = sc.render(spp=g_spp, seed=300 + i, guiding=1)
+
+        def guided(lr):
+            img = sc.render(spp=plain_spp, seed=200, guiding=1, guide_lr=lr)   # calibration: guided time per spp
             st = sc.stats
-            g_ms.append(st["render_ms"])
-            g_train.append(st["guide_train_ms"])
-            g_err.append(relmse(img[y0:y1, x0:x1], ref))
-            g_err3.append(relmse(img[y0:y1, x0:x1], ref, eps=1e-3))
-            steps, records = st["guide_steps"], st["guide_records"]
+            per_spp = (st["render_ms"] - st["guide_train_ms"]) / plain_spp
+            g_spp = max(33, int((t_budget - st["guide_train_ms"]) / per_spp))
+            r = {"spp": g_spp, "err": [], "err3": [], "ms": [], "train": []}
+            for i in range(seeds):
+                img = sc.render(spp=g_spp, seed=300 + i, guiding=1, guide_lr=lr)
+                st = sc.stats
+                r["ms"].append(st["render_ms"])
+                r["train"].append(st["guide_train_ms"])
+                r["err"].append(relmse(img[y0:y1, x0:x1], ref))
+                r["err3"].append(relmse(img[y0:y1, x0:x1], ref, eps=1e-3))
+                r["steps"], r["records"] = st["guide_steps"], st["guide_records"]
+            return r, img
+
+        res, img = guided(None)
+        g_spp, g_err, g_err3, g_ms, g_train = res["spp"], res["err"], res["err3"], res["ms"], res["train"]
+        steps, records = res["steps"], res["records"]
+        extra = {lr: guided(lr)[0] for lr in extra_lrs}
     pe, ge = float(np.mean(plain_err)), float(np.mean(g_err))
     pm, gm = float(np.mean(plain_ms)), float(np.mean(g_ms))
     npix = img.shape[0] * img.shape[1]
@@ -378,8 +388,14 @@ def guided_vs_plain(wr, name="door", plain_spp=256, seeds=2):
                 # the same with the 1e-3 epsilon of the reference's error image (util/errorimage.h:18)
                 "relmse_eps1e-3": {"plain": float(np.mean(plain_err3)), "guided": float(np.mean(g_err3)),
                                    "ratio_equal_time": (float(np.mean(g_err3)) * gm) / (float(np.mean(plain_err3)) * pm)},
+                "adam_lr": 1e-3,
                 "note": "ratio = (relMSE_guided x time_guided) / (relMSE_plain x time_plain); relMSE of an "
                         "unbiased estimator scales as 1/time, so this is the equal-time ratio"})
+    for lr, r in extra.items():
+        e, m = float(np.mean(r["err"])), float(np.mean(r["ms"]))
+        out["lr_%g" % lr] = {"adam_lr": lr, "spp": r["spp"], "relmse": e, "ms": m,
+                             "train_ms": float(np.mean(r["train"])), "adam_steps": r["steps"],
+                             "relmse_ratio_equal_time": (e * m) / (pe * pm)}
     return out
 
 
@@ -689,11 +705,12 @@ def main():
     if world == 1 and not args.no_guiding and args.workload in ("heightfield", "c5"):
         study = "c5" if args.workload == "c5" else "door"
         line["equal_time_relmse"] = guided_vs_plain(wr, study, plain_spp=1024 if study == "c5" else 256,
-                                                    seeds=1 if study == "c5" else 3)
+                                                    seeds=1 if study == "c5" else 3,
+                                                    extra_lrs=() if study == "c5" else (2e-3,))
         if args.workload == "heightfield" and not args.no_c5:
             # the second guided-vs-plain target (config 5, 10M triangles): plain Mpaths/s and the
             # equal-time ratio at 256 spp, two seeds
-            line["c5"] = guided_vs_plain(wr, "c5", plain_spp=256, seeds=2)
+            line["c5"] = guided_vs_plain(wr, "c5", plain_spp=256, seeds=2, extra_lrs=(2e-3,))
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()

@@ -75,7 +75,8 @@ typedef struct wr_render_desc {
                                 from the work, (waves + 2) * (num_path_vertices + 2) + 64). A render
                                 that has not drained when its bound is reached stops and returns
                                 WR_ERR_TIMEOUT; the handle stays usable */
-    int reserved[2];
+    float guide_lr;          /* Adam learning rate of the training phase; 0 = 1e-3 */
+    int reserved[1];
 } wr_render_desc;
 
 typedef struct wr_render_stats {

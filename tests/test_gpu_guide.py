@@ -357,3 +357,18 @@ def test_full_combination_crop_matches_reference(wr_lib, tmp_path, guiding):
     z = block_z(runs, ref, ref_pair=(ref_a, ref_b))
     assert np.abs(z).max() < 4.0, "max |z| %.2f" % np.abs(z).max()
     assert abs(img.mean() / ref.mean() - 1.0) < 0.01
+
+
+def test_guide_learning_rate_is_validated_and_used(wr_lib, cornell):
+    """wr_render_desc.guide_lr: negative or non-finite rates are rejected; two rates train two
+    different networks (same seeds otherwise), both giving finite images."""
+    for bad in (-1e-3, float("nan"), float("inf")):
+        with pytest.raises(wr_lib.WurstError) as e:
+            cornell.render(spp=4, seed=3, guiding=1, guide_train_spp=2, guide_steps=16, guide_lr=bad)
+        assert e.value.status == 1     # WR_ERR_INVALID_ARGUMENT
+    imgs, nets = [], []
+    for lr in (1e-3, 5e-3):
+        imgs.append(cornell.render(spp=8, seed=3, guiding=1, guide_train_spp=4, guide_steps=64, guide_lr=lr))
+        nets.append(cornell.guide_params().copy())
+    assert all(np.isfinite(i).all() for i in imgs)
+    assert not np.array_equal(nets[0], nets[1])

@@ -44,7 +44,7 @@ class RenderDesc(ctypes.Structure):
                 ("trace_block", ctypes.c_int), ("integrator", ctypes.c_int), ("guiding", ctypes.c_int),
                 ("guide_train_spp", ctypes.c_int), ("guide_pass_spp", ctypes.c_int), ("guide_batch", ctypes.c_int),
                 ("guide_steps", ctypes.c_int), ("guide_clamp", ctypes.c_float), ("fetch_threshold", ctypes.c_int),
-                ("max_iterations", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+                ("max_iterations", ctypes.c_int), ("guide_lr", ctypes.c_float), ("reserved", ctypes.c_int * 1)]
 
 
 class Job(ctypes.Structure):
@@ -217,7 +217,8 @@ class Scene:
     @staticmethod
     def _desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
               profile=0, trace_block=None, integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
-              guide_batch=None, guide_steps=None, guide_clamp=None, fetch_threshold=None, max_iterations=None):
+              guide_batch=None, guide_steps=None, guide_clamp=None, fetch_threshold=None, max_iterations=None,
+              guide_lr=None):
         d = RenderDesc()
         d.num_spp = int(spp or 0)
         d.num_path_vertices = int(num_path_vertices or 0)
@@ -239,18 +240,20 @@ class Scene:
         d.guide_clamp = float(guide_clamp or 0.0)
         d.fetch_threshold = int(fetch_threshold or 0)
         d.max_iterations = int(max_iterations or 0)
+        d.guide_lr = float(guide_lr or 0.0)
         return d
 
     def render(self, spp=None, num_path_vertices=None, seed=0, render_index=0, queue_capacity=None,
                grid_trace=None, grid_shade=None, use_graph=True, out=None, profile=0, trace_block=None,
                integrator=None, guiding=0, guide_train_spp=None, guide_pass_spp=None,
                guide_batch=None, guide_steps=None, guide_clamp=None, fetch_threshold=None,
-               max_iterations=None) -> np.ndarray:
+               max_iterations=None, guide_lr=None) -> np.ndarray:
         """Renders into host memory; returns an (H, W, 3) float64 image (row 0 = top).
         integrator: None (the render entry's), "nextevent_path_tracer", "primitive_path_tracer" or
         "light_splatting".
         guiding: 0 / "off" (plain NEE+MIS), 1 / "train" (learned proposal trained online on the first
-        guide_train_spp samples, default 32), 2 / "frozen" (the scene's current network, no training).
+        guide_train_spp samples, default 32), 2 / "frozen" (the scene's current network, no training);
+        guide_lr: the Adam learning rate of the training (default 1e-3).
         max_iterations: lowers the wavefront's iteration bound (debugging; a render that needs more
         raises WurstError with status WR_ERR_TIMEOUT)."""
         inf = self.info
@@ -258,7 +261,7 @@ class Scene:
             out = np.empty((inf["height"], inf["width"], 3), np.float64)
         d = self._desc(spp, num_path_vertices, seed, render_index, queue_capacity, grid_trace, grid_shade, use_graph,
                        profile, trace_block, integrator, guiding, guide_train_spp, guide_pass_spp, guide_batch,
-                       guide_steps, guide_clamp, fetch_threshold, max_iterations)
+                       guide_steps, guide_clamp, fetch_threshold, max_iterations, guide_lr)
         _check(load_library().wr_render(self._h, ctypes.byref(d), _ptr(out)))
         return out
 

@@ -842,7 +842,7 @@ HostJob scene_job(const wr::Scene &h, const wr_render_desc &desc) {
 }
 
 // ------------------------------------------------------------ guiding ----
-constexpr float kGuideLr = 2e-3f;          // Adam learning rate
+constexpr float kGuideLr = 1e-3f;          // default Adam learning rate (wr_render_desc.guide_lr = 0)
 constexpr double kGuideTimeShare = 0.18;   // default training budget: share of the render's device time
 constexpr double kGuideStepMsGuess = 0.035; // Adam step time assumed before the first one is measured
 
@@ -956,6 +956,9 @@ void render_guided(wr_scene &s, const wr_render_desc &desc, double *out, bool ou
     if (base.integrator != wrd::INTEGRATOR_NEE)
         throw Error(WR_ERR_UNSUPPORTED, "guiding applies to nextevent_path_tracer only");
     if (desc.guiding != 1 && desc.guiding != 2) throw Error(WR_ERR_INVALID_ARGUMENT, "guiding must be 0, 1 or 2");
+    if (!(desc.guide_lr >= 0.f) || !std::isfinite(desc.guide_lr))
+        throw Error(WR_ERR_INVALID_ARGUMENT, "guide_lr must be a finite value >= 0");
+    const float lr = desc.guide_lr > 0.f ? desc.guide_lr : kGuideLr;
     if (base.spp <= 0) throw Error(WR_ERR_INVALID_ARGUMENT, "num_spp must be positive");
     ensure_guide(s);
     cudaStream_t st = s.stream;
@@ -1031,7 +1034,7 @@ void render_guided(wr_scene &s, const wr_render_desc &desc, double *out, bool ou
             pass_steps = passes_left > 0 ? std::max(steps_left, 0) / passes_left : 0;
         }
         WR_CUDA(cudaEventRecord(s.ev0, st));
-        const double loss = pass_steps > 0 ? train_records(s, s.w_records.as<float4>(), n, batch, pass_steps, kGuideLr,
+        const double loss = pass_steps > 0 ? train_records(s, s.w_records.as<float4>(), n, batch, pass_steps, lr,
                                                           c_max, nullptr, &steps)
                                            : 0.0;
         WR_CUDA(cudaEventRecord(s.ev1, st));
