@@ -63,7 +63,7 @@ def scene_path(rank, world, dist, workload="heightfield"):
     """Writes the seeded workload once per node (rank 0), shared by the other ranks."""
     from wurstrenderer_b200 import scenes
     if workload == "jobs128":
-        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_cornell_v1")
+        d = os.path.join(tempfile.gettempdir(), "wurst_b200_bench_cornell_v2")
         p = os.path.join(d, "cornell.json")
         writer = lambda: scenes.write_cornell(d)
     elif workload in ("door", "c5"):

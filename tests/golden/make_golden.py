@@ -52,7 +52,8 @@ def write_fixture_scene(name, out_dir):
     if name.endswith("_ls"):   # the same scene rendered by light_splatting
         return with_integrator(write_fixture_scene(name[:-3], out_dir), "light_splatting")
     if name == "cornell":
-        return scenes.write_cornell(out_dir, name="cornell", resolution=(48, 48), spp=4, num_path_vertices=10)
+        return scenes.write_cornell(out_dir, name="cornell", resolution=(48, 48), spp=4, num_path_vertices=10,
+                                    spec=scenes.cornell_spec(box_angle=scenes.FIXTURE_BOX_ANGLE))
     if name == "zoo":
         return scenes.write_spec(out_dir, "zoo", scenes.material_zoo_spec(), scenes.CORNELL_CAMERA, (48, 40), 4, 10)
     if name == "env":

@@ -286,8 +286,14 @@ def nee_render(output, spp, num_path_vertices):
 # workloads
 # --------------------------------------------------------------------------
 
-def cornell_spec(seed=1001, light_ke=(17.0, 12.0, 4.0)):
-    """Procedural Cornell box: 5 walls (10 tris) + 2 boxes (24) + light (2) = 36 tris."""
+# rotation about y of the two boxes in the Cornell-box test fixtures (tests/golden/scenes): turned
+# boxes exercise faces that no axis slab bounds tightly; the workloads keep them axis-aligned
+FIXTURE_BOX_ANGLE = 0.3
+
+
+def cornell_spec(seed=1001, light_ke=(17.0, 12.0, 4.0), box_angle=0.0):
+    """Procedural Cornell box: 5 walls (10 tris) + 2 boxes (24) + light (2) = 36 tris. The boxes are
+    axis-aligned (workload C1) unless box_angle turns them about y (by -box_angle and +box_angle)."""
     rng = np.random.default_rng(seed)
     alb = lambda: tuple(rng.uniform(0.2, 0.8, 3))
     spec = SceneSpec()
@@ -303,9 +309,9 @@ def cornell_spec(seed=1001, light_ke=(17.0, 12.0, 4.0)):
               "right": (0.2, rng.uniform(0.6, 0.8), 0.2)}
     for name, (p, t) in walls.items():
         spec.add(name, Material("m_" + name, kd=colors[name]), p, t)
-    p, t = box((0.35, 0.3, 0.3), (0.6, 0.6, 0.6), angle_y=-0.3)
+    p, t = box((0.35, 0.3, 0.3), (0.6, 0.6, 0.6), angle_y=-box_angle)
     spec.add("short_box", Material("m_short_box", kd=alb()), p, t)
-    p, t = box((-0.35, 0.6, -0.35), (0.6, 1.2, 0.6), angle_y=0.3)
+    p, t = box((-0.35, 0.6, -0.35), (0.6, 1.2, 0.6), angle_y=box_angle)
     spec.add("tall_box", Material("m_tall_box", kd=alb()), p, t)
     y = 2.0 - 1e-3
     p, t = quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25))
@@ -327,10 +333,12 @@ def write_cornell(out_dir, name="cornell", resolution=(256, 256), spp=16,
 
 
 def write_cornell_lens(out_dir, name="lens", resolution=(48, 48), spp=4, num_path_vertices=10, radius=0.1):
-    """The Cornell box seen through a thin lens: the simple2 camera's "radius" key is both the
-    aperture radius and the focal distance (src/camera/thinlens.h:22-23)."""
+    """The Cornell box (fixture variant, turned boxes) seen through a thin lens: the simple2
+    camera's "radius" key is both the aperture radius and the focal distance
+    (src/camera/thinlens.h:22-23)."""
     cam = dict(CORNELL_CAMERA, resolution=list(resolution), radius=float(radius))
-    return write_scene(out_dir, name, cornell_spec(), cam, [nee_render(name + ".pfm", spp, num_path_vertices)])
+    return write_scene(out_dir, name, cornell_spec(box_angle=FIXTURE_BOX_ANGLE), cam,
+                       [nee_render(name + ".pfm", spp, num_path_vertices)])
 
 
 def write_srgb_zoo(out_dir, name="srgb", resolution=(48, 40), spp=4, num_path_vertices=10):
@@ -382,9 +390,10 @@ def write_phong_cornell(out_dir, name="phong_cornell", resolution=(128, 128), sp
 
 
 def material_zoo_spec(seed=7):
-    """Cornell box whose boxes exercise every BSDF: Oren-Nayar, Phong-only, Lambert+Phong."""
+    """Cornell box (fixture variant, turned boxes) whose boxes exercise every BSDF: Oren-Nayar,
+    Phong-only, Lambert+Phong."""
     rng = np.random.default_rng(seed)
-    spec = cornell_spec(seed)
+    spec = cornell_spec(seed, box_angle=FIXTURE_BOX_ANGLE)
     spec.materials["m_short_box"] = Material("m_short_box", kd=(0.6, 0.5, 0.4), sigma=0.4)
     spec.materials["m_tall_box"] = Material("m_tall_box", kd=(0.3, 0.35, 0.4), ks=(0.45, 0.4, 0.35),
                                             exponent=30.0)
