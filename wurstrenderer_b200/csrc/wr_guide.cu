@@ -15,8 +15,10 @@
 //                   ReLU -> smem) -> lobe parameters per path
 //   k_guide_train   forward (activations kept in smem), mixture-NLL gradient, backward:
 //                   dX = dH W (M128 N64 K64), dW += dH^T X (M64 N64 K128, MN-major operands,
-//                   accumulated in TMEM across all tiles of the CTA), one atomic flush per CTA
-//   k_guide_adam    Adam on the FP32 master weights, BF16 copies (W and W^T) for the kernels
+//                   accumulated in TMEM across all tiles of the CTA), the CTA's dW stored into
+//                   its own partial-gradient slot
+//   k_guide_adam    fixed-order sum of the partial slots, Adam on the FP32 master weights, and
+//                   the BF16 W and W^T images in the kernels' shared-memory operand layout
 #include <algorithm>
 #include <cmath>
 #include <cstdint>

@@ -35,11 +35,11 @@ constexpr int kPackedChunks = 5;
 constexpr int kRecordFloat4 = 5;
 
 struct GuideNet {
-    __nv_bfloat16 *w = nullptr;    // [layer][out][in] bf16 copy used by the kernels
-    __nv_bfloat16 *wt = nullptr;   // [layer][in][out] transposed bf16 copy (backward dX)
+    __nv_bfloat16 *w = nullptr;    // bf16 W of each layer as its shared-memory operand tile (8 KB per layer)
+    __nv_bfloat16 *wt = nullptr;   // bf16 W^T of each layer, the same way (backward dX)
     float *master = nullptr;       // FP32 master weights [layer][out][in]
     float *grad = nullptr;         // FP32 gradient summed over samples (filled by guide_sum_gradient)
-    float *partial = nullptr;      // per-CTA partial gradients, slots x kGuideParams
+    float *partial = nullptr;      // per-CTA partial gradients, slots x kGuideParams (layout: partial_offset)
     int slots = 0;                 // training CTAs (one per SM)
     float *m = nullptr, *v = nullptr;   // Adam moments
     uint32_t *err = nullptr;       // set to 1 when a tensor-core completion wait timed out
