@@ -18,7 +18,7 @@
 //                   accumulated in TMEM across all tiles of the CTA), the CTA's dW stored into
 //                   its own partial-gradient slot
 //   k_guide_adam    fixed-order sum of the partial slots, Adam on the FP32 master weights, and
-//                   the BF16 W and W^T images in the kernels' shared-memory operand layout
+//                   the BF16 W image in the kernels' shared-memory operand layout
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -229,8 +229,10 @@ __global__ void __launch_bounds__(kTile *kGroups, kInferCtasPerSm) k_guide_infer
 // rows. Warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31, so the thread of warpgroup j and
 // row r takes, in every epilogue, columns [16 j, 16 j + 16) of row r, and in the loss gradient
 // lobes 2 j and 2 j + 1 (the row's mixture density is summed over the four threads through
-// shared memory). One elected thread issues the MMAs; the dW products of a backward layer are
-// issued after the commit that the epilogue waits for, so they run under it.
+// shared memory). One elected thread issues the MMAs. The backward pass keeps every layer's
+// output gradient dH_l: the chain of dX products runs first (B = the W tile read MN-major, so no
+// transposed copy is needed), and the five dW products follow together after it, so none of them
+// delays a dX.
 constexpr int kTrainGroups = 4;
 constexpr int kTrainThreads = kTile * kTrainGroups;
 
@@ -247,75 +249,81 @@ __device__ __forceinline__ int partial_param(int u) {
     return (l * kW + n) * kW + col;
 }
 
-// shared memory: W and W^T images 40 KB each, X_0..X_4 80 KB, two dH tiles of 16 KB, each
-// followed by 8 KB of zeros (the operand reach of the weight-gradient MMA stays inside the
-// allocation for either reading of the descriptor's two strides), the density exchange
-// (4 x 128 floats), two mbarriers and the TMEM address slot
-constexpr int kTrainW = 0, kTrainWt = kWeightBytes, kTrainX = 2 * kWeightBytes;
+// shared memory: the W image 40 KB, X_0..X_4 80 KB (the layer inputs), dH_0..dH_4 80 KB (the
+// loss gradient at each layer's output) followed by 8 KB of zeros (the operand reach of the
+// weight-gradient MMA stays inside the allocation for either reading of the descriptor's two
+// strides), the density exchange (2 x 4 x 128 floats), two mbarriers and the TMEM address slot
+constexpr int kTrainW = 0, kTrainX = kWeightBytes;
 constexpr int kTrainDh = kTrainX + kLayers * kActBytes;
-constexpr int kTrainDhStride = kActBytes + 8192;
-constexpr int kTrainExch = kTrainDh + 2 * kTrainDhStride;
-constexpr int kTrainBarrier = kTrainExch + kTrainGroups * kTile * 4;
+constexpr int kTrainExch = kTrainDh + kLayers * kActBytes + 8192;
+constexpr int kTrainBarrier = kTrainExch + 2 * kTrainGroups * kTile * 4;
 constexpr size_t kTrainSmem = size_t(kTrainBarrier) + 64;
 static_assert(kTrainSmem <= 227 * 1024, "training tile does not fit in shared memory");
 
 // Terms of the mixture-NLL gradient (oracle: loss_grad_output) for lobes 2 J and 2 J + 1 of a
 // row, from the row's 40 used outputs o (5 per lobe: axis, sharpness, weight logit) and the
-// sample direction d. Returns the two lobes' share of the mixture density p(d).
+// sample direction d. The mixture weights are w_k = e_k / sum_k e_k with e_k = exp(logit_k - max);
+// the thread returns its two lobes' sums of e_k f_k and of e_k (the row's four threads add them up
+// through shared memory), so each lobe's exponential is evaluated by one thread only.
 struct LobeTerms {
-    float w[2], f[2], lam[2], cosk[2], mu[2][3], inr[2], e2[2], s[2];
+    float e[2], f[2], lam[2], cosk[2], mu[2][3], inr[2], e2[2], inv1me2[2], sig[2];
 };
 
 template <int J>
-__device__ __forceinline__ float lobe_terms(const float *o, f3 d, LobeTerms &t) {
+__device__ __forceinline__ float2 lobe_terms(const float *o, f3 d, LobeTerms &t) {
     float amax = -1e30f;
 #pragma unroll
     for (int k = 0; k < 8; ++k) amax = fmaxf(amax, o[5 * k + 4]);
-    float ew[8], wsum = 0.f;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        ew[k] = __expf(o[5 * k + 4] - amax);
-        wsum += ew[k];
-    }
-    const float inv_wsum = __fdividef(1.f, wsum);
-    float pp = 0.f;
+    float2 part = make_float2(0.f, 0.f);   // (sum e_k f_k, sum e_k) over this thread's lobes
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
         const int k = 2 * J + j;
         const float rx = o[5 * k], ry = o[5 * k + 1], rz = o[5 * k + 2];
-        t.inr[j] = __fdividef(1.f, fmaxf(sqrtf(rx * rx + ry * ry + rz * rz), 1e-12f));
+        t.inr[j] = rsqrtf(fmaxf(rx * rx + ry * ry + rz * rz, 1e-24f));   // 1 / max(|r|, 1e-12)
         t.mu[j][0] = rx * t.inr[j];
         t.mu[j][1] = ry * t.inr[j];
         t.mu[j][2] = rz * t.inr[j];
-        t.s[j] = o[5 * k + 3];
-        t.lam[j] = fminf(softplus(t.s[j]) + kLambdaMin, kLambdaMax);
-        t.w[j] = ew[k] * inv_wsum;
+        // softplus(s) = log(1 + e^s) and its derivative, the sigmoid e^s / (1 + e^s), from one exp
+        const float s = o[5 * k + 3];
+        float sp;
+        if (s > 20.f) {
+            sp = s;
+            t.sig[j] = 1.f;
+        } else {
+            const float es = __expf(s);
+            sp = __logf(1.f + es);
+            t.sig[j] = __fdividef(es, 1.f + es);
+        }
+        t.lam[j] = fminf(sp + kLambdaMin, kLambdaMax);
+        t.e[j] = __expf(o[5 * k + 4] - amax);
         t.cosk[j] = t.mu[j][0] * d.x + t.mu[j][1] * d.y + t.mu[j][2] * d.z;
         t.e2[j] = __expf(-2.f * t.lam[j]);   // lam >= kLambdaMin: 1 - e2 >= 0.63
-        t.f[j] = __fdividef(t.lam[j], 2.f * wrd::kPi * (1.f - t.e2[j])) * __expf(t.lam[j] * (t.cosk[j] - 1.f));
-        pp += t.w[j] * t.f[j];
+        t.inv1me2[j] = __fdividef(1.f, 1.f - t.e2[j]);
+        t.f[j] = t.lam[j] * t.inv1me2[j] * (0.5f / wrd::kPi) * __expf(t.lam[j] * (t.cosk[j] - 1.f));
+        part.x += t.e[j] * t.f[j];
+        part.y += t.e[j];
     }
-    return pp;
+    return part;
 }
 
-// d(-c log p)/d(outputs) of the two lobes (cc = the clamped loss weight, ip = 1 / p) into
-// columns [10 J, 10 J + 10) of a row of the dH tile; the thread of lobes 6 and 7 also zeroes
+// d(-c log p)/d(outputs) of the two lobes (cc = the clamped loss weight, ip = 1 / p, iw = 1 / sum e)
+// into columns [10 J, 10 J + 10) of a row of the dH tile; the thread of lobes 6 and 7 also zeroes
 // the unused columns 40..63
 template <int J>
-__device__ __forceinline__ void lobe_grads_store(const LobeTerms &t, f3 d, float cc, float ip, bool active,
+__device__ __forceinline__ void lobe_grads_store(const LobeTerms &t, f3 d, float cc, float ip, float iw, bool active,
                                                  unsigned char *tile, int row) {
     float go[10];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-        const float resp = t.w[j] * t.f[j] * ip;
-        const float dldl = __fdividef(1.f, t.lam[j]) - __fdividef(2.f * t.e2[j], 1.f - t.e2[j]) + (t.cosk[j] - 1.f);
-        const float sig = __fdividef(1.f, 1.f + __expf(-t.s[j]));
+        const float w = t.e[j] * iw;
+        const float resp = w * t.f[j] * ip;
+        const float dldl = __fdividef(1.f, t.lam[j]) - 2.f * t.e2[j] * t.inv1me2[j] + (t.cosk[j] - 1.f);
         const float a = -cc * resp * t.lam[j] * t.inr[j];
         go[5 * j + 0] = a * (d.x - t.mu[j][0] * t.cosk[j]);
         go[5 * j + 1] = a * (d.y - t.mu[j][1] * t.cosk[j]);
         go[5 * j + 2] = a * (d.z - t.mu[j][2] * t.cosk[j]);
-        go[5 * j + 3] = -cc * resp * dldl * sig;
-        go[5 * j + 4] = -cc * (resp - t.w[j]);
+        go[5 * j + 3] = -cc * resp * dldl * t.sig[j];
+        go[5 * j + 4] = -cc * (resp - w);
     }
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -327,7 +335,7 @@ __device__ __forceinline__ void lobe_grads_store(const LobeTerms &t, f3 d, float
         for (int c = 40; c < kW; c += 8) *reinterpret_cast<uint4 *>(tile + tile_offset(row, c)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-__device__ __forceinline__ float lobe_terms_of(int j, const float *o, f3 d, LobeTerms &t) {
+__device__ __forceinline__ float2 lobe_terms_of(int j, const float *o, f3 d, LobeTerms &t) {
     switch (j) {
     case 0: return lobe_terms<0>(o, d, t);
     case 1: return lobe_terms<1>(o, d, t);
@@ -336,13 +344,13 @@ __device__ __forceinline__ float lobe_terms_of(int j, const float *o, f3 d, Lobe
     }
 }
 
-__device__ __forceinline__ void lobe_grads_store_of(int j, const LobeTerms &t, f3 d, float cc, float ip, bool active,
-                                                    unsigned char *tile, int row) {
+__device__ __forceinline__ void lobe_grads_store_of(int j, const LobeTerms &t, f3 d, float cc, float ip, float iw,
+                                                    bool active, unsigned char *tile, int row) {
     switch (j) {
-    case 0: lobe_grads_store<0>(t, d, cc, ip, active, tile, row); break;
-    case 1: lobe_grads_store<1>(t, d, cc, ip, active, tile, row); break;
-    case 2: lobe_grads_store<2>(t, d, cc, ip, active, tile, row); break;
-    default: lobe_grads_store<3>(t, d, cc, ip, active, tile, row); break;
+    case 0: lobe_grads_store<0>(t, d, cc, ip, iw, active, tile, row); break;
+    case 1: lobe_grads_store<1>(t, d, cc, ip, iw, active, tile, row); break;
+    case 2: lobe_grads_store<2>(t, d, cc, ip, iw, active, tile, row); break;
+    default: lobe_grads_store<3>(t, d, cc, ip, iw, active, tile, row); break;
     }
 }
 
@@ -364,8 +372,8 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
                                                                  float c_max, double *loss_out) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *wt = smem + kTrainW;      // W image   5 x 8 KB
-    unsigned char *wtt = smem + kTrainWt;    // W^T image 5 x 8 KB
     unsigned char *xt = smem + kTrainX;      // X_0..X_4  5 x 16 KB (the layer inputs, kept for backward)
+    unsigned char *dht = smem + kTrainDh;    // dH_0..dH_4 5 x 16 KB (the gradients at the layer outputs)
     float *exch = reinterpret_cast<float *>(smem + kTrainExch);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kTrainBarrier);   // [0] MMA completion, [1] weights
     uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kTrainBarrier + 16);
@@ -385,9 +393,8 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
         mbar_init(mb, 1);
         mbar_init(mbw, 1);
     }
-    for (int i = tid; i < 2 * 512; i += kTrainThreads)   // the zeros behind both dH tiles
-        reinterpret_cast<uint4 *>(smem + kTrainDh + (i >> 9) * kTrainDhStride + kActBytes)[i & 511] =
-            make_uint4(0u, 0u, 0u, 0u);
+    for (int i = tid; i < 512; i += kTrainThreads)   // the zeros behind the dH tiles
+        reinterpret_cast<uint4 *>(dht + kLayers * kActBytes)[i] = make_uint4(0u, 0u, 0u, 0u);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
@@ -396,6 +403,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
     const uint32_t tD = tmem, tdW = tmem + 64;   // columns [0, 64) scratch, [64, 384) dW of layers 0..4
     const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
     const uint32_t id_fwd = idesc_bf16(128, 64, 0, 0);
+    const uint32_t id_dx = idesc_bf16(128, 64, 0, 1);   // B = the W tile read MN-major (rows = K = out)
     const uint32_t id_dw = idesc_bf16(64, 64, 1, 1);
     uint32_t phase = 0;
     // failed: a wait of this thread gave up; stop: the CTA's vote on it at the next barrier (a
@@ -421,13 +429,12 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
         }
         store_row_part(xt, r, x, grp);
         if (tile == blockIdx.x) {
-            // the previous kernels of the stream are complete from here on: the weight images may
+            // the previous kernels of the stream are complete from here on: the weight image may
             // be read and this CTA's partial-gradient slot written
             griddep_wait();
-            if (tid == 0) {   // both weight images in two bulk copies
-                mbar_expect_tx(mbw, 2 * kWeightBytes);
+            if (tid == 0) {   // the weight image in one bulk copy
+                mbar_expect_tx(mbw, kWeightBytes);
                 bulk_load(smem_addr(wt), g.w, kWeightBytes, mbw);
-                bulk_load(smem_addr(wtt), g.wt, kWeightBytes, mbw);
             }
         }
         fence_async_smem();
@@ -469,47 +476,50 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
             if (stop) break;
         }
         if (stop) break;
-        // loss gradient at the outputs -> dH tile 0 (bf16)
+        // loss gradient at the outputs -> dH_4 (bf16)
         const bool active = valid && c > 0.f;
         LobeTerms lt{};
-        exch[grp * kTile + r] = active ? lobe_terms_of(grp, out, dir, lt) : 0.f;
+        const float2 part = active ? lobe_terms_of(grp, out, dir, lt) : make_float2(0.f, 0.f);
+        exch[grp * kTile + r] = part.x;
+        exch[(kTrainGroups + grp) * kTile + r] = part.y;
         fence_before_sync();
         stop = __syncthreads_or(failed);
         fence_after_sync();
         if (stop) break;
-        const float p = fmaxf(exch[r] + exch[kTile + r] + exch[2 * kTile + r] + exch[3 * kTile + r], 1e-30f);
+        const float sum_ef = (exch[r] + exch[kTile + r]) + (exch[2 * kTile + r] + exch[3 * kTile + r]);
+        const float sum_e = (exch[4 * kTile + r] + exch[5 * kTile + r]) + (exch[6 * kTile + r] + exch[7 * kTile + r]);
+        const float iw = active ? __fdividef(1.f, sum_e) : 0.f;
+        const float p = fmaxf(sum_ef * iw, 1e-30f);
         const float cc = fminf(c, c_max);
         if (active && grp == 0) loss += double(-cc * __logf(p));
-        lobe_grads_store_of(grp, lt, dir, cc, __fdividef(1.f, p), active, smem + kTrainDh, r);
+        lobe_grads_store_of(grp, lt, dir, cc, __fdividef(1.f, p), iw, active, dht + (kLayers - 1) * kActBytes, r);
         fence_async_smem();
         fence_before_sync();
         __syncthreads();
         fence_after_sync();
-        // backward: dH alternates between the two tiles
-        int cur = 0;
+        // backward: the dX chain dH_l -> dH_{l-1}, then every layer's dW at once
         for (int l = kLayers - 1; l >= 0; --l) {
-            unsigned char *dh = smem + kTrainDh + cur * kTrainDhStride;
-            unsigned char *dh_next = smem + kTrainDh + (cur ^ 1) * kTrainDhStride;
             if (tid == 0) {
-                const uint32_t a0 = smem_addr(dh);
                 if (l > 0) {
-                    // dX = dH W_l : M = 128, N = 64 (in), K = 64 (out); B = the W^T tile
-                    const uint32_t c0 = smem_addr(wtt + l * 8192);
+                    // dX = dH_l W_l : M = 128, N = 64 (in), K = 64 (out); B = the W tile, MN-major
+                    const uint32_t a0 = smem_addr(dht + l * kActBytes), b0 = smem_addr(wt + l * 8192);
 #pragma unroll
                     for (int ks = 0; ks < 4; ++ks)
-                        mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(c0 + ks * 256, 128, 1024), id_fwd,
+                        mma_bf16(tD, smem_desc(a0 + ks * 256, 128, 1024), smem_desc(b0 + ks * 2048, 1024, 128), id_dx,
                                  ks > 0 ? 1u : 0u);
-                    mma_commit(mb);
-                }
-                // dW_l += dH^T X_l : M = 64 (out), N = 64 (in), K = 128 (rows), MN-major operands.
-                // Issued after the commit: it runs under this layer's epilogue and the next
-                // commit covers it (the epilogue after that one overwrites this dH tile)
-                const uint32_t b0 = smem_addr(xt + l * kActBytes);
+                } else {
+                    // dW_l += dH_l^T X_l for every layer: M = 64 (out), N = 64 (in), K = 128 (rows),
+                    // MN-major operands, accumulated in TMEM over the CTA's tiles
+#pragma unroll 1
+                    for (int k = kLayers - 1; k >= 0; --k) {
+                        const uint32_t a0 = smem_addr(dht + k * kActBytes), b0 = smem_addr(xt + k * kActBytes);
 #pragma unroll
-                for (int ks = 0; ks < 8; ++ks)
-                    mma_bf16(tdW + 64 * l, smem_desc(a0 + ks * 2048, 1024, 128), smem_desc(b0 + ks * 2048, 1024, 128),
-                             id_dw, (any_tile || ks > 0) ? 1u : 0u);
-                if (l == 0) mma_commit(mb);
+                        for (int ks = 0; ks < 8; ++ks)
+                            mma_bf16(tdW + 64 * k, smem_desc(a0 + ks * 2048, 1024, 128),
+                                     smem_desc(b0 + ks * 2048, 1024, 128), id_dw, (any_tile || ks > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(mb);
             }
             if (!mbar_wait(mb, phase, kWaitIters)) failed = true;
             phase ^= 1u;
@@ -518,14 +528,13 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_guide_train(GuideNet g, co
                 float v[16];
                 tmem_ld16(tD + lane_base + 16 * grp, v);
                 relu_mask_row(xt + l * kActBytes, r, v, 16 * grp, 2);   // input of layer l = ReLU output of layer l-1
-                store_row(dh_next, r, v, 16 * grp, 2);
+                store_row(dht + (l - 1) * kActBytes, r, v, 16 * grp, 2);
             }
             fence_async_smem();
             fence_before_sync();
             stop = __syncthreads_or(failed);
             fence_after_sync();
             if (stop) break;
-            cur ^= 1;
         }
         if (stop) break;
         any_tile = true;
@@ -635,7 +644,6 @@ __global__ void __launch_bounds__(kRedThreads) k_guide_adam(GuideNet g, float lr
     g.master[i] = w;
     const __nv_bfloat16 h = __float2bfloat16_rn(w);
     g.w[weight_image_index(l, nrow, k)] = h;
-    g.wt[weight_image_index(l, k, nrow)] = h;
 }
 
 // sum of c and number of records with c > 0 over records [0, n)
@@ -688,7 +696,6 @@ static void check(cudaError_t e, const char *what) {
 
 void guide_alloc(GuideNet &g) {
     check(cudaMalloc(&g.w, kParams * 2), "guide alloc");
-    check(cudaMalloc(&g.wt, kParams * 2), "guide alloc");
     check(cudaMalloc(&g.master, kParams * 4), "guide alloc");
     check(cudaMalloc(&g.grad, kParams * 4), "guide alloc");
     int dev = 0, sms = 148;
@@ -707,7 +714,7 @@ void guide_alloc(GuideNet &g) {
 }
 
 void guide_free(GuideNet &g) {
-    for (void *p : {(void *)g.w, (void *)g.wt, (void *)g.master, (void *)g.grad, (void *)g.partial, (void *)g.m,
+    for (void *p : {(void *)g.w, (void *)g.master, (void *)g.grad, (void *)g.partial, (void *)g.m,
                     (void *)g.v,
                     (void *)g.err})
         if (p) cudaFree(p);

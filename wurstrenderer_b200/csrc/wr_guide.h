@@ -36,7 +36,6 @@ constexpr int kRecordFloat4 = 5;
 
 struct GuideNet {
     __nv_bfloat16 *w = nullptr;    // bf16 W of each layer as its shared-memory operand tile (8 KB per layer)
-    __nv_bfloat16 *wt = nullptr;   // bf16 W^T of each layer, the same way (backward dX)
     float *master = nullptr;       // FP32 master weights [layer][out][in]
     float *grad = nullptr;         // FP32 gradient summed over samples (filled by guide_sum_gradient)
     float *partial = nullptr;      // per-CTA partial gradients, slots x kGuideParams (layout: partial_offset)
