@@ -2,7 +2,7 @@
 // triangle centroid, then the triangle index), after Karras, "Maximizing
 // Parallelism in the Construction of BVHs, Octrees, and k-d Trees" (HPG 2012).
 //
-//   k_lbvh_keys     centroid -> Morton code -> key (Morton << 32 | index)
+//   k_lbvh_keys     centroid -> Morton code on a cubic grid -> key (Morton << 32 | index)
 //   radix sort      CUB DeviceRadixSort on (key, triangle) pairs
 //   k_lbvh_topology one thread per inner node: key range, split, children, parents
 //   k_lbvh_refit    one thread per leaf walking to the root; the second thread to
@@ -200,8 +200,12 @@ BvhBuildResult build_bvh_lbvh(const std::vector<float> &tri_vertices, cudaStream
             hi[c] = std::max(hi[c], cen);
         }
     float3 lo3 = make_float3(lo[0], lo[1], lo[2]);
-    float3 inv = make_float3(hi[0] > lo[0] ? 1.f / (hi[0] - lo[0]) : 0.f, hi[1] > lo[1] ? 1.f / (hi[1] - lo[1]) : 0.f,
-                             hi[2] > lo[2] ? 1.f / (hi[2] - lo[2]) : 0.f);
+    // one scale for the three axes (the Morton grid's cells are cubes over the centroid box's
+    // longest side): on a flat scene, a grid stretched to the box per axis would split the thin
+    // axis as often as the long ones (600 against 568 Mpaths/s on the 1M-triangle workload)
+    const float ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    const float iext = ext > 0.f ? 1.f / ext : 0.f;
+    float3 inv = make_float3(iext, iext, iext);
     Tmp verts, keys, keys2, ids, ids2, child, pin, pleaf, box, flag, nodes, temp;
     verts.alloc(tri_vertices.size() * 4);
     keys.alloc(size_t(n) * 8);
