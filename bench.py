@@ -22,7 +22,9 @@ reduce and read-back of the reduced film).
 The default run also carries the guided-vs-plain equal-time studies of the two
 guided workloads against their FP64 reference crops: the door-gap room (config 4,
 `equal_time_relmse`) and the 10M-triangle full combination (config 5, `c5`, with
-its plain Mpaths/s).
+its plain Mpaths/s). Both train with config 4's Adam learning rate, 1e-3; each
+also repeats its guided renders at 2e-3 under `lr_0.002` (same plain renders).
+The `lbvh` key renders the same workload on the device-built LBVH tree.
 The CPU baseline runs the oracle (the reference's own renderer code compiled
 here, or its FP64 restatement) on the box's host cores on a bounded sample of
 the same workload (full frame at reduced spp; per-path work is unchanged).
