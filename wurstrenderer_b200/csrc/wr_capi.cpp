@@ -614,6 +614,8 @@ void render_jobs(wr_scene &s, const std::vector<HostJob> &jobs, const wr_render_
     r.fetch_min = desc.fetch_threshold > 0 ? desc.fetch_threshold : 20;
     r.num_jobs = int(table.size());
     r.job0 = table[0];
+    r.nee_only = 1;
+    for (const auto &j : table) r.nee_only &= j.integrator == wrd::INTEGRATOR_NEE ? 1 : 0;
     if (table.size() > 1) {
         upload(s.w_jobs, table, st);
         r.jobs = s.w_jobs.as<wrd::DevJob>();

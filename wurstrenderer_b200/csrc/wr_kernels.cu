@@ -545,6 +545,7 @@ __device__ __forceinline__ void dead_ray(const DevScene &s, f3 &o, f3 &d) {
 // proposal, one-sample MIS between the guide and the BSDF -- and compaction of the
 // continued path into the next wavefront. Called by all 32 lanes of a warp together
 // (warp-aggregated appends); `valid` is false for lanes past the end of the wavefront.
+template <bool NEE_ONLY>
 __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w, uint32_t i, bool valid,
                                            const wrg::PackedLobes *gl) {
     bool alive = false, shadow = false;
@@ -572,8 +573,8 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
         sample = __float_as_uint(t4.w);
         const uint32_t tri = __float_as_uint(h.w);
         const float t = h.x;
-        const bool primitive = J.integrator == INTEGRATOR_PRIMITIVE;
-        if (J.integrator == INTEGRATOR_LIGHT) {
+        const bool primitive = !NEE_ONLY && J.integrator == INTEGRATOR_PRIMITIVE;
+        if (!NEE_ONLY && J.integrator == INTEGRATOR_LIGHT) {
             // light_splatting: a vertex of the light subpath (randomWalk callback,
             // lightsplatting.h:85-104); emitter hits and misses end the subpath
             if (tri != MISS && !(__ldg(s.tri_mat + tri) & LIGHT_BIT)) {
@@ -762,11 +763,14 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
 }
 
 // GUIDED: the learned proposal is on (w.lobes); a separate instantiation keeps the plain
-// shade kernel's register count unchanged. Both run 3 blocks per SM: the guided kernel is
+// shade kernel's register count unchanged. NEE_ONLY: every job of the launch is
+// nextevent_path_tracer, so the primitive-tracer and light-splatting branches are compiled out
+// (fewer spills: 657.9 against 650.8 Mpaths/s on the 1M-triangle render; guided renders are
+// always NEE). Both run 3 blocks per SM: the guided kernel is
 // latency-bound, and at 80 registers (with spills) it measured faster than at 128 registers and
 // 2 blocks per SM (80.2 against 93.6 ms of shading in a 64-spp render of the door-gap room); 4
 // blocks (64 registers) gained nothing on it and cost 0.7 % on the plain 1M-triangle render.
-template <bool GUIDED>
+template <bool GUIDED, bool NEE_ONLY>
 __global__ void __launch_bounds__(kShadeBlock, 3) k_shade(DevScene s, WaveArgs w) {
     const uint32_t n = w.ctr[CTR_ACTIVE];
     if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 1, (unsigned long long)n);
@@ -783,9 +787,9 @@ __global__ void __launch_bounds__(kShadeBlock, 3) k_shade(DevScene s, WaveArgs w
 #pragma unroll
                 for (int c = 0; c < wrg::kPackedChunks; ++c) pl.c[c] = make_uint4(0u, 0u, 0u, 0u);
             }
-            shade_path(s, w, i, i < n, &pl);
+            shade_path<NEE_ONLY>(s, w, i, i < n, &pl);
         } else {
-            shade_path(s, w, i, i < n, nullptr);
+            shade_path<NEE_ONLY>(s, w, i, i < n, nullptr);
         }
     }
 }
@@ -1191,8 +1195,9 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
     switch (which) {
         case KERNEL_EXTEND: launch_trace(TRACE_EXTEND, s, w, r, st); break;
         case KERNEL_SHADE:
-            if (w.lobes) k_shade<true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
-            else k_shade<false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            if (w.lobes) k_shade<true, true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else if (r.nee_only) k_shade<false, true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else k_shade<false, false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
             break;
         case KERNEL_GUIDE:
             if (r.guide)
@@ -1289,7 +1294,7 @@ int occupancy_blocks(int which, int trace_block, bool phong, bool wide) {
         else if (trace_block == 256) nb = extend_occupancy_3<256>(phong, wide);
         else nb = extend_occupancy_3<128>(phong, wide);
     } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false, false>, kShadeBlock, 0);
     }
     return nb;
 }

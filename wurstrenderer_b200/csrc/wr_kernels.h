@@ -43,6 +43,8 @@ struct RenderLaunch {
     int record;                 // 1: collect training records
     int guide_sms;              // SM count (grid of the inference kernel)
     int fetch_min;              // dynamic ray fetching threshold (lanes still traversing)
+    int nee_only;               // 1: every job is nextevent_path_tracer (shade without the other
+                                // integrators' branches); 0: any mix of integrators
 };
 
 enum KernelId { KERNEL_EXTEND = 0, KERNEL_SHADE = 1, KERNEL_RAYGEN = 2, KERNEL_SHADOW = 3, KERNEL_ADVANCE = 4,

@@ -185,6 +185,9 @@ extern "C" int wr_render_device_noalloc(wr_scene *scene, const wr_render_desc *d
     r.job0.sample_begin = 0;
     r.job0.seed = desc.seed;
     r.job0.integrator = integrator;
+    // the same shade kernel as wr_render_device picks for a one-job NEE render, so that both entry
+    // points compute the same image
+    r.nee_only = integrator == wrd::INTEGRATOR_NEE ? 1 : 0;
     r.total_pix = uint32_t(npix);
     r.total_samples = (unsigned long long)npix * unsigned(spp);
     const unsigned long long waves = (r.total_samples + kCapacity - 1) / kCapacity;
