@@ -545,9 +545,10 @@ __device__ __forceinline__ void dead_ray(const DevScene &s, f3 &o, f3 &d) {
 // proposal, one-sample MIS between the guide and the BSDF -- and compaction of the
 // continued path into the next wavefront. Called by all 32 lanes of a warp together
 // (warp-aggregated appends); `valid` is false for lanes past the end of the wavefront.
-template <bool NEE_ONLY>
+template <bool NEE_ONLY, bool RECORD>
 __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w, uint32_t i, bool valid,
                                            const wrg::PackedLobes *gl) {
+    float4 *const records = RECORD ? w.records : nullptr;   // training records (guided training passes)
     bool alive = false, shadow = false;
     f3 so = mk(0, 0, 0), sd = mk(0, 0, 1), sc = mk(0, 0, 0);
     float stmax = 0.f;
@@ -563,7 +564,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
         // last reads of this bounce's path state (streaming: evict-first in L2)
         const float4 o4 = __ldcs(&w.cur.o[i]), d4 = __ldcs(&w.cur.d[i]), t4 = __ldcs(&w.cur.thr[i]);
         meta = __ldcs(&w.cur.meta[i]);
-        if (w.records) rec = __ldcs(&w.cur.rec[i]);
+        if (records) rec = __ldcs(&w.cur.rec[i]);
         const uint32_t depth = meta & 0xffu, job = meta >> 8;
         const DevJob &J = job_at(w, job);
         const float4 h = __ldcs(&w.hit[i]);
@@ -624,7 +625,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                 const f3 c = thr * env_eval(s, d) * mis;
                 if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
                     film_add(w, pixel, c);
-                    if (w.records) record_contribution(w.records, rec, c);
+                    if (records) record_contribution(records, rec, c);
                 }
             }
         } else {
@@ -644,7 +645,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                                           __ldg(&s.lights[li].intensity[2])) * mis;
                     if (!is_zero(c) && isfinite(c.x + c.y + c.z)) {
                         film_add(w, pixel, c);
-                        if (w.records) record_contribution(w.records, rec, c);
+                        if (records) record_contribution(records, rec, c);
                     }
                 }
             } else if (int(depth) + 2 < J.nverts) {
@@ -725,7 +726,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
                     nd = normalize(fr.to_world(outL));
                     nthr = thr * wgt;
                     npdf = pdfW;
-                    if (w.records) {
+                    if (records) {
                         want_rec = true;
                         rec_pos = pos;
                         rec_wo = wi;
@@ -737,12 +738,12 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
         }
     }
     push_shadow(w, shadow, so, sd, stmax, shadow_slot == MISS ? pixel : shadow_slot, sc, rec);
-    if (w.records) {   // training record of this vertex (parent: the path's previous record)
+    if (records) {   // training record of this vertex (parent: the path's previous record)
         uint32_t nr;
         const uint32_t r = warp_append(w.rec_count, want_rec, nr);
         nrec = rec;
         if (want_rec && r < w.rec_capacity) {
-            float4 *R = w.records + wrg::kRecordFloat4 * size_t(r);
+            float4 *R = records + wrg::kRecordFloat4 * size_t(r);
             R[0] = make_float4(rec_pos.x, rec_pos.y, rec_pos.z, 0.f);
             R[1] = make_float4(rec_n.x, rec_n.y, rec_n.z, __uint_as_float(rec));
             R[2] = make_float4(rec_wo.x, rec_wo.y, rec_wo.z, 0.f);
@@ -758,7 +759,7 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
         __stcs(&w.nxt.d[j], make_float4(nd.x, nd.y, nd.z, __uint_as_float(pixel)));
         __stcs(&w.nxt.thr[j], make_float4(nthr.x, nthr.y, nthr.z, __uint_as_float(sample)));
         __stcs(&w.nxt.meta[j], meta + 1u);
-        if (w.records) __stcs(&w.nxt.rec[j], nrec);
+        if (records) __stcs(&w.nxt.rec[j], nrec);
     }
 }
 
@@ -766,11 +767,12 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const WaveArgs &w,
 // shade kernel's register count unchanged. NEE_ONLY: every job of the launch is
 // nextevent_path_tracer, so the primitive-tracer and light-splatting branches are compiled out
 // (fewer spills: 657.9 against 650.8 Mpaths/s on the 1M-triangle render; guided renders are
-// always NEE). Both run 3 blocks per SM: the guided kernel is
+// always NEE). RECORD: the launch collects training records (guided training passes only); the
+// other launches, the final guided pass among them, run without that code. Both run 3 blocks per SM: the guided kernel is
 // latency-bound, and at 80 registers (with spills) it measured faster than at 128 registers and
 // 2 blocks per SM (80.2 against 93.6 ms of shading in a 64-spp render of the door-gap room); 4
 // blocks (64 registers) gained nothing on it and cost 0.7 % on the plain 1M-triangle render.
-template <bool GUIDED, bool NEE_ONLY>
+template <bool GUIDED, bool NEE_ONLY, bool RECORD>
 __global__ void __launch_bounds__(kShadeBlock, 3) k_shade(DevScene s, WaveArgs w) {
     const uint32_t n = w.ctr[CTR_ACTIVE];
     if (w.prof && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(w.prof + 1, (unsigned long long)n);
@@ -787,9 +789,9 @@ __global__ void __launch_bounds__(kShadeBlock, 3) k_shade(DevScene s, WaveArgs w
 #pragma unroll
                 for (int c = 0; c < wrg::kPackedChunks; ++c) pl.c[c] = make_uint4(0u, 0u, 0u, 0u);
             }
-            shade_path<NEE_ONLY>(s, w, i, i < n, &pl);
+            shade_path<NEE_ONLY, RECORD>(s, w, i, i < n, &pl);
         } else {
-            shade_path<NEE_ONLY>(s, w, i, i < n, nullptr);
+            shade_path<NEE_ONLY, RECORD>(s, w, i, i < n, nullptr);
         }
     }
 }
@@ -1195,9 +1197,11 @@ void launch_kernel(int which, const DevScene &s, const WaveBuffers &b, const Ren
     switch (which) {
         case KERNEL_EXTEND: launch_trace(TRACE_EXTEND, s, w, r, st); break;
         case KERNEL_SHADE:
-            if (w.lobes) k_shade<true, true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
-            else if (r.nee_only) k_shade<false, true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
-            else k_shade<false, false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            if (w.lobes && w.records) k_shade<true, true, true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else if (w.lobes) k_shade<true, true, false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else if (w.records) k_shade<false, false, true><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else if (r.nee_only) k_shade<false, true, false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
+            else k_shade<false, false, false><<<r.grid_shade, kShadeBlock, 0, st>>>(s, w);
             break;
         case KERNEL_GUIDE:
             if (r.guide)
@@ -1294,7 +1298,7 @@ int occupancy_blocks(int which, int trace_block, bool phong, bool wide) {
         else if (trace_block == 256) nb = extend_occupancy_3<256>(phong, wide);
         else nb = extend_occupancy_3<128>(phong, wide);
     } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false, false>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false, false, false>, kShadeBlock, 0);
     }
     return nb;
 }
