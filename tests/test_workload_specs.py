@@ -67,3 +67,15 @@ def test_door_room_of_config_4():
     assert len(lights) == 1
     ext = lights[0].positions.max(axis=0) - lights[0].positions.min(axis=0)
     assert np.allclose(sorted(ext)[1:], [1.0, 1.0], atol=1e-6)   # the 1 x 1 emitter
+
+
+@pytest.mark.timeout(600)
+def test_full_combination_of_config_5():
+    spec = scenes.full_combination_spec()
+    assert spec.num_triangles == 9980450   # about 10M
+    lights = [m for m in spec.meshes if any(spec.materials[m.material].ke)]
+    assert len(lights) == 16
+    exps = [m.exponent for m in spec.materials.values() if m.exponent > 0]
+    assert max(exps) <= 2000.0 and max(exps) > 1000.0   # glossy Phong up to exponent 2000
+    sky = scenes.envmap_image(2048, 1024)
+    assert sky.shape == (1024, 2048, 3) and sky.dtype == np.float32 and (sky > 0).all()
